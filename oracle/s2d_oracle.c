@@ -1,0 +1,449 @@
+/*
+ * s2d_oracle.c -- CPU restatement of SeisAcoMod2D's per-shot forward path.
+ *
+ * TEST INFRASTRUCTURE (the checker, never the product): loaded only by
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg.
+ *
+ * Every routine names the reference lines it restates.  Paths are relative to
+ * the SeisAcoMod2D source tree:
+ *   CM  = src/src_cpu/cpumodelling.cpp
+ *   CK  = src/src_cpu/cpu_modelling_kernels.cpp
+ * Arithmetic in the ORC_F64 variant keeps the reference's float/double mix and
+ * operation order, so its seismograms are expected to equal the reference's
+ * bit for bit; the ORC_F32 variant runs the same steps in FP32.
+ */
+#include "s2d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_PI 3.141592654 /* CM:9, CK:7 */
+
+/* 4th-order staggered coefficients, CK:9-10.  The reference's macro
+ * "-1.0f/24.0f" is a float quotient, so a1 carries float rounding. */
+static const float ORC_A0 = 1.125f;
+static const float ORC_A1 = -1.0f / 24.0f;
+
+void orc_derive(const orc_params *p, orc_derived *d) {
+    /* CM:168-193 */
+    float inv_dx = 1.0f / p->dx, inv_dz = 1.0f / p->dz;
+    d->fd_nt = (int)ceilf(p->rec_len / p->fd_dt);
+    d->real_nt = (int)ceilf(p->rec_len / p->real_dt);
+    d->dtdx = (double)(p->fd_dt * inv_dx);
+    d->dtdz = (double)(p->fd_dt * inv_dz);
+    d->dt_factor = (int)(p->real_dt / p->fd_dt);
+    /* CM:183: sqrt(6.0f) resolves to the float overload of std::sqrt. */
+    double td = sqrtf(6.0f) / (ORC_PI * p->fm);
+    d->nts = (int)(5.0f * td / p->fd_dt) + 1;
+    if (d->nts > d->fd_nt) d->nts = d->fd_nt;
+    d->nnz = 2 * p->nb + p->nz;
+    d->nnx = 2 * p->nb + p->nx;
+}
+
+void orc_ricker(const orc_params *p, const orc_derived *d, double *w) {
+    /* CK:33-62 with iss == 2 */
+    double t0 = 1.5 * sqrt(6.0) / (ORC_PI * (double)p->fm);
+    for (int i = 0; i < d->nts; i++) {
+        double t = (double)(i * p->fd_dt);
+        double a = ORC_PI * (double)p->fm * (t - t0);
+        double a2 = a * a;
+        w[i] = (1.0f - 2.0f * a2) * exp(-a2);
+    }
+}
+
+int orc_cell(const orc_params *p, float x, float z) {
+    /* CM:288-289 and CK:15-22 */
+    int nnz = 2 * p->nb + p->nz;
+    float inv_dx = 1.0f / p->dx, inv_dz = 1.0f / p->dz;
+    int ix = (int)(x * inv_dx), iz = (int)(z * inv_dz);
+    return nnz * (ix + p->nb) + (iz + p->nb);
+}
+
+/* CM:39-60: copy [nx1][nz1] into the padded grid and replicate the edges. */
+static void expand(float *b, const float *a, int nb, int nnz, int nnx, int nz1, int nx1) {
+    for (int ix = 0; ix < nx1; ix++)
+        for (int iz = 0; iz < nz1; iz++) b[(nb + ix) * nnz + (nb + iz)] = a[ix * nz1 + iz];
+    for (int ix = 0; ix < nnx; ix++) {
+        for (int iz = 0; iz < nb; iz++) b[ix * nnz + iz] = b[ix * nnz + nb];
+        for (int iz = nz1 + nb; iz < nnz; iz++) b[ix * nnz + iz] = b[ix * nnz + nb + nz1 - 1];
+    }
+    for (int iz = 0; iz < nnz; iz++) {
+        for (int ix = 0; ix < nb; ix++) b[ix * nnz + iz] = b[nb * nnz + iz];
+        for (int ix = nb + nx1; ix < nnx; ix++) b[ix * nnz + iz] = b[(nb + nx1 - 1) * nnz + iz];
+    }
+}
+
+/* CK:64-121: kappa = vp^2 rho (double), buoyancy b = 1/rho, and its two
+ * staggered averages.  bz (reference bu1) averages along z; its last row is
+ * read from bx before bx is filled, so it is 0 (CK:100).  bx (reference bu2)
+ * averages along x; its last column copies bz of column nnx-2 (CK:115-119). */
+static void stagger(const float *vpe, const float *rhoe, float *bue, float *bx, float *bz,
+                    double *kappa, int nnz, int nnx) {
+    size_t N = (size_t)nnz * nnx;
+    memset(bx, 0, N * sizeof(float));
+    memset(bz, 0, N * sizeof(float));
+    for (size_t id = 0; id < N; id++) {
+        double vp2 = (double)vpe[id] * (double)vpe[id];
+        kappa[id] = vp2 * (double)rhoe[id];
+        bue[id] = rhoe[id] > 0.0f ? 1.0f / rhoe[id] : 10000000000.0f;
+    }
+    for (int i2 = 0; i2 < nnx; i2++) {
+        for (int i1 = 0; i1 < nnz - 1; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            bz[id] = 0.5f * (bue[id + 1] + bue[id]);
+        }
+        bz[(size_t)i2 * nnz + nnz - 1] = bx[(size_t)i2 * nnz + nnz - 2];
+    }
+    for (int i2 = 0; i2 < nnx - 1; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            bx[id] = 0.5f * (bue[id + nnz] + bue[id]);
+        }
+    for (int i1 = 0; i1 < nnz; i1++) bx[(size_t)(nnx - 1) * nnz + i1] = bz[(size_t)(nnx - 2) * nnz + i1];
+}
+
+/* CK:123-153: sponge at integer nodes.  spg uses the float overload of exp
+ * (its argument is float), spg1 the double one. */
+static void sponge_a(float fac, float *damp, float *damp1, int nb, int n) {
+    float *spg = (float *)calloc(nb + 1, sizeof(float));
+    float *spg1 = (float *)calloc(nb + 1, sizeof(float));
+    for (int i = 0; i < nb; i++) {
+        float x = (float)(nb - (i + 1));
+        float t = fac * x;
+        spg[i] = expf(-(t * t));
+        spg1[i] = (float)exp(-0.5 * (t * t));
+    }
+    for (int i = 0; i < nb; i++) {
+        damp[i] = spg[i];
+        damp1[i] = spg1[i];
+        damp[nb + n + i] = spg[nb - i - 1];
+        damp1[nb + n + i] = spg1[nb - i - 1];
+    }
+    for (int i = 0; i < n; i++) {
+        damp[i + nb] = 1.0f;
+        damp1[i + nb] = 1.0f;
+    }
+    free(spg);
+    free(spg1);
+}
+
+/* CK:155-199: sponge at half nodes. */
+static void sponge_b(float fac, float *damp, float *damp1, int nb, int n) {
+    float *spg = (float *)calloc(nb + 1, sizeof(float));
+    float *spg1 = (float *)calloc(nb + 1, sizeof(float));
+    for (int i = 0; i < nb - 1; i++) {
+        float x = (float)(nb - 1 - (i + 1)) + 0.5f;
+        float t = fac * x;
+        spg[i] = expf(-(t * t));
+        spg1[i] = (float)exp(-0.5 * (t * t));
+    }
+    for (int i = 0; i < nb - 1; i++) {
+        damp[i] = spg[i];
+        damp1[i] = spg1[i];
+    }
+    for (int i = 0; i < n + 1; i++) {
+        damp[i + nb - 1] = 1.0f;
+        damp1[i + nb - 1] = 1.0f;
+    }
+    for (int i = 0; i < nb; i++) {
+        float x = (float)((i + 1) - 1) + 0.5f;
+        float t = fac * x;
+        spg[i] = expf(-(t * t));
+        spg1[i] = (float)exp(-0.5 * (t * t));
+    }
+    for (int i = 0; i < nb; i++) {
+        damp[nb + n + i] = spg[i];
+        damp1[nb + n + i] = spg1[i];
+    }
+    free(spg);
+    free(spg1);
+}
+
+/* ---------------- FP64 step: CM:115-156 with CK:201-368 ------------------ */
+
+typedef struct {
+    int nnx, nnz;
+    size_t N;
+    double *p, *px, *pz, *vx, *vz, *d1, *d2;
+    const double *kw1, *kw2, *bw1, *bw2; /* CM:270-281 */
+    const float *damp1a, *damp2a, *damp1b, *damp2b;
+} f64_state;
+
+static void f64_step(f64_state *s, int isrc, double src_add, int inject) {
+    const int nnz = s->nnz, nnx = s->nnx;
+    const size_t N = s->N;
+    double *d1 = s->d1, *d2 = s->d2;
+    memset(d1, 0, N * sizeof(double));
+    memset(d2, 0, N * sizeof(double));
+    /* CK:201-229  der2 = D-x vx */
+    for (int i2 = 2; i2 < nnx - 1; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            d2[id] = ORC_A0 * (s->vx[id] - s->vx[id - nnz]) + ORC_A1 * (s->vx[id + nnz] - s->vx[id - 2 * nnz]);
+        }
+    for (int i1 = 0; i1 < nnz; i1++) {
+        size_t id = (size_t)i1 + (size_t)1 * nnz;
+        d2[id] = s->vx[id] - s->vx[id - nnz];
+        id = (size_t)i1 + (size_t)(nnx - 1) * nnz;
+        d2[id] = s->vx[id] - s->vx[id - nnz];
+    }
+    /* CK:231-258  der1 = D-z vz */
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 2; i1 < nnz - 1; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            d1[id] = ORC_A0 * (s->vz[id] - s->vz[id - 1]) + ORC_A1 * (s->vz[id + 1] - s->vz[id - 2]);
+        }
+    for (int i2 = 0; i2 < nnx; i2++) {
+        size_t id = (size_t)(nnz - 1) + (size_t)i2 * nnz;
+        d1[id] = s->vz[id] - s->vz[id - 1];
+        id = (size_t)1 + (size_t)i2 * nnz;
+        d1[id] = s->vz[id] - s->vz[id - 1];
+    }
+    /* CK:335-351  split-field pressure with sponge */
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            s->px[id] = s->damp2a[i2] * s->px[id] + s->kw2[id] * d2[id];
+            s->pz[id] = s->damp1a[i1] * s->pz[id] + s->kw1[id] * d1[id];
+        }
+    /* CM:136-140  source */
+    if (inject) s->px[isrc] = s->px[isrc] + src_add;
+    /* CK:318-333 */
+    for (size_t id = 0; id < N; id++) s->p[id] = s->px[id] + s->pz[id];
+    memset(d1, 0, N * sizeof(double));
+    memset(d2, 0, N * sizeof(double));
+    /* CK:260-287  der2 = D+x p */
+    for (int i2 = 1; i2 < nnx - 2; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            d2[id] = ORC_A0 * (s->p[id + nnz] - s->p[id]) + ORC_A1 * (s->p[id + 2 * nnz] - s->p[id - nnz]);
+        }
+    for (int i1 = 0; i1 < nnz; i1++) {
+        size_t id = (size_t)i1;
+        d2[id] = s->p[id + nnz] - s->p[id];
+        id = (size_t)i1 + (size_t)(nnx - 2) * nnz;
+        d2[id] = s->p[id + nnz] - s->p[id];
+    }
+    /* CK:289-316  der1 = D+z p */
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 1; i1 < nnz - 2; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            d1[id] = ORC_A0 * (s->p[id + 1] - s->p[id]) + ORC_A1 * (s->p[id + 2] - s->p[id - 1]);
+        }
+    for (int i2 = 0; i2 < nnx; i2++) {
+        size_t id = (size_t)(nnz - 2) + (size_t)i2 * nnz;
+        d1[id] = s->p[id + 1] - s->p[id];
+        id = (size_t)i2 * nnz;
+        d1[id] = s->p[id + 1] - s->p[id];
+    }
+    /* CK:353-368 */
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            s->vx[id] = s->damp2b[i2] * s->vx[id] + s->bw2[id] * d2[id];
+            s->vz[id] = s->damp1b[i1] * s->vz[id] + s->bw1[id] * d1[id];
+        }
+}
+
+/* ---------------- FP32 step: same scheme, FP32 arithmetic ---------------- */
+
+/* The same four derivative operators, with the per-row coefficient pair
+ * (c0, c1) that encodes the reference's edge rows: 4th order inside, plain
+ * difference on the rows CK:217-227 / 247-256 / 276-285 / 305-314 list, and
+ * zero on the row each operator leaves at 0. */
+static inline void dm_coef(int i, int n, float *c0, float *c1) { /* D- : rows [2,n-2] 4th, 1 and n-1 2nd, 0 zero */
+    if (i >= 2 && i <= n - 2) { *c0 = ORC_A0; *c1 = ORC_A1; }
+    else if (i == 1 || i == n - 1) { *c0 = 1.0f; *c1 = 0.0f; }
+    else { *c0 = 0.0f; *c1 = 0.0f; }
+}
+static inline void dp_coef(int i, int n, float *c0, float *c1) { /* D+ : rows [1,n-3] 4th, 0 and n-2 2nd, n-1 zero */
+    if (i >= 1 && i <= n - 3) { *c0 = ORC_A0; *c1 = ORC_A1; }
+    else if (i == 0 || i == n - 2) { *c0 = 1.0f; *c1 = 0.0f; }
+    else { *c0 = 0.0f; *c1 = 0.0f; }
+}
+
+typedef struct {
+    int nnx, nnz;
+    size_t N;
+    float *p, *px, *pz, *vx, *vz;
+    const float *kappa, *bx, *bz;
+    const float *damp1a, *damp2a, *damp1b, *damp2b;
+    const float *kxa, *kza, *kxb, *kzb; /* dt/d * damp?1 folded per column / row */
+} f32_state;
+
+#define AT(a, ix, iz) ((ix) < 0 || (ix) >= nnx || (iz) < 0 || (iz) >= nnz ? 0.0f : (a)[(size_t)(ix) * nnz + (iz)])
+
+static void f32_step(f32_state *s, int isrc, float src_add, int inject) {
+    const int nnz = s->nnz, nnx = s->nnx;
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx0, cx1;
+        dm_coef(ix, nnx, &cx0, &cx1);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz0, cz1;
+            dm_coef(iz, nnz, &cz0, &cz1);
+            size_t id = (size_t)ix * nnz + iz;
+            float dvx = cx0 * (AT(s->vx, ix, iz) - AT(s->vx, ix - 1, iz)) + cx1 * (AT(s->vx, ix + 1, iz) - AT(s->vx, ix - 2, iz));
+            float dvz = cz0 * (AT(s->vz, ix, iz) - AT(s->vz, ix, iz - 1)) + cz1 * (AT(s->vz, ix, iz + 1) - AT(s->vz, ix, iz - 2));
+            float k = s->kappa[id];
+            s->px[id] = s->damp2a[ix] * s->px[id] + (s->kxa[ix] * k) * dvx;
+            s->pz[id] = s->damp1a[iz] * s->pz[id] + (s->kza[iz] * k) * dvz;
+        }
+    }
+    if (inject) s->px[isrc] = s->px[isrc] + src_add;
+    for (size_t id = 0; id < s->N; id++) s->p[id] = s->px[id] + s->pz[id];
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx0, cx1;
+        dp_coef(ix, nnx, &cx0, &cx1);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz0, cz1;
+            dp_coef(iz, nnz, &cz0, &cz1);
+            size_t id = (size_t)ix * nnz + iz;
+            float dpx = cx0 * (AT(s->p, ix + 1, iz) - AT(s->p, ix, iz)) + cx1 * (AT(s->p, ix + 2, iz) - AT(s->p, ix - 1, iz));
+            float dpz = cz0 * (AT(s->p, ix, iz + 1) - AT(s->p, ix, iz)) + cz1 * (AT(s->p, ix, iz + 2) - AT(s->p, ix, iz - 1));
+            s->vx[id] = s->damp2b[ix] * s->vx[id] + (s->kxb[ix] * s->bx[id]) * dpx;
+            s->vz[id] = s->damp1b[iz] * s->vz[id] + (s->kzb[iz] * s->bz[id]) * dpz;
+        }
+    }
+}
+#undef AT
+
+/* ------------------------------ driver ---------------------------------- */
+
+int orc_forward(const orc_params *prm, int precision,
+                const float *vp, const float *rho,
+                float sx, float sz, int nrec, const float *gx, const float *gz,
+                const double *wavelet, int nwav, int kt_stop,
+                float *seis, double *state_out) {
+    if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz || !seis))) return -1;
+    if (prm->nx < 1 || prm->nz < 1 || prm->nb < 2) return -1;
+    if (precision != ORC_F64 && precision != ORC_F32) return -1;
+    orc_derived d;
+    orc_derive(prm, &d);
+    if (d.dt_factor < 1 || d.fd_nt < 1) return -2;
+    const int nnx = d.nnx, nnz = d.nnz, nb = prm->nb;
+    const size_t N = (size_t)nnx * nnz;
+
+    /* CM:207-230 */
+    float *vel = (float *)calloc(N, sizeof(float));
+    float *den = (float *)calloc(N, sizeof(float));
+    float *bue = (float *)calloc(N, sizeof(float));
+    float *bx = (float *)calloc(N, sizeof(float));
+    float *bz = (float *)calloc(N, sizeof(float));
+    double *kappa = (double *)calloc(N, sizeof(double));
+    expand(vel, vp, nb, nnz, nnx, prm->nz, prm->nx);
+    expand(den, rho, nb, nnz, nnx, prm->nz, prm->nx);
+    stagger(vel, den, bue, bx, bz, kappa, nnz, nnx);
+
+    /* CM:233-234 (plus the one-past-the-end sample read at kt == nts, CM:136,
+     * taken as 0 here) */
+    int nw = wavelet ? nwav : d.nts;
+    double *w = (double *)calloc((size_t)(nw > 0 ? nw : 0) + 1, sizeof(double));
+    if (wavelet) memcpy(w, wavelet, (size_t)nw * sizeof(double));
+    else orc_ricker(prm, &d, w);
+
+    /* CM:254-259 */
+    float *damp2a = (float *)calloc(nnx, sizeof(float)), *damp2a1 = (float *)calloc(nnx, sizeof(float));
+    float *damp2b = (float *)calloc(nnx, sizeof(float)), *damp2b1 = (float *)calloc(nnx, sizeof(float));
+    float *damp1a = (float *)calloc(nnz, sizeof(float)), *damp1a1 = (float *)calloc(nnz, sizeof(float));
+    float *damp1b = (float *)calloc(nnz, sizeof(float)), *damp1b1 = (float *)calloc(nnz, sizeof(float));
+    const float fac = 0.05f;
+    sponge_a(fac, damp2a, damp2a1, nb, prm->nx);
+    sponge_b(fac, damp2b, damp2b1, nb, prm->nx);
+    sponge_a(fac, damp1a, damp1a1, nb, prm->nz);
+    sponge_b(fac, damp1b, damp1b1, nb, prm->nz);
+
+    /* CM:284-292, 329-338 */
+    int isrc = orc_cell(prm, sx, sz);
+    int *gcell = (int *)calloc((size_t)nrec + 1, sizeof(int));
+    for (int g = 0; g < nrec; g++) gcell[g] = orc_cell(prm, gx[g], gz[g]);
+    if (isrc < 0 || (size_t)isrc >= N) goto bad_pos;
+    for (int g = 0; g < nrec; g++)
+        if (gcell[g] < 0 || (size_t)gcell[g] >= N) goto bad_pos;
+
+    int nsteps = (kt_stop > 0 && kt_stop < d.fd_nt) ? kt_stop : d.fd_nt;
+    float *temp = (float *)calloc((size_t)nrec * d.real_nt + 1, sizeof(float));
+    const float dxdz = prm->dx * prm->dz;
+
+    if (precision == ORC_F64) {
+        double *kw1 = (double *)malloc(N * sizeof(double)), *kw2 = (double *)malloc(N * sizeof(double));
+        double *bw1 = (double *)malloc(N * sizeof(double)), *bw2 = (double *)malloc(N * sizeof(double));
+        /* CM:270-281 */
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz < nnz; iz++) {
+                size_t id = (size_t)iz + (size_t)ix * nnz;
+                kw2[id] = d.dtdx * kappa[id] * damp2a1[ix];
+                kw1[id] = d.dtdz * kappa[id] * damp1a1[iz];
+                bw2[id] = d.dtdx * bx[id] * damp2b1[ix];
+                bw1[id] = d.dtdz * bz[id] * damp1b1[iz];
+            }
+        f64_state s = {nnx, nnz, N, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
+                       kw1, kw2, bw1, bw2, damp1a, damp2a, damp1b, damp2b};
+        double **f[7] = {&s.p, &s.px, &s.pz, &s.vx, &s.vz, &s.d1, &s.d2};
+        for (int k = 0; k < 7; k++) *f[k] = (double *)calloc(N, sizeof(double));
+        for (int kt = 0; kt < nsteps; kt++) {
+            /* CM:136-140 */
+            double wk = kt < nw ? w[kt] : 0.0;
+            double add = prm->fd_dt * wk * kappa[isrc] / (dxdz);
+            f64_step(&s, isrc, add, kt <= d.nts);
+            /* CM:356-360 */
+            if ((kt + 1) % d.dt_factor == 0) {
+                int it = (kt + 1) / d.dt_factor - 1;
+                if (it < d.real_nt)
+                    for (int g = 0; g < nrec; g++) temp[(size_t)it * nrec + g] = (float)s.p[gcell[g]];
+            }
+        }
+        if (state_out) {
+            memcpy(state_out + 0 * N, s.px, N * sizeof(double));
+            memcpy(state_out + 1 * N, s.pz, N * sizeof(double));
+            memcpy(state_out + 2 * N, s.vx, N * sizeof(double));
+            memcpy(state_out + 3 * N, s.vz, N * sizeof(double));
+            memcpy(state_out + 4 * N, s.p, N * sizeof(double));
+        }
+        for (int k = 0; k < 7; k++) free(*f[k]);
+        free(kw1); free(kw2); free(bw1); free(bw2);
+    } else {
+        float *kf = (float *)malloc(N * sizeof(float));
+        for (size_t id = 0; id < N; id++) kf[id] = (float)kappa[id];
+        float *kxa = (float *)malloc(nnx * sizeof(float)), *kxb = (float *)malloc(nnx * sizeof(float));
+        float *kza = (float *)malloc(nnz * sizeof(float)), *kzb = (float *)malloc(nnz * sizeof(float));
+        for (int ix = 0; ix < nnx; ix++) { kxa[ix] = (float)(d.dtdx * damp2a1[ix]); kxb[ix] = (float)(d.dtdx * damp2b1[ix]); }
+        for (int iz = 0; iz < nnz; iz++) { kza[iz] = (float)(d.dtdz * damp1a1[iz]); kzb[iz] = (float)(d.dtdz * damp1b1[iz]); }
+        f32_state s = {nnx, nnz, N, NULL, NULL, NULL, NULL, NULL, kf, bx, bz,
+                       damp1a, damp2a, damp1b, damp2b, kxa, kza, kxb, kzb};
+        float **f[5] = {&s.p, &s.px, &s.pz, &s.vx, &s.vz};
+        for (int k = 0; k < 5; k++) *f[k] = (float *)calloc(N, sizeof(float));
+        for (int kt = 0; kt < nsteps; kt++) {
+            double wk = kt < nw ? w[kt] : 0.0;
+            float add = (float)(prm->fd_dt * wk * kappa[isrc] / (dxdz));
+            f32_step(&s, isrc, add, kt <= d.nts);
+            if ((kt + 1) % d.dt_factor == 0) {
+                int it = (kt + 1) / d.dt_factor - 1;
+                if (it < d.real_nt)
+                    for (int g = 0; g < nrec; g++) temp[(size_t)it * nrec + g] = s.p[gcell[g]];
+            }
+        }
+        if (state_out) {
+            float *src[5] = {s.px, s.pz, s.vx, s.vz, s.p};
+            for (int k = 0; k < 5; k++)
+                for (size_t id = 0; id < N; id++) state_out[k * N + id] = src[k][id];
+        }
+        for (int k = 0; k < 5; k++) free(*f[k]);
+        free(kf); free(kxa); free(kxb); free(kza); free(kzb);
+    }
+
+    /* CK:370-381: [real_nt][nrec] -> [nrec][real_nt] */
+    for (int t = 0; t < d.real_nt; t++)
+        for (int g = 0; g < nrec; g++) seis[(size_t)g * d.real_nt + t] = temp[(size_t)t * nrec + g];
+    free(temp);
+    free(vel); free(den); free(bue); free(bx); free(bz); free(kappa); free(w); free(gcell);
+    free(damp2a); free(damp2a1); free(damp2b); free(damp2b1);
+    free(damp1a); free(damp1a1); free(damp1b); free(damp1b1);
+    return 0;
+
+bad_pos:
+    free(vel); free(den); free(bue); free(bx); free(bz); free(kappa); free(w); free(gcell);
+    free(damp2a); free(damp2a1); free(damp2b); free(damp2b1);
+    free(damp1a); free(damp1a1); free(damp1b); free(damp1b1);
+    return -3;
+}

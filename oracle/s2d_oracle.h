@@ -1,0 +1,73 @@
+/*
+ * CPU restatement of SeisAcoMod2D's forward-modelling path (one shot).
+ *
+ * TEST INFRASTRUCTURE.  This library is the checker for the CUDA product
+ * path: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg
+ * load it.  The product library never links or calls it.
+ *
+ * Two arithmetic variants of the same scheme:
+ *   orc_forward(..., ORC_F64, ...)  the reference's own FP64 wavefields with
+ *                                   its float/double mix, operation order kept
+ *                                   (src/src_cpu/cpumodelling.cpp,
+ *                                    src/src_cpu/cpu_modelling_kernels.cpp);
+ *   orc_forward(..., ORC_F32, ...)  the same steps with FP32 wavefields and
+ *                                   FP32 per-cell coefficients, the arithmetic
+ *                                   the CUDA kernels use.
+ */
+#ifndef S2D_ORACLE_H
+#define S2D_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_F64 = 64, ORC_F32 = 32 };
+
+typedef struct {
+    int nx, nz;        /* physical grid, x-major [nx][nz] */
+    int nb;            /* sponge width in cells (reference: npml, cpumodelling.cpp:15) */
+    float dx, dz;      /* metres */
+    float rec_len;     /* "Time"      seconds */
+    float fd_dt;       /* "FD DT"     seconds */
+    float real_dt;     /* "DATA DT"   seconds */
+    float fm;          /* "Frequency" Hz */
+} orc_params;
+
+typedef struct {
+    int nnx, nnz;      /* padded grid */
+    int fd_nt;         /* FD steps            (cpumodelling.cpp:174) */
+    int real_nt;       /* recorded samples    (cpumodelling.cpp:175) */
+    int dt_factor;     /* FD steps per sample (cpumodelling.cpp:179) */
+    int nts;           /* wavelet length      (cpumodelling.cpp:183-188) */
+    double dtdx, dtdz; /* (double)(dt * (1/d))  (cpumodelling.cpp:177) */
+} orc_derived;
+
+/* Derived run constants exactly as the reference computes them. */
+void orc_derive(const orc_params *p, orc_derived *d);
+
+/* Ricker wavelet of length d->nts (cpu_modelling_kernels.cpp:33-62). */
+void orc_ricker(const orc_params *p, const orc_derived *d, double *w);
+
+/* Padded cell index of a position in metres (cpumodelling.cpp:284-292,
+ * cpu_modelling_kernels.cpp:15-22). */
+int orc_cell(const orc_params *p, float x, float z);
+
+/*
+ * One shot.  vp, rho: [nx][nz] float32.  Receivers at (gx[g], gz[g]) metres.
+ * wavelet: NULL for the reference Ricker, else nwav samples (entries at
+ * kt >= nwav count as 0).  kt_stop: number of FD steps to run (<= 0 means
+ * the full fd_nt).  seis: [nrec][real_nt] float32, zero-filled beyond the
+ * last recorded sample.  state_out (optional): px,pz,vx,vz,p after the last
+ * step, 5 arrays of nnx*nnz doubles, x-major.
+ * Returns 0 on success, negative on bad arguments.
+ */
+int orc_forward(const orc_params *p, int precision,
+                const float *vp, const float *rho,
+                float sx, float sz, int nrec, const float *gx, const float *gz,
+                const double *wavelet, int nwav, int kt_stop,
+                float *seis, double *state_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+"""Generate the golden seismograms in tests/golden/ from the reference itself.
+
+Runs the reference CPU binary (SeisAcoMod2D src/src_cpu, built unmodified by
+``make -C oracle ref`` and, for other sponge widths, ``make -C oracle ref
+NB=<nb>`` whose only change is the npml constant) on each case of
+``cases.py`` and stores, per case, ``<case>.npz`` with:
+
+  seis      float32 [nrec][real_nt]  the reference's output file
+  src       float32 (2,)             source (x, z) metres (from test_geometry.txt)
+  rec       float32 (nrec, 2)        receivers (x, z) metres, as the reference built them
+  params    json                     the run parameters
+  jobcard   text                     the job card the reference read
+  geomfile  text                     the shot or geometry file it read
+
+Needs the reference tree (to build the binary), so it runs in the development
+container; the committed .npz files are what the tests use everywhere.
+Usage: python tests/golden/make_golden.py [case ...]
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from cases import CASES, explicit_geometry, model  # noqa: E402
+from seis2d_b200 import formats as F  # noqa: E402
+
+
+def run_case(name: str, c: dict) -> dict:
+    nb = c["nb"]
+    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref" if nb == 32 else f"seis_ref_nb{nb}")
+    args = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"]
+    if nb != 32:
+        args.append(f"NB={nb}")
+    subprocess.run(args, check=True)
+    vp, rho = model(c["model"], c["nx"], c["nz"], c["dx"], c["dz"])
+    with tempfile.TemporaryDirectory() as wd:
+        F.write_model(os.path.join(wd, "vp.bin"), vp)
+        F.write_model(os.path.join(wd, "rho.bin"), rho)
+        kind, spec = c["geom"]
+        card = {
+            "Velocity": "vp.bin", "Density": "rho.bin", "NX": c["nx"], "NZ": c["nz"],
+            "DX": c["dx"], "DZ": c["dz"], "Time": c["T"], "FD DT": c["dt"], "DATA DT": c["ddt"],
+            "Frequency": c["f"], "Output Directory": "out", "Free surface": 0,
+            "Job type New or Restart": "New", "Order of FD Operator": 4,
+        }
+        if kind == "shot":
+            F.write_shotfile(os.path.join(wd, "geom.txt"), spec)
+            card.update({"Read source receiver flag": 1, "if choice=0, Geometry file": "NA",
+                         "if choice=1, Shot file": "geom.txt"})
+        else:
+            F.write_geometry(os.path.join(wd, "geom.txt"),
+                             explicit_geometry(spec, c["nx"], c["nz"], c["dx"], c["dz"]))
+            card.update({"Read source receiver flag": 0, "if choice=0, Geometry file": "geom.txt",
+                         "if choice=1, Shot file": "NA"})
+        F.write_jobcard(os.path.join(wd, "case.json"), card)
+        os.makedirs(os.path.join(wd, "out"))
+        r = subprocess.run([binary, "case.json"], cwd=wd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"{name}: reference exited {r.returncode}\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+        g = np.loadtxt(os.path.join(wd, "test_geometry.txt"), dtype=np.float64, ndmin=2)
+        src = np.array([g[0, 1], g[0, 0]], np.float32)
+        rec = np.stack([g[1:, 1], g[1:, 0]], axis=1).astype(np.float32)
+        seis = F.read_seismogram(os.path.join(wd, "out", "case_seismogram.bin"), rec.shape[0])
+        jobcard = open(os.path.join(wd, "case.json")).read()
+        geomfile = open(os.path.join(wd, "geom.txt")).read()
+    params = dict(c)
+    params.pop("geom")
+    params["geom_kind"] = kind
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(out, seis=seis, src=src, rec=rec, params=json.dumps(params),
+                        jobcard=jobcard, geomfile=geomfile)
+    return {"case": name, "nrec": int(rec.shape[0]), "nt": int(seis.shape[1]),
+            "max_abs": float(np.abs(seis).max()), "bytes": os.path.getsize(out)}
+
+
+def main(argv):
+    names = argv or list(CASES)
+    for n in names:
+        print(json.dumps(run_case(n, CASES[n])))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
