@@ -1,0 +1,394 @@
+"""Benchmark of the SeisAcoMod2D forward-modelling hot path on B200.
+
+Workload (default ``c2``): two-layer model on a 5000 x 5000 grid, dx = dz = 5 m,
+vp 2000/3500 m/s, rho 1800/2300 kg/m^3 with the interface at 2500 cells,
+60-cell sponge (5120 x 5120 padded), 20 Hz Ricker, dt = 0.5 ms, nt = 4000,
+64 shots per GPU evenly spaced along the surface (depth 2 cells), each recorded
+by 5000 surface receivers; all shots of a GPU advance together (batched).
+
+A bench step advances the whole batch by ``chunk`` FD steps (default 200) of
+that job, continuing from the previous step's wavefields, with source
+injection and receiver recording exactly as in the full run; the metric is a
+rate (padded-cell updates per second), so the full 4000-step job runs at the
+same rate.  Inputs (models, shot tables, wavefields) stay in HBM; the state
+of 64 shots (54 GB) is far larger than L2, so no L2 flush is needed.
+
+Printed: one JSON line with the metric, the end-to-end rate through the C ABI
+from pinned host buffers (``e2e``), the roofline of the step kernel, the
+reference CPU path timed on this host (``cpu_baseline``), plain (shot after
+shot) vs batched rates, and the SM clocks sampled during the timed region.
+
+``--impl reference`` times the reference's own CPU implementation
+(oracle/_ref, SeisAcoMod2D src/src_cpu built unmodified apart from the sponge
+width) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG = 44.0  # algorithmic bytes per padded-cell update: 4 state fields r+w (32) + 3 materials (12)
+
+WORKLOADS = {
+    "c2": dict(nx=5000, nz=5000, d=5.0, nb=60, vp=(2000.0, 3500.0), rho=(1800.0, 2300.0), iface=2500,
+               f=20.0, dt=0.0005, T=2.0, nshots=64, nrec=5000,
+               desc="two-layer 5000x5000 d=5m nb=60, 20 Hz, dt 0.5 ms, nt 4000, 64 shots x 5000 receivers"),
+    "c1": dict(nx=1000, nz=1000, d=10.0, nb=40, vp=(1500.0, 3000.0), rho=(1000.0, 2000.0), iface=500,
+               f=15.0, dt=0.001, T=2.0, nshots=1, nrec=1000,
+               desc="two-layer 1000x1000 d=10m nb=40, 15 Hz, dt 1 ms, nt 2000, 1 shot x 1000 receivers"),
+}
+
+
+def build_workload(w, rank=0, world=1):
+    nx, nz = w["nx"], w["nz"]
+    vp = np.empty((nx, nz), np.float32)
+    rho = np.empty((nx, nz), np.float32)
+    vp[:, : w["iface"]] = w["vp"][0]
+    vp[:, w["iface"]:] = w["vp"][1]
+    rho[:, : w["iface"]] = w["rho"][0]
+    rho[:, w["iface"]:] = w["rho"][1]
+    d = w["d"]
+    ntot = w["nshots"] * world
+    # shot k of the global list at ix = round((k + 0.5) * nx / ntot), iz = 2
+    ks = range(rank * w["nshots"], (rank + 1) * w["nshots"])
+    src = [(float(int(round((k + 0.5) * nx / ntot)) * d), 2 * d) for k in ks]
+    if w["nshots"] == 1 and world == 1:
+        src = [(float(nx // 2) * d, 2 * d)]
+    rec = np.stack([np.arange(w["nrec"], dtype=np.float32) * d, np.full(w["nrec"], 2 * d, np.float32)], 1)
+    return vp, rho, src, rec
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(workload):
+    """DRAM bytes per step launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        t = json.load(open(p)).get(workload)
+        if t:
+            return float(t["dram_bytes_per_launch"])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref, the reference's own src/src_cpu)
+
+def ref_cpu_rate(w, nsteps_pair=(4, 84), threads=None, tmpdir=None):
+    """Gcell/s of the reference CPU time loop on one shot of workload ``w``:
+    two runs of nsteps_pair FD steps, rate from the difference (set-up cancels)."""
+    from seis2d_b200 import formats as F
+    nb = w["nb"]
+    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref" if nb == 32 else f"seis_ref_nb{nb}")
+    if not os.path.exists(binary):
+        return None, f"{binary} not built"
+    vp, rho, src, rec = build_workload(dict(w, nshots=1), 0, 1)
+    times = []
+    env = dict(os.environ)
+    threads = threads or os.cpu_count()
+    env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory(dir=tmpdir) as wd:
+        F.write_model(os.path.join(wd, "vp.bin"), vp)
+        F.write_model(os.path.join(wd, "rho.bin"), rho)
+        F.write_shotfile(os.path.join(wd, "shots.txt"),
+                         [(src[0][0], src[0][1], w["nrec"], 0, w["d"], 1)])
+        os.makedirs(os.path.join(wd, "out"))
+        for n in nsteps_pair:
+            T = n * w["dt"]
+            F.write_jobcard(os.path.join(wd, "job.json"), {
+                "Velocity": "vp.bin", "Density": "rho.bin", "NX": w["nx"], "NZ": w["nz"], "DX": w["d"],
+                "DZ": w["d"], "Time": T, "FD DT": w["dt"], "DATA DT": w["dt"], "Frequency": w["f"],
+                "Read source receiver flag": 1, "if choice=0, Geometry file": "NA",
+                "if choice=1, Shot file": "shots.txt", "Output Directory": "out", "Free surface": 0,
+                "Job type New or Restart": "New", "Order of FD Operator": 4})
+            r = subprocess.run([binary, "--no-stability", "--time", "job.json"], cwd=wd, env=env,
+                               capture_output=True, text=True)
+            if r.returncode != 0:
+                return None, f"reference exited {r.returncode}"
+            t = [float(l.split()[1]) for l in r.stdout.splitlines() if l.startswith("ORACLE_TIME")]
+            from seis2d_b200 import Wave, derive_steps
+            nsteps = derive_steps(Wave(T, w["dt"], w["dt"], w["f"]))["fd_nt"]
+            times.append((t[0], nsteps))
+    (t0, n0), (t1, n1) = times
+    cells = (w["nx"] + 2 * nb) * (w["nz"] + 2 * nb)
+    rate = cells * (n1 - n0) / max(t1 - t0, 1e-9) / 1e9
+    sample = (f"1 shot of the workload, {n0} and {n1} FD steps ({t0:.2f} s, {t1:.2f} s wall incl. set-up); "
+              f"rate from the difference")
+    return {"value": rate, "unit": "Gcell/s", "cores": threads, "kind": "reference", "sample": sample}, None
+
+
+def run_reference_arm(args, w, world, rank):
+    if rank != 0:
+        return 0
+    vals = []
+    info = None
+    # Each step is one bounded sample (two short runs of one shot); warm-up
+    # samples are shorter still.
+    for _ in range(min(args.warmup, 1)):
+        ref_cpu_rate(w, (2, 4))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        info, err = ref_cpu_rate(w)
+        if info is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return 0
+        vals.append(info["value"])
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    info["value"] = v
+    line = {
+        "impl": "reference", "metric": "padded-grid cell-updates per second, batched forward modelling",
+        "value": v, "unit": "Gcell/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["desc"], "sample": info["sample"]},
+        "cpu_baseline": info, "e2e": {"value": v, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--chunk", type=int, default=200, help="FD steps per bench step")
+    ap.add_argument("--shots", type=int, default=0, help="override shots per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    w = dict(WORKLOADS[args.workload])
+    if args.shots:
+        w["nshots"] = args.shots
+    if args.impl == "reference":
+        return run_reference_arm(args, w, world, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from seis2d_b200 import Context, Shot, Wave, derive_steps
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    wave = Wave(w["T"], w["dt"], w["dt"], w["f"])
+    steps = derive_steps(wave)
+    fd_nt = steps["fd_nt"]
+    chunk = max(1, min(args.chunk, fd_nt // max(1, args.warmup + args.steps)))
+    vp, rho, src, rec = build_workload(w, rank, world)
+    nshots = len(src)
+    cells_shot = (w["nx"] + 2 * w["nb"]) * (w["nz"] + 2 * w["nb"])
+    cells_step = cells_shot * nshots  # per FD step, this rank
+
+    ctx = Context(local)
+    m = ctx.model(vp, rho, w["d"], w["d"], w["nb"])
+    shots = [Shot(m, s, rec) for s in src]
+    nrec_tot = nshots * rec.shape[0]
+    seis_dev = torch.zeros(nrec_tot * steps["real_nt"], dtype=torch.float32, device="cuda")
+
+    # ---- batched, device-resident (value) ----
+    kt = 0
+    launches = 0
+    for _ in range(args.warmup):
+        ctx.forward(shots, wave, kt_begin=kt, kt_count=chunk, out=seis_dev)
+        kt += chunk
+    barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        ctx.forward(shots, wave, kt_begin=kt, kt_count=chunk, out=seis_dev, sync=False)
+        st = ctx.last_stats
+        launches += st.kernel_launches
+        kt += chunk
+    ev1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t_max = torch.tensor([ms], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms = float(t_max.item())
+    total_cells = cells_step * chunk * args.steps * world
+    value = total_cells / (ms * 1e-3) / 1e9
+    ms_per_step = ms / args.steps
+
+    # per-launch roofline of the step kernel (one launch per FD step), timed
+    # by the library's CUDA events on the stream it launches on
+    kt_r = kt
+    n_r = min(chunk, fd_nt - kt_r)
+    roof = None
+    if n_r > 0:
+        ctx.forward(shots, wave, kt_begin=kt_r, kt_count=n_r, out=seis_dev)
+        st = ctx.last_stats
+        per_launch_s = st.loop_ms * 1e-3 / n_r
+        peak, peak_kind = measured_peak()
+        achieved = B_ALG * cells_step / per_launch_s / 1e9
+        tr = traffic_per_launch(args.workload)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": tr, "peak_source": peak_kind, "bytes_per_launch": B_ALG * cells_step,
+                "launch_ms": per_launch_s * 1e3}
+
+    # ---- plain: the same shots one after another ----
+    plain = None
+    if not args.no_plain and nshots > 1:
+        pch = max(1, chunk // 4)
+        ctx.forward(shots, wave, kt_begin=0, kt_count=pch, out=seis_dev, plain=True)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.forward(shots, wave, kt_begin=pch, kt_count=pch, out=seis_dev, plain=True, sync=False)
+        e1.record()
+        barrier()
+        pms = e0.elapsed_time(e1)
+        prate = cells_step * pch / (pms * 1e-3) / 1e9
+        plain = {"value": prate * world, "unit": "Gcell/s", "speedup_batched_vs_plain": value / (prate * world),
+                 "sample": f"{nshots} shots x {pch} FD steps, shot after shot"}
+
+    # ---- end to end through the C ABI from pinned host memory ----
+    e2e = None
+    if not args.no_e2e:
+        vp_h = torch.from_numpy(vp).pin_memory()
+        rho_h = torch.from_numpy(rho).pin_memory()
+        out_h = torch.zeros(nrec_tot * steps["real_nt"], dtype=torch.float32).pin_memory()
+        short = Wave(chunk * w["dt"], w["dt"], w["dt"], w["f"])
+        real_short = derive_steps(short)["real_nt"]
+        out_h = out_h[: nrec_tot * real_short]
+        n_e2e = max(1, min(args.steps, 3))
+
+        def one():
+            mm = ctx.model(vp_h.numpy(), rho_h.numpy(), w["d"], w["d"], w["nb"])
+            ctx.forward([Shot(mm, s, rec) for s in src], short, out=out_h.numpy())
+            mm.release()
+
+        one()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            one()
+        barrier()
+        et = torch.tensor([time.perf_counter() - t0], device="cuda")
+        if dist is not None:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        ecells = cells_step * derive_steps(short)["fd_nt"] * n_e2e * world
+        e2e = {"value": ecells / float(et.item()) / 1e9, "unit": "Gcell/s",
+               "h2d_bytes_per_step": int(vp.nbytes + rho.nbytes),
+               "d2h_bytes_per_step": int(nrec_tot * real_short * 4),
+               "sample": f"{n_e2e} calls: model upload + {nshots} shots x {derive_steps(short)['fd_nt']} FD steps "
+                         f"+ seismogram download, pinned host buffers"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu, err = ref_cpu_rate(w)
+        if cpu is None:
+            cpu = {"unavailable": err}
+
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": "padded-grid cell-updates per second, batched forward modelling",
+            "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["desc"], "shots_per_gpu": nshots, "fd_steps_per_bench_step": chunk,
+                       "padded_grid": [w["nx"] + 2 * w["nb"], w["nz"] + 2 * w["nb"]],
+                       "l2": "inputs larger than L2 (wavefield state %.1f GB per GPU)" % (cells_step * 32 / 1e9),
+                       "parallelism": f"shots sharded over {world} GPU(s), no collective"},
+            "shots_per_s": value * 1e9 / (cells_shot * fd_nt),
+            "plain": plain, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

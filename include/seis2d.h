@@ -1,0 +1,178 @@
+/*
+ * seis2d.h -- C ABI of libseis2d, the B200 (sm_100a) implementation of
+ * SeisAcoMod2D's forward-modelling hot path: the per-shot 2-D acoustic
+ * 4th-order staggered-grid time loop with split-field sponge, Ricker source
+ * injection and receiver sampling.
+ *
+ * Reference seam replaced:
+ *   void modelling_module(int my_nsrc, geo2d_t *mygeo2d_sp);
+ *   (src/src_cpu/modelling.h:106, defined by every backend:
+ *    src/src_cpu/cpumodelling.cpp:158, src/src_gpu/gpumodelling.cu:238)
+ * That function takes its inputs from globals (mod_sp, wave_sp, job_sp;
+ * src/src_cpu/modelling.h:13-61) and writes the seismogram files itself.
+ * Here the same inputs arrive as arguments, the seismograms are returned in
+ * caller-owned buffers, and file I/O lives in the host driver entry points at
+ * the end of this header (s2d_run_jobcard), which keep the reference's
+ * job-card, geometry, model and seismogram formats.
+ *
+ * Conventions
+ *   - Plain C types only; every entry point returns an int status
+ *     (S2D_OK = 0, negative = error class) and never aborts the process
+ *     (the reference calls MPI::COMM_WORLD.Abort with negative codes).
+ *   - The caller owns every buffer it passes.  The library owns the device
+ *     memory of a context and frees it in s2d_destroy.
+ *   - A context is bound to one CUDA device.  Calls on one context are not
+ *     thread-safe; distinct contexts may be used from distinct threads.
+ *   - Grids are x-major [nx][nz] with z contiguous, as the reference's model
+ *     files and geo2d_t coordinates (metres).
+ */
+#ifndef SEIS2D_H
+#define SEIS2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define S2D_API __attribute__((visibility("default")))
+#else
+#define S2D_API
+#endif
+
+#define S2D_ABI_VERSION 1
+
+/* status codes */
+#define S2D_OK 0
+#define S2D_ERR_ARG -1      /* bad argument (null pointer, size, id)        */
+#define S2D_ERR_CUDA -2     /* CUDA runtime error (text in s2d_last_error)  */
+#define S2D_ERR_NOMEM -3    /* device or host allocation failed             */
+#define S2D_ERR_GEOM -4     /* source/receiver outside the grid             */
+#define S2D_ERR_STATE -5    /* call out of order (e.g. bad continuation)    */
+#define S2D_ERR_IO -6       /* file missing, unreadable or of wrong size     */
+#define S2D_ERR_JOBCARD -7  /* job card key missing or malformed            */
+#define S2D_ERR_STABILITY -8 /* stability / dispersion criterion violated    */
+#define S2D_ERR_TIMEOUT -9  /* a bounded device-side wait gave up           */
+#define S2D_ERR_NODEV -10   /* no usable CUDA device                         */
+
+/* flags for s2d_forward */
+#define S2D_SEIS_DEVICE 0x1u   /* seis_out is a device pointer                 */
+#define S2D_PLAIN 0x2u         /* shots one after another (reference order)    */
+#define S2D_NO_GRAPH 0x4u      /* launch the time loop step by step            */
+#define S2D_SYNC 0x8u          /* return only when device work has finished    */
+
+/* flags for s2d_model_create */
+#define S2D_MODEL_DEVICE 0x1u  /* vp and rho are device pointers               */
+
+/* Source/receiver position in metres; layout of crd2d_t
+ * (src/src_cpu/modelling.h:35-38). */
+typedef struct {
+    float x, z;
+} s2d_coord;
+
+/* Time-stepping parameters; layout of wave_t (src/src_cpu/modelling.h:27-31):
+ * record length "Time", "FD DT", "DATA DT" in seconds, "Frequency" in Hz. */
+typedef struct {
+    float rec_len, fd_dt, real_dt, dom_freq;
+} s2d_wave;
+
+/* One shot: the model it runs on, its source and its receivers.  Replaces one
+ * entry of geo2d_t (src/src_cpu/modelling.h:40-45).  rec points to nrec host
+ * coordinates. */
+typedef struct {
+    int model_id;
+    s2d_coord src;
+    int nrec;
+    const s2d_coord *rec;
+} s2d_shot;
+
+/* Constants the reference derives from s2d_wave
+ * (src/src_cpu/cpumodelling.cpp:168-188). */
+typedef struct {
+    int fd_nt;     /* FD steps            ceil(Time / FD DT)                 */
+    int real_nt;   /* samples per trace   ceil(Time / DATA DT)               */
+    int dt_factor; /* FD steps per sample (int)(DATA DT / FD DT)             */
+    int nts;       /* Ricker length       (int)(5*sqrt(6)/(pi f)/FD DT) + 1  */
+} s2d_steps;
+
+/* Per-call performance record (device time of the time loop). */
+typedef struct {
+    double loop_ms;          /* CUDA-event time of the FD time loop           */
+    double cell_updates;     /* padded cells x steps advanced                 */
+    double gcells_per_s;     /* cell_updates / loop_ms                        */
+    int kernel_launches;     /* launches of the library's own kernels         */
+    int graph_used;          /* 1 if the loop ran as a CUDA graph             */
+} s2d_stats;
+
+/* ---- library / context ------------------------------------------------ */
+
+/* ABI version of the loaded library (S2D_ABI_VERSION). */
+S2D_API int s2d_abi_version(void);
+
+/* Create a context on CUDA device `device`.  No counterpart in the reference
+ * (its backends use globals and cudaSetDevice(0), src/src_gpu/gpumodelling.cu:285). */
+S2D_API int s2d_create(void **ctx, int device);
+
+/* Free every device buffer and graph of the context. */
+S2D_API void s2d_destroy(void *ctx);
+
+/* Text of the last error on this context (never NULL). */
+S2D_API const char *s2d_last_error(const void *ctx);
+
+/* Derived step counts for a wave description, host-only, no device needed
+ * (src/src_cpu/cpumodelling.cpp:174-188). */
+S2D_API int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out);
+
+/* ---- models -------------------------------------------------------------- */
+
+/*
+ * Upload a model: nx*nz vp (m/s) and rho (kg/m^3), x-major, grid spacing
+ * dx, dz (m) and sponge width nb cells on each side (the reference fixes
+ * nb = 32, src/src_cpu/cpumodelling.cpp:15).  The library expands it into the
+ * sponge by edge replication (cpumodelling.cpp:39-60) and forms
+ * kappa = vp^2 rho and the staggered buoyancies (cpu_modelling_kernels.cpp:
+ * 64-121) on the device.  Returns a model id in *model_id.
+ */
+S2D_API int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb,
+                     const float *vp, const float *rho, unsigned flags, int *model_id);
+
+/* Release a model's device memory. */
+S2D_API int s2d_model_destroy(void *ctx, int model_id);
+
+/* ---- forward modelling ---------------------------------------------------- */
+
+/*
+ * Run the FD time loop for `nshots` shots (the loop of
+ * src/src_cpu/cpumodelling.cpp:326-380 with FDOperator_4 at :115-156).
+ *
+ *   wave        time stepping; every shot uses the same one
+ *   wavelet     NULL for the reference Ricker (cpu_modelling_kernels.cpp:33-62),
+ *               else nwavelet source samples, one per FD step (missing
+ *               samples count as 0)
+ *   kt_begin    0 starts all shots from rest; > 0 continues the previous
+ *               call's shots from that FD step (must equal where it stopped)
+ *   kt_count    FD steps to run in this call; <= 0 runs to the end (fd_nt)
+ *   seis_out    nshots consecutive blocks, block s is [nrec_s][real_nt]
+ *               float32 (sample fastest) -- the reference's output file
+ *               layout (cpumodelling.cpp:367-374).  Samples recorded in this
+ *               call's step range are written; others are left as they are.
+ *   flags       S2D_SEIS_DEVICE, S2D_PLAIN, S2D_NO_GRAPH, S2D_SYNC
+ *   stats       optional, filled with the device time of the loop
+ *
+ * Without S2D_PLAIN all shots advance together, one launch per FD step
+ * covering every shot (models of different sizes included), captured as a
+ * CUDA graph.  With S2D_PLAIN each shot runs its whole loop before the next
+ * starts, as the reference does.  Each shot starts from a zero wavefield (the
+ * reference zeroes only the first nnz cells between shots of one rank,
+ * cpumodelling.cpp:343-348; its first shot per rank is the behaviour kept).
+ */
+S2D_API int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wave,
+                const double *wavelet, int nwavelet, int kt_begin, int kt_count,
+                float *seis_out, unsigned flags, s2d_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEIS2D_H */

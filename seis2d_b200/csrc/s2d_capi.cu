@@ -1,0 +1,650 @@
+// C ABI of libseis2d: contexts, models and the forward time loop.
+//
+// Replaces modelling_module() (src/src_cpu/modelling.h:106) for one device:
+// the set-up of cpumodelling.cpp:168-292 is done once per model / run, and the
+// shot loop of cpumodelling.cpp:326-380 becomes either one batched launch per
+// FD step covering all shots (default) or the reference's shot-after-shot
+// order (S2D_PLAIN).  The per-step launches are captured as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/seis2d.h"
+#include "s2d_internal.h"
+#include "s2d_setup.h"
+
+using namespace s2d;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        reset();
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
+        return e;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct Model {
+    int nx = 0, nz = 0, nb = 0, nnx = 0, nnz = 0, ld = 0, nxa = 0;
+    float dx = 0, dz = 0;
+    size_t field_elems = 0;  // nxa * ld
+    DevBuf vp, rho;          // raw [nx][nz] copies (source amplitude needs vp, rho at the source)
+    DevBuf kappa, bx, bz;    // padded layout
+    std::vector<float> damp2a, damp2a1, damp2b, damp2b1, damp1a, damp1a1, damp1b, damp1b1;
+    // coefficient tables for one fd_dt, rebuilt when fd_dt changes
+    float coef_dt = -1.0f;
+    DevBuf xcoef, zcoef;
+};
+
+struct ShotHost {
+    int model_id;
+    int src_x, src_z;
+    int nrec;
+    size_t seis_off;  // element offset of the shot's [nrec][real_nt] block
+};
+
+struct Batch {
+    int nshots = 0;
+    bool plain = false;
+    RunSteps steps{};
+    int kt_next = 0;
+    std::vector<ShotHost> shots;
+    std::vector<ShotDev> shot_dev;   // host mirror
+    std::vector<GroupDev> groups;    // batched mode
+    std::vector<std::unique_ptr<DevBuf>> state;   // 8 per shot
+    std::vector<std::unique_ptr<DevBuf>> aux;     // amp tables, receiver tables
+    DevBuf shots_d, groups_d, args_d;
+    DevBuf seis_int;                 // internal seismogram buffer (host output)
+    float *seis_d = nullptr;         // where the kernels record
+    size_t seis_elems = 0;
+    int grid = 0, block = 128;
+    std::map<int, cudaGraphExec_t> graphs;  // by step count
+    std::vector<int> plain_group_tasks;
+    ~Batch() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    }
+};
+
+// Device buffers of finished batches, kept for reuse by the next batch of
+// the same sizes (state fields are the large allocations: a repeated run
+// then needs no cudaMalloc).  Flushed when an allocation fails.
+struct Pool {
+    std::multimap<size_t, std::unique_ptr<DevBuf>> free;
+    std::unique_ptr<DevBuf> take(size_t bytes, cudaError_t *err) {
+        auto it = free.find(bytes);
+        if (it != free.end()) {
+            auto b = std::move(it->second);
+            free.erase(it);
+            *err = cudaSuccess;
+            return b;
+        }
+        auto b = std::make_unique<DevBuf>();
+        *err = b->alloc(bytes);
+        if (*err == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            free.clear();
+            *err = b->alloc(bytes);
+        }
+        return b;
+    }
+    void give(std::unique_ptr<DevBuf> b) {
+        if (b && b->p) free.emplace(b->bytes, std::move(b));
+    }
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err = "no error";
+    std::map<int, std::unique_ptr<Model>> models;
+    int next_model = 1;
+    std::unique_ptr<Batch> batch;
+    Pool pool;
+    // Return the current batch's state buffers to the pool and drop it.
+    void drop_batch() {
+        if (!batch) return;
+        for (auto &b : batch->state) pool.give(std::move(b));
+        batch.reset();
+    }
+};
+
+int fail(Ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? S2D_ERR_NOMEM : S2D_ERR_CUDA,    \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+// Columns per x-segment for a group: long segments amortise the 3-column
+// warm-up of the streaming window; enough tasks must exist to fill the GPU.
+int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps) {
+    static const int cand[] = {1024, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16};
+    for (int L : cand) {
+        long nsegs = (nnx + L - 1) / L;
+        if (tasks_per_seg * nsegs >= 4 * resident_warps) return std::min(L, nnx);
+    }
+    return 16;
+}
+
+int build_coef(Ctx *c, Model &m, float fd_dt) {
+    if (m.coef_dt == fd_dt && m.xcoef.p) return S2D_OK;
+    const float inv_dx = 1.0f / m.dx, inv_dz = 1.0f / m.dz;
+    const double dtdx = (double)(fd_dt * inv_dx), dtdz = (double)(fd_dt * inv_dz);
+    std::vector<float4> xc(m.nxa), zc(m.ld);
+    for (auto &v : xc) v = make_float4(0, 0, 0, 0);
+    for (auto &v : zc) v = make_float4(0, 0, 0, 0);
+    // kappaw2 = dtdx*kappa*damp2a1, buw2 = dtdx*bu2*damp2b1 (cpumodelling.cpp:270-281):
+    // the per-column factors dtdx*damp?1 are folded here, kappa / b per cell in the kernel.
+    for (int x = 0; x < m.nnx; ++x)
+        xc[x + S2D_GX] = make_float4(m.damp2a[x], (float)(dtdx * m.damp2a1[x]), m.damp2b[x], (float)(dtdx * m.damp2b1[x]));
+    for (int z = 0; z < m.nnz; ++z)
+        zc[z + S2D_GZ] = make_float4(m.damp1a[z], (float)(dtdz * m.damp1a1[z]), m.damp1b[z], (float)(dtdz * m.damp1b1[z]));
+    if (!m.xcoef.p) CK(m.xcoef.alloc(sizeof(float4) * m.nxa));
+    if (!m.zcoef.p) CK(m.zcoef.alloc(sizeof(float4) * m.ld));
+    CK(cudaMemcpyAsync(m.xcoef.p, xc.data(), sizeof(float4) * m.nxa, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(m.zcoef.p, zc.data(), sizeof(float4) * m.ld, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    m.coef_dt = fd_dt;
+    return S2D_OK;
+}
+
+// One pass over `nsteps` FD steps starting at kt_begin, for the launch
+// arguments `args` (a whole batch, or one shot of a plain run).
+int run_loop(Ctx *c, Batch &b, StepArgs args, int kt_begin, int nsteps, bool use_graph, int *launches,
+             bool *graph_used) {
+    if (nsteps <= 0) return S2D_OK;
+    args.kt_base = kt_begin;
+    StepArgs *args_d = b.args_d.as<StepArgs>();
+    int e = launch_set_args(args, args_d, c->stream);
+    if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+    *launches += 1;
+    if (!use_graph) {
+        for (int k = 0; k < nsteps; ++k) {
+            e = launch_step(args_d, k, b.grid, b.block, c->stream);
+            if (e) return fail(c, S2D_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)e));
+        }
+        *launches += nsteps;
+        return S2D_OK;
+    }
+    auto it = b.graphs.find(nsteps);
+    if (it == b.graphs.end()) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < nsteps; ++k) {
+            e = launch_step(args_d, k, b.grid, b.block, c->stream);
+            if (e) {
+                cudaStreamEndCapture(c->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                return fail(c, S2D_ERR_CUDA, "step capture: %s", cudaGetErrorString((cudaError_t)e));
+            }
+        }
+        CK(cudaStreamEndCapture(c->stream, &g));
+        cudaGraphExec_t ge;
+        cudaError_t ce = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        CK(ce);
+        it = b.graphs.emplace(nsteps, ge).first;
+    }
+    CK(cudaGraphLaunch(it->second, c->stream));
+    *launches += nsteps;
+    *graph_used = true;
+    return S2D_OK;
+}
+
+// Build the device tables of a new batch (kt_begin == 0).
+int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave, const double *wavelet,
+                int nwavelet, float *seis_user, unsigned flags) {
+    c->drop_batch();
+    auto bp = std::make_unique<Batch>();
+    Batch &b = *bp;
+    b.nshots = nshots;
+    b.plain = (flags & S2D_PLAIN) != 0;
+    // every shot must reference an existing model; all share wave
+    for (int s = 0; s < nshots; ++s) {
+        auto it = c->models.find(shots[s].model_id);
+        if (it == c->models.end()) return fail(c, S2D_ERR_ARG, "shot %d: unknown model id %d", s, shots[s].model_id);
+        if (shots[s].nrec < 0 || (shots[s].nrec > 0 && !shots[s].rec))
+            return fail(c, S2D_ERR_ARG, "shot %d: bad receiver list", s);
+    }
+    const Model &m0 = *c->models[shots[0].model_id];
+    b.steps = derive_steps(wave, m0.dx, m0.dz);
+    const RunSteps &rs = b.steps;
+    if (rs.fd_nt < 1 || rs.real_nt < 1 || rs.dt_factor < 1)
+        return fail(c, S2D_ERR_ARG, "bad time stepping: fd_nt=%d real_nt=%d dt_factor=%d", rs.fd_nt, rs.real_nt,
+                    rs.dt_factor);
+    // source wavelet: the reference Ricker (length nts, injected while kt <= nts,
+    // the sample at kt == nts being 0) or the caller's samples
+    std::vector<double> w;
+    int inject_last;
+    if (wavelet) {
+        if (nwavelet < 0) return fail(c, S2D_ERR_ARG, "negative wavelet length");
+        w.assign(wavelet, wavelet + nwavelet);
+        inject_last = nwavelet - 1;
+    } else {
+        w = ricker(wave, rs.nts);
+        inject_last = rs.nts;
+    }
+    size_t seis_total = 0;
+    b.shots.resize(nshots);
+    for (int s = 0; s < nshots; ++s) {
+        Model &m = *c->models[shots[s].model_id];
+        int e = build_coef(c, m, wave.fd_dt);
+        if (e) return e;
+        ShotHost &h = b.shots[s];
+        h.model_id = shots[s].model_id;
+        h.nrec = shots[s].nrec;
+        cell_of(shots[s].src.x, shots[s].src.z, m.dx, m.dz, m.nb, h.src_x, h.src_z);
+        if (h.src_x < 0 || h.src_x >= m.nnx || h.src_z < 0 || h.src_z >= m.nnz)
+            return fail(c, S2D_ERR_GEOM, "shot %d: source (%g, %g) m is outside the grid", s, shots[s].src.x,
+                        shots[s].src.z);
+        h.seis_off = seis_total;
+        seis_total += (size_t)h.nrec * rs.real_nt;
+    }
+    b.seis_elems = seis_total;
+    if (flags & S2D_SEIS_DEVICE) {
+        b.seis_d = seis_user;
+    } else {
+        CK(b.seis_int.alloc(std::max<size_t>(seis_total, 1) * sizeof(float)));
+        b.seis_d = b.seis_int.as<float>();
+    }
+    if (seis_total) CK(cudaMemsetAsync(b.seis_d, 0, seis_total * sizeof(float), c->stream));
+
+    b.shot_dev.resize(nshots);
+    for (int s = 0; s < nshots; ++s) {
+        Model &m = *c->models[shots[s].model_id];
+        ShotHost &h = b.shots[s];
+        ShotDev &d = b.shot_dev[s];
+        std::memset(&d, 0, sizeof d);
+        const size_t fb = m.field_elems * sizeof(float);
+        for (int par = 0; par < 2; ++par)
+            for (int f = 0; f < 4; ++f) {
+                cudaError_t ae;
+                b.state.push_back(c->pool.take(fb, &ae));
+                CK(ae);
+                CK(cudaMemsetAsync(b.state.back()->p, 0, fb, c->stream));
+                d.st[par][f] = b.state.back()->as<float>();
+            }
+        d.kappa = m.kappa.as<float>();
+        d.bx = m.bx.as<float>();
+        d.bz = m.bz.as<float>();
+        d.xcoef = m.xcoef.as<float4>();
+        d.zcoef = m.zcoef.as<float4>();
+        d.nnx = m.nnx;
+        d.nnz = m.nnz;
+        d.ld = m.ld;
+        d.src_x = h.src_x;
+        d.src_z = h.src_z;
+        d.real_nt = rs.real_nt;
+        d.seis = b.seis_d + h.seis_off;
+        // source amplitude per step: fd_dt * w[kt] * kappa[src] / (dx*dz)
+        // (cpumodelling.cpp:136-140), kappa = vp^2 rho in double at the source
+        const int mx = std::min(std::max(h.src_x - m.nb, 0), m.nx - 1);
+        const int mz = std::min(std::max(h.src_z - m.nb, 0), m.nz - 1);
+        float vr[2];
+        CK(cudaMemcpy(&vr[0], m.vp.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&vr[1], m.rho.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
+        const double ksrc = ((double)vr[0] * (double)vr[0]) * (double)vr[1];
+        const float dxdz = m.dx * m.dz;
+        std::vector<float> amp(rs.fd_nt, 0.0f);
+        for (int kt = 0; kt < rs.fd_nt && kt <= inject_last; ++kt) {
+            const double wk = kt < (int)w.size() ? w[kt] : 0.0;
+            amp[kt] = (float)(wave.fd_dt * wk * ksrc / dxdz);
+        }
+        // receivers grouped by column
+        std::vector<int> rx(h.nrec), rz(h.nrec);
+        for (int g = 0; g < h.nrec; ++g) {
+            cell_of(shots[s].rec[g].x, shots[s].rec[g].z, m.dx, m.dz, m.nb, rx[g], rz[g]);
+            if (rx[g] < 0 || rx[g] >= m.nnx || rz[g] < 0 || rz[g] >= m.nnz)
+                return fail(c, S2D_ERR_GEOM, "shot %d receiver %d: (%g, %g) m is outside the grid", s, g,
+                            shots[s].rec[g].x, shots[s].rec[g].z);
+        }
+        std::vector<int> ptr(m.nnx + 1, 0), ez(h.nrec), eid(h.nrec);
+        for (int g = 0; g < h.nrec; ++g) ptr[rx[g] + 1]++;
+        for (int x = 0; x < m.nnx; ++x) ptr[x + 1] += ptr[x];
+        std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+        for (int g = 0; g < h.nrec; ++g) {
+            const int k = fill[rx[g]]++;
+            ez[k] = rz[g];
+            eid[k] = g;
+        }
+        b.aux.emplace_back(new DevBuf());
+        DevBuf &ab = *b.aux.back();
+        const size_t n_amp = (size_t)rs.fd_nt, n_ptr = (size_t)m.nnx + 1, n_rec = (size_t)std::max(h.nrec, 1);
+        const size_t bytes = sizeof(float) * n_amp + sizeof(int) * (n_ptr + 2 * n_rec) + 64;
+        CK(ab.alloc(bytes));
+        char *base = ab.as<char>();
+        float *amp_d = reinterpret_cast<float *>(base);
+        int *ptr_d = reinterpret_cast<int *>(base + sizeof(float) * n_amp);
+        int *ez_d = ptr_d + n_ptr;
+        int *eid_d = ez_d + n_rec;
+        CK(cudaMemcpy(amp_d, amp.data(), sizeof(float) * n_amp, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ptr_d, ptr.data(), sizeof(int) * n_ptr, cudaMemcpyHostToDevice));
+        if (h.nrec) {
+            CK(cudaMemcpy(ez_d, ez.data(), sizeof(int) * h.nrec, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(eid_d, eid.data(), sizeof(int) * h.nrec, cudaMemcpyHostToDevice));
+        }
+        d.amp = amp_d;
+        d.rec_ptr = ptr_d;
+        d.rec_z = ez_d;
+        d.rec_id = eid_d;
+    }
+    CK(b.shots_d.alloc(sizeof(ShotDev) * nshots));
+    CK(cudaMemcpy(b.shots_d.p, b.shot_dev.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
+    CK(b.args_d.alloc(sizeof(StepArgs)));
+
+    // launch shape: 4 warps per block, grid = resident blocks (grid-stride over tasks)
+    int bps = 0;
+    if (step_kernel_occupancy(b.block, &bps) || bps < 1) bps = 1;
+    const long resident_warps = (long)c->sm_count * bps * (b.block / 32);
+    // groups: shots sharing a model, tasks interleaved over the group's shots.
+    // In plain mode every shot is a group of its own and runs alone.
+    std::vector<int> order;
+    std::map<int, std::vector<int>> by_model;
+    std::vector<int> model_order;
+    for (int s = 0; s < nshots; ++s) {
+        if (!by_model.count(shots[s].model_id)) model_order.push_back(shots[s].model_id);
+        by_model[shots[s].model_id].push_back(s);
+    }
+    long max_tasks = 0;
+    if (b.plain) {
+        for (int s = 0; s < nshots; ++s) {
+            const Model &m = *c->models[shots[s].model_id];
+            GroupDev g{};
+            g.nshots = 1;
+            g.shot0 = s;
+            g.nstrips = num_strips(m.nnz);
+            g.seg_len = choose_seg_len(m.nnx, g.nstrips, resident_warps);
+            g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
+            g.task_begin = 0;
+            b.groups.push_back(g);
+            max_tasks = std::max<long>(max_tasks, (long)g.nstrips * g.nsegs);
+        }
+    } else {
+        // shots of one model must be contiguous in the shot table for shot0
+        // indexing; keep the caller's order inside each model and reorder the
+        // device table only (seis offsets stay the caller's).
+        std::vector<ShotDev> reordered;
+        int task = 0;
+        for (int mid : model_order) {
+            const Model &m = *c->models[mid];
+            const std::vector<int> &ss = by_model[mid];
+            GroupDev g{};
+            g.task_begin = task;
+            g.nshots = (int)ss.size();
+            g.shot0 = (int)reordered.size();
+            g.nstrips = num_strips(m.nnz);
+            b.groups.push_back(g);
+            for (int s : ss) reordered.push_back(b.shot_dev[s]);
+        }
+        long per_seg_total = 0;
+        for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
+        for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+            GroupDev &g = b.groups[gi];
+            const Model &m = *c->models[model_order[gi]];
+            g.seg_len = choose_seg_len(m.nnx, per_seg_total, resident_warps);
+            g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
+        }
+        task = 0;
+        for (auto &g : b.groups) {
+            g.task_begin = task;
+            task += g.nshots * g.nstrips * g.nsegs;
+        }
+        max_tasks = task;
+        CK(cudaMemcpy(b.shots_d.p, reordered.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
+    }
+    CK(b.groups_d.alloc(sizeof(GroupDev) * b.groups.size()));
+    CK(cudaMemcpy(b.groups_d.p, b.groups.data(), sizeof(GroupDev) * b.groups.size(), cudaMemcpyHostToDevice));
+    const long blocks_needed = (max_tasks * 32 + b.block - 1) / b.block;
+    b.grid = (int)std::max<long>(1, std::min<long>(blocks_needed, (long)c->sm_count * bps));
+    CK(cudaStreamSynchronize(c->stream));
+    c->batch = std::move(bp);
+    return S2D_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int s2d_abi_version(void) { return S2D_ABI_VERSION; }
+
+int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out) {
+    if (!wave || !out) return S2D_ERR_ARG;
+    if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0)) return S2D_ERR_ARG;
+    RunSteps r = derive_steps(*wave, 1.0f, 1.0f);
+    out->fd_nt = r.fd_nt;
+    out->real_nt = r.real_nt;
+    out->dt_factor = r.dt_factor;
+    out->nts = r.nts;
+    return S2D_OK;
+}
+
+int s2d_create(void **ctx, int device) {
+    if (!ctx) return S2D_ERR_ARG;
+    *ctx = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return S2D_ERR_NODEV;
+    }
+    if (device < 0 || device >= n) return S2D_ERR_ARG;
+    auto c = new Ctx();
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        delete c;
+        cudaGetLastError();
+        return S2D_ERR_CUDA;
+    }
+    *ctx = c;
+    return S2D_OK;
+}
+
+void s2d_destroy(void *ctx) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->batch.reset();
+    c->pool.free.clear();
+    c->models.clear();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *s2d_last_error(const void *ctx) {
+    const Ctx *c = static_cast<const Ctx *>(ctx);
+    return c ? c->err.c_str() : "null context";
+}
+
+int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, const float *vp, const float *rho,
+                     unsigned flags, int *model_id) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c) return S2D_ERR_ARG;
+    if (!vp || !rho || !model_id) return fail(c, S2D_ERR_ARG, "null model pointer");
+    if (nx < 1 || nz < 1 || nb < 2 || !(dx > 0) || !(dz > 0))
+        return fail(c, S2D_ERR_ARG, "bad model shape nx=%d nz=%d nb=%d dx=%g dz=%g", nx, nz, nb, dx, dz);
+    CK(cudaSetDevice(c->device));
+    auto m = std::make_unique<Model>();
+    m->nx = nx; m->nz = nz; m->nb = nb; m->dx = dx; m->dz = dz;
+    m->nnx = nx + 2 * nb;
+    m->nnz = nz + 2 * nb;
+    m->ld = leading_dim(m->nnz);
+    m->nxa = m->nnx + 2 * S2D_GX;
+    m->field_elems = (size_t)m->nxa * m->ld;
+    const size_t raw = (size_t)nx * nz * sizeof(float);
+    CK(m->vp.alloc(raw));
+    CK(m->rho.alloc(raw));
+    const cudaMemcpyKind kind = (flags & S2D_MODEL_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(m->vp.p, vp, raw, kind, c->stream));
+    CK(cudaMemcpyAsync(m->rho.p, rho, raw, kind, c->stream));
+    const size_t fb = m->field_elems * sizeof(float);
+    CK(m->kappa.alloc(fb));
+    CK(m->bx.alloc(fb));
+    CK(m->bz.alloc(fb));
+    DevBuf bue;
+    CK(bue.alloc(fb));
+    CK(cudaMemsetAsync(m->kappa.p, 0, fb, c->stream));
+    CK(cudaMemsetAsync(m->bx.p, 0, fb, c->stream));
+    CK(cudaMemsetAsync(m->bz.p, 0, fb, c->stream));
+    CK(cudaMemsetAsync(bue.p, 0, fb, c->stream));
+    int e = launch_prepare_model(m->vp.as<float>(), m->rho.as<float>(), nx, nz, nb, m->ld, m->kappa.as<float>(),
+                                 bue.as<float>(), m->bx.as<float>(), m->bz.as<float>(), c->stream);
+    if (e) return fail(c, S2D_ERR_CUDA, "prepare_model: %s", cudaGetErrorString((cudaError_t)e));
+    CK(cudaStreamSynchronize(c->stream));
+    sponge_a(nb, nx, m->damp2a, m->damp2a1);
+    sponge_b(nb, nx, m->damp2b, m->damp2b1);
+    sponge_a(nb, nz, m->damp1a, m->damp1a1);
+    sponge_b(nb, nz, m->damp1b, m->damp1b1);
+    const int id = c->next_model++;
+    c->models[id] = std::move(m);
+    *model_id = id;
+    return S2D_OK;
+}
+
+int s2d_model_destroy(void *ctx, int model_id) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c) return S2D_ERR_ARG;
+    auto it = c->models.find(model_id);
+    if (it == c->models.end()) return fail(c, S2D_ERR_ARG, "unknown model id %d", model_id);
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    c->drop_batch();  // a batch may reference the model
+    c->models.erase(it);
+    return S2D_OK;
+}
+
+int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wave, const double *wavelet,
+                int nwavelet, int kt_begin, int kt_count, float *seis_out, unsigned flags, s2d_stats *stats) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c) return S2D_ERR_ARG;
+    if (!shots || nshots < 1 || !wave) return fail(c, S2D_ERR_ARG, "no shots or no wave description");
+    if (!seis_out) return fail(c, S2D_ERR_ARG, "null seismogram buffer");
+    if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0))
+        return fail(c, S2D_ERR_ARG, "wave parameters must be positive");
+    if (kt_begin < 0) return fail(c, S2D_ERR_ARG, "negative kt_begin");
+    CK(cudaSetDevice(c->device));
+    if (kt_begin == 0) {
+        int e = setup_batch(c, shots, nshots, *wave, wavelet, nwavelet, seis_out, flags);
+        if (e) {
+            c->drop_batch();
+            return e;
+        }
+    } else {
+        if (!c->batch || c->batch->nshots != nshots || c->batch->kt_next != kt_begin ||
+            c->batch->plain != ((flags & S2D_PLAIN) != 0))
+            return fail(c, S2D_ERR_STATE, "continuation at kt=%d does not follow the previous call", kt_begin);
+        if (flags & S2D_SEIS_DEVICE) {
+            if (c->batch->seis_d != seis_out)
+                return fail(c, S2D_ERR_STATE, "continuation must record into the same device buffer");
+        }
+    }
+    Batch &b = *c->batch;
+    const RunSteps &rs = b.steps;
+    const int kt_end = (kt_count <= 0) ? rs.fd_nt : std::min(rs.fd_nt, kt_begin + kt_count);
+    const int nsteps = kt_end - kt_begin;
+    if (nsteps < 0) return fail(c, S2D_ERR_ARG, "kt_begin %d beyond fd_nt %d", kt_begin, rs.fd_nt);
+    const bool use_graph = !(flags & S2D_NO_GRAPH);
+    int launches = 0;
+    bool graph_used = false;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    StepArgs a{};
+    a.shots = b.shots_d.as<ShotDev>();
+    a.dt_factor = rs.dt_factor;
+    a.fd_nt = rs.fd_nt;
+    if (b.plain) {
+        for (int s = 0; s < nshots; ++s) {
+            a.groups = b.groups_d.as<GroupDev>() + s;
+            a.ngroups = 1;
+            a.total_tasks = b.groups[s].nstrips * b.groups[s].nsegs;
+            int e = run_loop(c, b, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
+            if (e) return e;
+        }
+    } else {
+        a.groups = b.groups_d.as<GroupDev>();
+        a.ngroups = (int)b.groups.size();
+        a.total_tasks = 0;
+        for (auto &g : b.groups) a.total_tasks += g.nshots * g.nstrips * g.nsegs;
+        int e = run_loop(c, b, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
+        if (e) return e;
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    b.kt_next = kt_end;
+    // seismogram samples recorded in [kt_begin, kt_end), widened to the whole
+    // trace at the run's start and end so unrecorded samples read as zero
+    if (!(flags & S2D_SEIS_DEVICE) && b.seis_elems) {
+        int t0 = kt_begin == 0 ? 0 : (kt_begin + 1 + rs.dt_factor - 1) / rs.dt_factor - 1;
+        int t1 = kt_end >= rs.fd_nt ? rs.real_nt : kt_end / rs.dt_factor;
+        t0 = std::max(0, std::min(t0, rs.real_nt));
+        t1 = std::max(t0, std::min(t1, rs.real_nt));
+        if (t1 > t0) {
+            const size_t rows = b.seis_elems / rs.real_nt;
+            CK(cudaMemcpy2DAsync(seis_out + t0, sizeof(float) * rs.real_nt, b.seis_d + t0, sizeof(float) * rs.real_nt,
+                                 sizeof(float) * (t1 - t0), rows, cudaMemcpyDeviceToHost, c->stream));
+        }
+        CK(cudaStreamSynchronize(c->stream));
+    } else if (flags & S2D_SYNC) {
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (stats) {
+        CK(cudaEventSynchronize(c->ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        double cells = 0;
+        for (int s = 0; s < nshots; ++s) {
+            const Model &m = *c->models[b.shots[s].model_id];
+            cells += (double)m.nnx * m.nnz;
+        }
+        stats->loop_ms = ms;
+        stats->cell_updates = cells * nsteps;
+        stats->gcells_per_s = ms > 0 ? stats->cell_updates / (ms * 1e6) : 0.0;
+        stats->kernel_launches = launches;
+        stats->graph_used = graph_used ? 1 : 0;
+    }
+    return S2D_OK;
+}
+
+}  // extern "C"

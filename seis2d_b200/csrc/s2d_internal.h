@@ -1,0 +1,85 @@
+// Internal layout and launch structures of libseis2d (not part of the ABI).
+//
+// Device layout of every per-cell field (state, materials):
+//   element (x, z) of the padded grid lives at  base[(x + S2D_GX) * ld + (z + S2D_GZ)]
+//   for x in [-S2D_GX, nnx + S2D_GX) and z in [-S2D_GZ, ld - S2D_GZ).
+// Cells outside [0,nnx) x [0,nnz) are ghost cells: zero-filled once and never
+// written, so that stencil reads near the grid edge need no branches.  The
+// 1-D coefficient tables hold zeros at ghost indices, which makes every value
+// the step computes at a ghost cell exactly zero.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#define S2D_GX 4            // ghost columns on each side
+#define S2D_GZ 4            // ghost rows above z = 0
+#define S2D_ZPT 4           // rows per lane (one float4)
+#define S2D_STRIP_ROWS 128  // rows a warp reads (32 lanes x 4)
+#define S2D_STRIP_OUT 120   // rows a warp writes; strip k writes [120k, 120k+120)
+
+namespace s2d {
+
+constexpr float kA0 = 1.125f;              // cpu_modelling_kernels.cpp:9
+constexpr float kA1 = -1.0f / 24.0f;       // cpu_modelling_kernels.cpp:10 (float quotient)
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Strips a grid of nnz rows needs, and the leading dimension that holds them.
+inline int num_strips(int nnz) { return (nnz + S2D_STRIP_OUT - 1) / S2D_STRIP_OUT; }
+inline int leading_dim(int nnz) { return round_up(S2D_GZ + S2D_STRIP_OUT * num_strips(nnz) + 8, 32); }
+
+// One shot of a launch.  State pointers point at the allocation base
+// (ghost origin); st[parity][field] with fields px, pz, vx, vz.
+struct ShotDev {
+    float *st[2][4];
+    const float *kappa, *bx, *bz;  // materials, same layout as the state
+    const float4 *xcoef;           // [nnx + 2 GX]: damp2a, kx*damp2a1, damp2b, kx*damp2b1
+    const float4 *zcoef;           // [ld]:         damp1a, kz*damp1a1, damp1b, kz*damp1b1
+    int nnx, nnz, ld;
+    int src_x, src_z;              // padded cell of the source
+    const float *amp;              // [fd_nt] value added to px at the source after step kt
+    const int *rec_ptr;            // [nnx + 1] receivers grouped by column (CSR)
+    const int *rec_z;              // padded row of each receiver entry
+    const int *rec_id;             // index of the entry's trace in seis
+    float *seis;                   // [nrec][real_nt]
+    int real_nt;
+    int pad_;
+};
+
+// Shots that share one grid shape; their tasks are interleaved so that the
+// warps streaming the same tile of the same model for different shots run
+// together and share the model's tiles through L2.
+struct GroupDev {
+    int task_begin;   // first flat task index of the group
+    int nshots;       // shots in the group
+    int shot0;        // index of the group's first shot in the shot table
+    int nstrips;      // strips per shot
+    int nsegs;        // x-segments per strip
+    int seg_len;      // columns per x-segment
+    int pad_[2];
+};
+
+// Arguments of one launch sequence.  They live in device memory and are
+// written by a one-thread kernel in stream order before each sequence, so a
+// captured graph of step launches serves every continuation and every shot.
+struct StepArgs {
+    const ShotDev *shots;
+    const GroupDev *groups;
+    int ngroups;
+    int total_tasks;
+    int dt_factor;
+    int fd_nt;
+    int kt_base;          // FD step of the launch with kt_off = 0
+    int pad_;
+};
+
+// Host-side launch helpers implemented in s2d_kernels.cu.
+int launch_step(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream);
+int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
+int launch_prepare_model(const float *vp, const float *rho, int nx, int nz, int nb, int ld,
+                         float *kappa, float *bue_scratch, float *bx, float *bz, void *stream);
+int step_kernel_occupancy(int block, int *blocks_per_sm);
+int step_kernel_attributes(int *regs, int *local_bytes);
+
+}  // namespace s2d

@@ -1,0 +1,172 @@
+"""Parity of the CUDA forward path (through the C ABI) with the reference.
+
+Golden seismograms were produced by the reference CPU binary itself
+(tests/golden/make_golden.py); the oracle (oracle/s2d_oracle.c, bit-exact
+with the reference on those cases) covers the other inputs.  Bar: relative
+L2 of the FP32 seismogram against the reference's FP64 one <= 1e-5.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cases import CASES, model
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5  # seismogram rel-L2, FP32 CUDA vs FP64 reference
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from seis2d_b200 import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _golden(name):
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    c = json.loads(str(z["params"]))
+    vp, rho = model(c["model"], c["nx"], c["nz"], c["dx"], c["dz"])
+    return z, c, vp, rho
+
+
+def _wave(c):
+    from seis2d_b200 import Wave
+    return Wave(c["T"], c["dt"], c["ddt"], c["f"])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_parity(ctx, name):
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden(name)
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    seis = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
+    ref = z["seis"]
+    assert seis.shape == ref.shape
+    err = O.rel_l2(seis, ref)
+    assert err <= TOL, err
+    # against the FP32 CPU restatement of the same arithmetic: tighter
+    p = O.Params(c["nx"], c["nz"], c["nb"], c["dx"], c["dz"], c["T"], c["dt"], c["ddt"], c["f"])
+    s32 = O.forward(p, vp, rho, z["src"], z["rec"][:, 0], z["rec"][:, 1], O.F32)
+    assert O.rel_l2(seis, s32) <= 2e-6
+    m.release()
+
+
+def test_state_after_few_steps_matches_oracle(ctx):
+    """Cell-by-cell p after 1, 2 and 10 steps on an odd-sized grid, through
+    the seismogram of a receiver at every cell of a few rows and columns."""
+    from seis2d_b200 import Shot, Wave
+    nx, nz, nb = 37, 29, 32
+    vp = np.full((nx, nz), 2000.0, np.float32)
+    vp[:, 15:] = 2600.0
+    rho = np.full((nx, nz), 1500.0, np.float32)
+    rho[20:, :] = 2100.0
+    dx = dz = 10.0
+    m = ctx.model(vp, rho, dx, dz, nb)
+    # receivers on every physical cell
+    xs, zs = np.meshgrid(np.arange(nx) * dx, np.arange(nz) * dz, indexing="ij")
+    rec = np.stack([xs.ravel(), zs.ravel()], 1).astype(np.float32)
+    wave = Wave(0.012, 0.001, 0.001, 25.0)
+    seis = ctx.forward([Shot(m, (180.0, 60.0), rec)], wave)[0]  # [ncell][12]
+    p = O.Params(nx, nz, nb, dx, dz, 0.012, 0.001, 0.001, 25.0)
+    ref = O.forward(p, vp, rho, (180.0, 60.0), rec[:, 0], rec[:, 1], O.F64)
+    for k in (0, 1, 9):
+        a, b = seis[:, k], ref[:, k]
+        assert O.rel_l2(a, b) < 1e-5, (k, O.rel_l2(a, b))
+
+
+def test_plain_batched_graph_modes_agree(ctx):
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("twolayer_split_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    shots = [Shot(m, (x, 20.0), z["rec"]) for x in (300.0, 800.0, 1200.0)]
+    w = _wave(c)
+    batched = ctx.forward(shots, w)
+    plain = ctx.forward(shots, w, plain=True)
+    nograph = ctx.forward(shots, w, graph=False)
+    for a, b, d in zip(batched, plain, nograph):
+        np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(a, d)
+    # the middle shot is the golden one
+    assert O.rel_l2(batched[1], z["seis"]) <= TOL
+
+
+def test_continuation_equals_single_call(ctx):
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("gradient_endonleft_nb40")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    w = _wave(c)
+    shots = [Shot(m, tuple(z["src"]), z["rec"])]
+    whole = ctx.forward(shots, w)[0]
+    nrec, nt = whole.shape
+    out = np.full(nrec * nt, np.nan, np.float32)
+    k = 0
+    for n in (1, 97, 200, 0):  # 0: to the end
+        ctx.forward(shots, w, kt_begin=k, kt_count=n, out=out)
+        k += n
+    np.testing.assert_array_equal(out.reshape(nrec, nt), whole)
+
+
+def test_uneven_models_in_one_batch(ctx):
+    """Shots on models of different sizes in one launch sequence equal the
+    same shots run alone."""
+    from seis2d_b200 import Shot
+    shots, singles = [], []
+    w = None
+    for name in ("twolayer_split_nb32", "layers_endonright_near_nb32", "corner_source_nb40"):
+        z, c, vp, rho = _golden(name)
+        w = _wave(c) if w is None else w
+        m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+        shots.append(Shot(m, tuple(z["src"]), z["rec"]))
+    both = ctx.forward(shots, w)
+    for s, got in zip(shots, both):
+        alone = ctx.forward([s], w)[0]
+        np.testing.assert_array_equal(got, alone)
+
+
+def test_device_output_matches_host(ctx):
+    import torch
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("edges_explicit_nb32")
+    m = ctx.model(torch.from_numpy(vp).cuda(), torch.from_numpy(rho).cuda(), c["dx"], c["dz"], c["nb"])
+    w = _wave(c)
+    host = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], w)[0]
+    dev = torch.zeros(host.size, dtype=torch.float32, device="cuda")
+    ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], w, out=dev)
+    np.testing.assert_array_equal(dev.cpu().numpy().reshape(host.shape), host)
+    assert O.rel_l2(host, z["seis"]) <= TOL
+
+
+def test_custom_wavelet_equals_ricker(ctx):
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("twolayer_split_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    p = O.Params(c["nx"], c["nz"], c["nb"], c["dx"], c["dz"], c["T"], c["dt"], c["ddt"], c["f"])
+    w = O.ricker(p)  # nts samples; the reference's sample at kt == nts is 0
+    w = np.concatenate([w, [0.0]])
+    a = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c), wavelet=w)[0]
+    b = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
+    np.testing.assert_array_equal(a, b)
+
+
+def test_errors_are_statuses(ctx):
+    from seis2d_b200 import Shot
+    from seis2d_b200._lib import Seis2dError, S2D_ERR_GEOM, S2D_ERR_STATE
+    z, c, vp, rho = _golden("twolayer_split_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    far = np.array([[1e6, 0.0]], np.float32)
+    with pytest.raises(Seis2dError) as e:
+        ctx.forward([Shot(m, (100.0, 0.0), far)], _wave(c))
+    assert e.value.code == S2D_ERR_GEOM
+    with pytest.raises(Seis2dError) as e:
+        ctx.forward([Shot(m, (100.0, 0.0), z["rec"])], _wave(c), kt_begin=5, kt_count=5,
+                    out=np.zeros(z["seis"].size, np.float32))
+    assert e.value.code == S2D_ERR_STATE
+    # context still usable after errors
+    s = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
+    assert O.rel_l2(s, z["seis"]) <= TOL
