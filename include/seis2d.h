@@ -121,6 +121,24 @@ S2D_API void s2d_destroy(void *ctx);
 /* Text of the last error on this context (never NULL). */
 S2D_API const char *s2d_last_error(const void *ctx);
 
+/*
+ * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
+ *   "variant"     0 bulk-copy pipeline, 1 plain loads (default), 2 bulk-copy
+ *                 pipeline compiled for 128 registers
+ *   "block"       threads per block: 32, 64, 96 or 128 (default 128)
+ *   "task_order"  0: consecutive warps take the shots of one tile;
+ *                 1: consecutive warps take adjacent strips of one shot (default)
+ *   "stages"      bulk-copy ring depth per warp, 2..16 (default 5)
+ *   "seg_len"     columns per x-segment of a warp task, 0 = automatic
+ *   "spin_limit"  polls of a pipeline barrier before the wait gives up and the
+ *                 call returns S2D_ERR_TIMEOUT (default 2^20)
+ *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of
+ *                 that pipeline iteration of its first task, so its bounded
+ *                 wait runs out (no fault, no hang); -1 (default) disables
+ * Options apply to the next s2d_forward call.
+ */
+S2D_API int s2d_set_option(void *ctx, const char *key, long value);
+
 /* Derived step counts for a wave description, host-only, no device needed
  * (src/src_cpu/cpumodelling.cpp:174-188). */
 S2D_API int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out);

@@ -58,6 +58,7 @@ SIGNATURES = {
     "s2d_destroy": ([C.c_void_p], None),
     "s2d_last_error": ([C.c_void_p], C.c_char_p),
     "s2d_derive_steps": ([C.POINTER(Wave), C.POINTER(Steps)], C.c_int),
+    "s2d_set_option": ([C.c_void_p, C.c_char_p, C.c_long], C.c_int),
     "s2d_model_create": ([C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
                           C.c_void_p, C.c_void_p, C.c_uint, C.POINTER(C.c_int)], C.c_int),
     "s2d_model_destroy": ([C.c_void_p, C.c_int], C.c_int),

@@ -99,6 +99,10 @@ class Context:
         except Exception:
             pass
 
+    def set_option(self, key: str, value: int):
+        """Step-kernel tuning knob (see s2d_set_option in include/seis2d.h)."""
+        self._check(L.lib().s2d_set_option(self._h, key.encode(), int(value)))
+
     def model(self, vp, rho, dx: float, dz: float, nb: int = 32) -> Model:
         """Upload a ``[nx][nz]`` model (numpy or CUDA tensor, float32)."""
         flags = 0

@@ -80,9 +80,8 @@ struct Batch {
     DevBuf seis_int;                 // internal seismogram buffer (host output)
     float *seis_d = nullptr;         // where the kernels record
     size_t seis_elems = 0;
-    int grid = 0, block = 128;
-    std::map<int, cudaGraphExec_t> graphs;  // by step count
-    std::vector<int> plain_group_tasks;
+    long max_tasks = 0;              // largest task count of one launch sequence
+    std::map<std::vector<long>, cudaGraphExec_t> graphs;  // by (steps, launch config)
     ~Batch() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
     }
@@ -115,9 +114,27 @@ struct Pool {
     }
 };
 
+// Launch configuration of the step kernel.
+struct LaunchCfg {
+    int variant = kVariantBulk;
+    int block = 128;      // threads per block (whole warps)
+    int stages = 5;       // bulk-copy ring depth per warp
+    size_t smem = 0;
+    int grid = 0;
+};
+
 struct Ctx {
     int device = 0;
     int sm_count = 0;
+    // tuning options (s2d_set_option)
+    int opt_variant = kVariantLdg;   // fastest on the c2 batch (see profiles/)
+    int opt_block = 128;
+    int opt_stages = 5;
+    int opt_seg_len = 0;      // 0 = automatic
+    int opt_spin_limit = 1 << 20;
+    int opt_fault_iter = -1;  // test knob, see s2d_set_option
+    int opt_order = 1;        // task order (StepArgs::task_order)
+    DevBuf dev_err;           // device error word of the step kernels
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err = "no error";
@@ -157,7 +174,7 @@ int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps) {
     static const int cand[] = {1024, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16};
     for (int L : cand) {
         long nsegs = (nnx + L - 1) / L;
-        if (tasks_per_seg * nsegs >= 4 * resident_warps) return std::min(L, nnx);
+        if (tasks_per_seg * nsegs >= 24 * resident_warps) return std::min(L, nnx);
     }
     return 16;
 }
@@ -184,30 +201,60 @@ int build_coef(Ctx *c, Model &m, float fd_dt) {
     return S2D_OK;
 }
 
+// Launch configuration from the context's options: block size, ring depth,
+// shared memory and a grid of exactly the resident blocks (the kernels loop
+// over tasks), capped by the work available.
+int launch_config(Ctx *c, long max_tasks, LaunchCfg *out) {
+    LaunchCfg lc;
+    lc.variant = c->opt_variant;
+    lc.block = std::max(32, std::min(128, c->opt_block / 32 * 32));
+    lc.stages = std::max(2, std::min(16, c->opt_stages));
+    lc.smem = lc.variant == kVariantLdg ? 0 : bulk_smem_bytes(lc.block / 32, lc.stages);
+    int e = step_kernel_prepare(lc.variant, lc.smem);
+    if (e) return fail(c, S2D_ERR_ARG, "step kernel does not accept %zu B of shared memory: %s", lc.smem,
+                       cudaGetErrorString((cudaError_t)e));
+    int bps = 0;
+    e = step_kernel_occupancy(lc.variant, lc.block, lc.smem, &bps);
+    if (e || bps < 1)
+        return fail(c, S2D_ERR_ARG, "launch configuration (variant %d, block %d, stages %d) cannot run", lc.variant,
+                    lc.block, lc.stages);
+    const long resident = (long)c->sm_count * bps;
+    const long needed = (max_tasks * 32 + lc.block - 1) / lc.block;
+    lc.grid = (int)std::max<long>(1, std::min<long>(resident, std::max<long>(needed, 1)));
+    *out = lc;
+    return S2D_OK;
+}
+
 // One pass over `nsteps` FD steps starting at kt_begin, for the launch
 // arguments `args` (a whole batch, or one shot of a plain run).
-int run_loop(Ctx *c, Batch &b, StepArgs args, int kt_begin, int nsteps, bool use_graph, int *launches,
-             bool *graph_used) {
+int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin, int nsteps, bool use_graph,
+             int *launches, bool *graph_used) {
     if (nsteps <= 0) return S2D_OK;
     args.kt_base = kt_begin;
+    args.stages = lc.stages;
+    args.err = c->dev_err.as<int>();
+    args.spin_limit = c->opt_spin_limit;
+    args.fault_iter = c->opt_fault_iter;
+    args.task_order = c->opt_order;
     StepArgs *args_d = b.args_d.as<StepArgs>();
     int e = launch_set_args(args, args_d, c->stream);
     if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
     *launches += 1;
     if (!use_graph) {
         for (int k = 0; k < nsteps; ++k) {
-            e = launch_step(args_d, k, b.grid, b.block, c->stream);
+            e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
             if (e) return fail(c, S2D_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)e));
         }
         *launches += nsteps;
         return S2D_OK;
     }
-    auto it = b.graphs.find(nsteps);
+    const std::vector<long> key = {nsteps, lc.variant, lc.block, lc.stages, (long)lc.smem, lc.grid};
+    auto it = b.graphs.find(key);
     if (it == b.graphs.end()) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < nsteps; ++k) {
-            e = launch_step(args_d, k, b.grid, b.block, c->stream);
+            e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
             if (e) {
                 cudaStreamEndCapture(c->stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -219,7 +266,7 @@ int run_loop(Ctx *c, Batch &b, StepArgs args, int kt_begin, int nsteps, bool use
         cudaError_t ce = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         CK(ce);
-        it = b.graphs.emplace(nsteps, ge).first;
+        it = b.graphs.emplace(key, ge).first;
     }
     CK(cudaGraphLaunch(it->second, c->stream));
     *launches += nsteps;
@@ -368,10 +415,14 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
     CK(cudaMemcpy(b.shots_d.p, b.shot_dev.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
     CK(b.args_d.alloc(sizeof(StepArgs)));
 
-    // launch shape: 4 warps per block, grid = resident blocks (grid-stride over tasks)
-    int bps = 0;
-    if (step_kernel_occupancy(b.block, &bps) || bps < 1) bps = 1;
-    const long resident_warps = (long)c->sm_count * bps * (b.block / 32);
+    // segment lengths are chosen for the resident warp count of the current
+    // launch configuration (grid = resident blocks, grid-stride over tasks)
+    LaunchCfg lc;
+    {
+        int e = launch_config(c, 1, &lc);
+        if (e) return e;
+    }
+    const long resident_warps = (long)lc.grid * (lc.block / 32);
     // groups: shots sharing a model, tasks interleaved over the group's shots.
     // In plain mode every shot is a group of its own and runs alone.
     std::vector<int> order;
@@ -389,7 +440,8 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             g.nshots = 1;
             g.shot0 = s;
             g.nstrips = num_strips(m.nnz);
-            g.seg_len = choose_seg_len(m.nnx, g.nstrips, resident_warps);
+            g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, m.nnx)
+                                           : choose_seg_len(m.nnx, g.nstrips, resident_warps);
             g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
             g.task_begin = 0;
             b.groups.push_back(g);
@@ -417,7 +469,8 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         for (size_t gi = 0; gi < b.groups.size(); ++gi) {
             GroupDev &g = b.groups[gi];
             const Model &m = *c->models[model_order[gi]];
-            g.seg_len = choose_seg_len(m.nnx, per_seg_total, resident_warps);
+            g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, m.nnx)
+                                           : choose_seg_len(m.nnx, per_seg_total, resident_warps);
             g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
         }
         task = 0;
@@ -430,10 +483,24 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
     }
     CK(b.groups_d.alloc(sizeof(GroupDev) * b.groups.size()));
     CK(cudaMemcpy(b.groups_d.p, b.groups.data(), sizeof(GroupDev) * b.groups.size(), cudaMemcpyHostToDevice));
-    const long blocks_needed = (max_tasks * 32 + b.block - 1) / b.block;
-    b.grid = (int)std::max<long>(1, std::min<long>(blocks_needed, (long)c->sm_count * bps));
+    b.max_tasks = max_tasks;
     CK(cudaStreamSynchronize(c->stream));
     c->batch = std::move(bp);
+    return S2D_OK;
+}
+
+// Read and clear the step kernels' error word (after the stream is idle).
+int check_device_error(Ctx *c) {
+    int h = 0;
+    CK(cudaMemcpy(&h, c->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        CK(cudaMemset(c->dev_err.p, 0, sizeof(int)));
+        if (c->batch) c->batch->kt_next = -1;  // the wavefields are not valid any more
+        return fail(c, S2D_ERR_TIMEOUT,
+                    "a step-kernel pipeline wait ran out of its spin limit (device error bits 0x%x); "
+                    "the affected steps were not computed",
+                    h);
+    }
     return S2D_OK;
 }
 
@@ -444,6 +511,38 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
 extern "C" {
 
 int s2d_abi_version(void) { return S2D_ABI_VERSION; }
+
+int s2d_set_option(void *ctx, const char *key, long value) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c || !key) return S2D_ERR_ARG;
+    const std::string k(key);
+    if (k == "variant") {
+        if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128)
+            return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
+        c->opt_variant = (int)value;
+    } else if (k == "block") {
+        if (value < 32 || value > 128 || value % 32)
+            return fail(c, S2D_ERR_ARG, "block must be 1 to 4 whole warps (the step kernels are built for <= 128 threads)");
+        c->opt_block = (int)value;
+    } else if (k == "stages") {
+        if (value < 2 || value > 16) return fail(c, S2D_ERR_ARG, "stages must be in [2, 16]");
+        c->opt_stages = (int)value;
+    } else if (k == "seg_len") {
+        if (value < 0) return fail(c, S2D_ERR_ARG, "seg_len must be >= 0");
+        c->opt_seg_len = (int)value;
+    } else if (k == "spin_limit") {
+        if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
+        c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "task_order") {
+        if (value != 0 && value != 1) return fail(c, S2D_ERR_ARG, "task_order must be 0 or 1");
+        c->opt_order = (int)value;
+    } else if (k == "inject_wait_fault") {
+        c->opt_fault_iter = value < 0 ? -1 : (int)value;
+    } else {
+        return fail(c, S2D_ERR_ARG, "unknown option '%s'", key);
+    }
+    return S2D_OK;
+}
 
 int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out) {
     if (!wave || !out) return S2D_ERR_ARG;
@@ -472,6 +571,8 @@ int s2d_create(void **ctx, int device) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = c->dev_err.alloc(sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->dev_err.p, 0, sizeof(int));
     if (e != cudaSuccess) {
         delete c;
         cudaGetLastError();
@@ -590,6 +691,11 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     const bool use_graph = !(flags & S2D_NO_GRAPH);
     int launches = 0;
     bool graph_used = false;
+    LaunchCfg lc;
+    {
+        int e = launch_config(c, b.max_tasks, &lc);
+        if (e) return e;
+    }
     CK(cudaEventRecord(c->ev0, c->stream));
     StepArgs a{};
     a.shots = b.shots_d.as<ShotDev>();
@@ -600,7 +706,7 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
             a.groups = b.groups_d.as<GroupDev>() + s;
             a.ngroups = 1;
             a.total_tasks = b.groups[s].nstrips * b.groups[s].nsegs;
-            int e = run_loop(c, b, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
+            int e = run_loop(c, b, lc, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
             if (e) return e;
         }
     } else {
@@ -608,7 +714,7 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         a.ngroups = (int)b.groups.size();
         a.total_tasks = 0;
         for (auto &g : b.groups) a.total_tasks += g.nshots * g.nstrips * g.nsegs;
-        int e = run_loop(c, b, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
+        int e = run_loop(c, b, lc, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
         if (e) return e;
     }
     CK(cudaEventRecord(c->ev1, c->stream));
@@ -628,6 +734,10 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         CK(cudaStreamSynchronize(c->stream));
     } else if (flags & S2D_SYNC) {
         CK(cudaStreamSynchronize(c->stream));
+    }
+    if (!(flags & S2D_SEIS_DEVICE) || (flags & S2D_SYNC)) {
+        int e = check_device_error(c);
+        if (e) return e;
     }
     if (stats) {
         CK(cudaEventSynchronize(c->ev1));

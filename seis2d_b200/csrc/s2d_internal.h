@@ -71,15 +71,38 @@ struct StepArgs {
     int dt_factor;
     int fd_nt;
     int kt_base;          // FD step of the launch with kt_off = 0
+    int stages;           // bulk-copy pipeline depth (shared-memory ring stages per warp)
+    int *err;             // device error word (S2D_DEV_ERR_* bits), 0 when all waits completed
+    int spin_limit;       // polls of an mbarrier before a wait counts as timed out
+    int fault_iter;       // test knob: pipeline iteration whose copies are not issued (-1: none)
+    int task_order;       // 0: shot fastest, 1: strip fastest (see task_of)
     int pad_;
 };
 
+// Device error bits reported through StepArgs::err.
+#define S2D_DEV_ERR_WAIT 1    // a pipeline wait gave up (bounded spin ran out)
+#define S2D_DEV_ERR_DRAIN 2   // copies still in flight after the bounded drain
+
+// Step kernel variants.
+enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2 };
+
+// Shared memory of one pipeline stage: 7 slots of one 128-row column each
+// (vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3).
+constexpr int kSlotBytes = S2D_STRIP_ROWS * 4;
+constexpr int kSlots = 7;
+constexpr int kStageBytes = kSlots * kSlotBytes;
+inline size_t bulk_smem_bytes(int warps_per_block, int stages) {
+    return (size_t)warps_per_block * stages * (kStageBytes + 8);
+}
+
 // Host-side launch helpers implemented in s2d_kernels.cu.
-int launch_step(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream);
+int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int block, size_t smem,
+                void *stream);
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
 int launch_prepare_model(const float *vp, const float *rho, int nx, int nz, int nb, int ld,
                          float *kappa, float *bue_scratch, float *bx, float *bz, void *stream);
-int step_kernel_occupancy(int block, int *blocks_per_sm);
-int step_kernel_attributes(int *regs, int *local_bytes);
+int step_kernel_prepare(int variant, size_t smem);
+int step_kernel_occupancy(int variant, int block, size_t smem, int *blocks_per_sm);
+int step_kernel_attributes(int variant, int *regs, int *local_bytes);
 
 }  // namespace s2d

@@ -9,18 +9,28 @@
 //   * A warp owns a strip of 128 rows (each lane 4 consecutive z rows, one
 //     float4) and streams along x over a segment of columns.  It keeps
 //     sliding windows of vx (4 columns), new p (4 columns) and vz (3 columns)
-//     in registers, so every field is read from HBM once per step, and the
-//     x-stencils need no shared memory.
+//     in registers, so every field is read from HBM once per step and the
+//     x-stencils need no shared-memory exchange.
 //   * z-neighbours come from the adjacent lanes by warp shuffles.  The strip
 //     overlaps its neighbours by 4 rows on each side and writes only the
 //     middle 120 rows, so warps never exchange data and never synchronise.
 //   * State is double-buffered (read parity kt&1, write the other), which is
 //     what lets pressure and velocity of one step share a single pass.
 //
+// Two ways to bring the columns in:
+//   kVariantBulk  each warp runs its own asynchronous pipeline: one lane issues
+//                 cp.async.bulk copies (TMA engine) of the 512-byte column
+//                 pieces `stages` iterations ahead into a shared-memory ring,
+//                 completion tracked by one mbarrier per stage (transaction
+//                 bytes).  Loads need no registers while in flight, so a warp
+//                 keeps several columns of HBM traffic outstanding.
+//   kVariantLdg   plain 128-bit read-only loads into registers.
+//
 // Traffic per cell-update: px, pz, vx, vz read once and written once
 // (32 B) and kappa, bx, bz read once (12 B, shared through L2 by the shots
 // of a batch that use the same model).
 #include <cuda_runtime.h>
+#include <cstdint>
 
 #include "s2d_internal.h"
 
@@ -55,151 +65,138 @@ __device__ __forceinline__ float comp(const float4 &v, int i) {
     return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
-// One (shot, strip, x-segment) task of one FD step.
-__device__ __forceinline__ void run_task(const ShotDev &S, int strip, int xa, int seg_len, int kt,
-                                         int par, bool rec, int slot, int lane) {
-    const int nnx = S.nnx, nnz = S.nnz;
-    const size_t ld = (size_t)S.ld;
-    const int xb = min(nnx, xa + seg_len);
-    const int c = strip * S2D_STRIP_OUT - 4;  // first row the warp reads
-    const int z0 = c + S2D_ZPT * lane;         // first row of this lane
-    const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
-
-    const float *__restrict__ pxi = S.st[par][0] + off;
-    const float *__restrict__ pzi = S.st[par][1] + off;
-    const float *__restrict__ vxi = S.st[par][2] + off;
-    const float *__restrict__ vzi = S.st[par][3] + off;
-    float *__restrict__ pxo = S.st[par ^ 1][0] + off;
-    float *__restrict__ pzo = S.st[par ^ 1][1] + off;
-    float *__restrict__ vxo = S.st[par ^ 1][2] + off;
-    float *__restrict__ vzo = S.st[par ^ 1][3] + off;
-    const float *__restrict__ kap = S.kappa + off;
-    const float *__restrict__ bxp = S.bx + off;
-    const float *__restrict__ bzp = S.bz + off;
-
-    // Row constants of this lane's four rows.
-    const float4 *zc = S.zcoef + (z0 + S2D_GZ);
-    const float4 zc0 = __ldg(zc + 0), zc1 = __ldg(zc + 1), zc2 = __ldg(zc + 2), zc3 = __ldg(zc + 3);
+// Per-lane constants of one task: the lane's four rows and the shot data.
+struct Lane {
+    float4 zc[4];                 // damp1a, kz*damp1a1, damp1b, kz*damp1b1 per row
     float cm0[4], cm1[4], cp0[4], cp1[4];
+    int z0;                       // first row of the lane
+    bool owner;                   // writes its rows (lanes 1..30)
+    int sdz;                      // source row - z0
+    float amp;                    // source term of this step
+};
+
+__device__ __forceinline__ void lane_setup(Lane &ln, const ShotDev &S, int c, int lane, int kt) {
+    ln.z0 = c + S2D_ZPT * lane;
+    const float4 *zc = S.zcoef + (ln.z0 + S2D_GZ);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        dm_coef(z0 + i, nnz, cm0[i], cm1[i]);
-        dp_coef(z0 + i, nnz, cp0[i], cp1[i]);
+        ln.zc[i] = __ldg(zc + i);
+        dm_coef(ln.z0 + i, S.nnz, ln.cm0[i], ln.cm1[i]);
+        dp_coef(ln.z0 + i, S.nnz, ln.cp0[i], ln.cp1[i]);
     }
-    const bool owner = lane >= 1 && lane <= 30;  // rows [c+4, c+124)
-    const int sdz = S.src_z - z0;
-    const float amp = __ldg(S.amp + kt);
-    const bool src_lane = sdz >= 0 && sdz < 4;
+    ln.owner = lane >= 1 && lane <= 30;
+    ln.sdz = S.src_z - ln.z0;
+    ln.amp = __ldg(S.amp + kt);
+}
 
-    float4 vq0, vq1, vq2, vq3;  // vx at columns L-3 .. L
-    float4 pq0, pq1, pq2, pq3;  // new p at columns L-4 .. L-1
-    float4 zq0, zq1, zq2;       // old vz at columns L-3 .. L-1
-    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    vq1 = ld4(vxi + (ptrdiff_t)(xa - 3) * (ptrdiff_t)ld);
-    vq2 = ld4(vxi + (ptrdiff_t)(xa - 2) * (ptrdiff_t)ld);
-    vq3 = ld4(vxi + (ptrdiff_t)(xa - 1) * (ptrdiff_t)ld);
-    vq0 = zero;
-    pq1 = pq2 = pq3 = zero;
-    zq1 = zq2 = zero;
+// Pressure at column P from vx at P-2..P+1 (q0..q3), old px, pz, kappa and vz
+// at P (cpu_modelling_kernels.cpp:201-258 and 335-351, cpumodelling.cpp:136-142).
+// Returns new p; new px, pz in pxn, pzn.
+__device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int P, const float4 &q0,
+                                           const float4 &q1, const float4 &q2, const float4 &q3, const float4 &px,
+                                           const float4 &pz, const float4 &kk, const float4 &vz, float4 &pxn,
+                                           float4 &pzn) {
+    const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
+    float cx0, cx1;
+    dm_coef(P, S.nnx, cx0, cx1);
+    const float up_z = __shfl_up_sync(kFull, vz.z, 1);
+    const float up_w = __shfl_up_sync(kFull, vz.w, 1);
+    const float dn_x = __shfl_down_sync(kFull, vz.x, 1);
+    const float dz0 = ln.cm0[0] * (vz.x - up_w) + ln.cm1[0] * (vz.y - up_z);
+    const float dz1 = ln.cm0[1] * (vz.y - vz.x) + ln.cm1[1] * (vz.z - up_w);
+    const float dz2 = ln.cm0[2] * (vz.z - vz.y) + ln.cm1[2] * (vz.w - vz.x);
+    const float dz3 = ln.cm0[3] * (vz.w - vz.z) + ln.cm1[3] * (dn_x - vz.y);
+    const float dx0 = cx0 * (q2.x - q1.x) + cx1 * (q3.x - q0.x);
+    const float dx1 = cx0 * (q2.y - q1.y) + cx1 * (q3.y - q0.y);
+    const float dx2 = cx0 * (q2.z - q1.z) + cx1 * (q3.z - q0.z);
+    const float dx3 = cx0 * (q2.w - q1.w) + cx1 * (q3.w - q0.w);
+    pxn.x = xc.x * px.x + (xc.y * kk.x) * dx0;
+    pxn.y = xc.x * px.y + (xc.y * kk.y) * dx1;
+    pxn.z = xc.x * px.z + (xc.y * kk.z) * dx2;
+    pxn.w = xc.x * px.w + (xc.y * kk.w) * dx3;
+    pzn.x = ln.zc[0].x * pz.x + (ln.zc[0].y * kk.x) * dz0;
+    pzn.y = ln.zc[1].x * pz.y + (ln.zc[1].y * kk.y) * dz1;
+    pzn.z = ln.zc[2].x * pz.z + (ln.zc[2].y * kk.z) * dz2;
+    pzn.w = ln.zc[3].x * pz.w + (ln.zc[3].y * kk.w) * dz3;
+    if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
+        if (ln.sdz == 0) pxn.x += ln.amp;
+        else if (ln.sdz == 1) pxn.y += ln.amp;
+        else if (ln.sdz == 2) pxn.z += ln.amp;
+        else pxn.w += ln.amp;
+    }
+    return make_float4(pxn.x + pzn.x, pxn.y + pzn.y, pxn.z + pzn.z, pxn.w + pzn.w);
+}
 
-    for (int L = xa; L <= xb + 2; ++L) {
-        // ---- pressure at column P = L - 1 (p computed on [xa-1, xb+1]) ----
-        const int P = L - 1;
-        const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
-        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
-        vq0 = vq1; vq1 = vq2; vq2 = vq3;
-        vq3 = ld4(vxi + colL);
-        const float4 px = ld4(pxi + colP);
-        const float4 pz = ld4(pzi + colP);
-        const float4 kk = ld4(kap + colP);
-        const float4 vz = ld4(vzi + colP);
-        const float4 xcP = __ldg(S.xcoef + (P + S2D_GX));
-        float cx0, cx1;
-        dm_coef(P, nnx, cx0, cx1);
-
-        const float vz_up_z = __shfl_up_sync(kFull, vz.z, 1);
-        const float vz_up_w = __shfl_up_sync(kFull, vz.w, 1);
-        const float vz_dn_x = __shfl_down_sync(kFull, vz.x, 1);
-        const float dz0 = cm0[0] * (vz.x - vz_up_w) + cm1[0] * (vz.y - vz_up_z);
-        const float dz1 = cm0[1] * (vz.y - vz.x) + cm1[1] * (vz.z - vz_up_w);
-        const float dz2 = cm0[2] * (vz.z - vz.y) + cm1[2] * (vz.w - vz.x);
-        const float dz3 = cm0[3] * (vz.w - vz.z) + cm1[3] * (vz_dn_x - vz.y);
-        const float dx0 = cx0 * (vq2.x - vq1.x) + cx1 * (vq3.x - vq0.x);
-        const float dx1 = cx0 * (vq2.y - vq1.y) + cx1 * (vq3.y - vq0.y);
-        const float dx2 = cx0 * (vq2.z - vq1.z) + cx1 * (vq3.z - vq0.z);
-        const float dx3 = cx0 * (vq2.w - vq1.w) + cx1 * (vq3.w - vq0.w);
-
-        float4 pxn, pzn;
-        pxn.x = xcP.x * px.x + (xcP.y * kk.x) * dx0;
-        pxn.y = xcP.x * px.y + (xcP.y * kk.y) * dx1;
-        pxn.z = xcP.x * px.z + (xcP.y * kk.z) * dx2;
-        pxn.w = xcP.x * px.w + (xcP.y * kk.w) * dx3;
-        pzn.x = zc0.x * pz.x + (zc0.y * kk.x) * dz0;
-        pzn.y = zc1.x * pz.y + (zc1.y * kk.y) * dz1;
-        pzn.z = zc2.x * pz.z + (zc2.y * kk.z) * dz2;
-        pzn.w = zc3.x * pz.w + (zc3.y * kk.w) * dz3;
-        if (P == S.src_x && src_lane) {  // cpumodelling.cpp:136-140
-            if (sdz == 0) pxn.x += amp;
-            else if (sdz == 1) pxn.y += amp;
-            else if (sdz == 2) pxn.z += amp;
-            else pxn.w += amp;
-        }
-        const float4 pn = make_float4(pxn.x + pzn.x, pxn.y + pzn.y, pxn.z + pzn.z, pxn.w + pzn.w);
-        const bool in_seg_p = P >= xa && P < xb;
-        if (in_seg_p && owner) {
-            st4(pxo + colP, pxn);
-            st4(pzo + colP, pzn);
-        }
-        if (rec && in_seg_p) {
-            const int j1 = __ldg(S.rec_ptr + P + 1);
-            for (int j = __ldg(S.rec_ptr + P); j < j1; ++j) {
-                const int d = __ldg(S.rec_z + j) - z0;
-                if (owner && d >= 0 && d < 4)
-                    S.seis[(size_t)__ldg(S.rec_id + j) * S.real_nt + slot] = comp(pn, d);
-            }
-        }
-        pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
-        zq0 = zq1; zq1 = zq2; zq2 = vz;
-
-        // ---- velocity at column V = L - 3 ----
-        if (L >= xa + 3) {
-            const int V = L - 3;
-            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-            const float4 bx = ld4(bxp + colV);
-            const float4 bz = ld4(bzp + colV);
-            const float4 xcV = __ldg(S.xcoef + (V + S2D_GX));
-            float ux0, ux1;
-            dp_coef(V, nnx, ux0, ux1);
-            const float ex0 = ux0 * (pq2.x - pq1.x) + ux1 * (pq3.x - pq0.x);
-            const float ex1 = ux0 * (pq2.y - pq1.y) + ux1 * (pq3.y - pq0.y);
-            const float ex2 = ux0 * (pq2.z - pq1.z) + ux1 * (pq3.z - pq0.z);
-            const float ex3 = ux0 * (pq2.w - pq1.w) + ux1 * (pq3.w - pq0.w);
-            const float4 q = pq1;
-            const float q_up_w = __shfl_up_sync(kFull, q.w, 1);
-            const float q_dn_x = __shfl_down_sync(kFull, q.x, 1);
-            const float q_dn_y = __shfl_down_sync(kFull, q.y, 1);
-            const float ez0 = cp0[0] * (q.y - q.x) + cp1[0] * (q.z - q_up_w);
-            const float ez1 = cp0[1] * (q.z - q.y) + cp1[1] * (q.w - q.x);
-            const float ez2 = cp0[2] * (q.w - q.z) + cp1[2] * (q_dn_x - q.y);
-            const float ez3 = cp0[3] * (q_dn_x - q.w) + cp1[3] * (q_dn_y - q.z);
-            float4 vxn, vzn;
-            vxn.x = xcV.z * vq0.x + (xcV.w * bx.x) * ex0;
-            vxn.y = xcV.z * vq0.y + (xcV.w * bx.y) * ex1;
-            vxn.z = xcV.z * vq0.z + (xcV.w * bx.z) * ex2;
-            vxn.w = xcV.z * vq0.w + (xcV.w * bx.w) * ex3;
-            vzn.x = zc0.z * zq0.x + (zc0.w * bz.x) * ez0;
-            vzn.y = zc1.z * zq0.y + (zc1.w * bz.y) * ez1;
-            vzn.z = zc2.z * zq0.z + (zc2.w * bz.z) * ez2;
-            vzn.w = zc3.z * zq0.w + (zc3.w * bz.w) * ez3;
-            if (owner) {
-                st4(vxo + colV, vxn);
-                st4(vzo + colV, vzn);
-            }
-        }
+// Receiver sampling of new p at column P (cpumodelling.cpp:356-360).
+__device__ __forceinline__ void record(const Lane &ln, const ShotDev &S, int P, const float4 &pn, int slot) {
+    const int j1 = __ldg(S.rec_ptr + P + 1);
+    for (int j = __ldg(S.rec_ptr + P); j < j1; ++j) {
+        const int d = __ldg(S.rec_z + j) - ln.z0;
+        if (ln.owner && d >= 0 && d < 4) S.seis[(size_t)__ldg(S.rec_id + j) * S.real_nt + slot] = comp(pn, d);
     }
 }
 
-__global__ void __launch_bounds__(128) step_kernel(const StepArgs *__restrict__ A, int kt_off) {
+// Velocities at column V from new p at V-1..V+2 (p0..p3), old vx, vz at V and
+// bx, bz at V (cpu_modelling_kernels.cpp:260-316 and 353-368).
+__device__ __forceinline__ void v_update(const Lane &ln, const ShotDev &S, int V, const float4 &p0,
+                                         const float4 &p1, const float4 &p2, const float4 &p3, const float4 &vx,
+                                         const float4 &vz, const float4 &bx, const float4 &bz, float4 &vxn,
+                                         float4 &vzn) {
+    const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
+    float ux0, ux1;
+    dp_coef(V, S.nnx, ux0, ux1);
+    const float ex0 = ux0 * (p2.x - p1.x) + ux1 * (p3.x - p0.x);
+    const float ex1 = ux0 * (p2.y - p1.y) + ux1 * (p3.y - p0.y);
+    const float ex2 = ux0 * (p2.z - p1.z) + ux1 * (p3.z - p0.z);
+    const float ex3 = ux0 * (p2.w - p1.w) + ux1 * (p3.w - p0.w);
+    const float4 q = p1;
+    const float up_w = __shfl_up_sync(kFull, q.w, 1);
+    const float dn_x = __shfl_down_sync(kFull, q.x, 1);
+    const float dn_y = __shfl_down_sync(kFull, q.y, 1);
+    const float ez0 = ln.cp0[0] * (q.y - q.x) + ln.cp1[0] * (q.z - up_w);
+    const float ez1 = ln.cp0[1] * (q.z - q.y) + ln.cp1[1] * (q.w - q.x);
+    const float ez2 = ln.cp0[2] * (q.w - q.z) + ln.cp1[2] * (dn_x - q.y);
+    const float ez3 = ln.cp0[3] * (dn_x - q.w) + ln.cp1[3] * (dn_y - q.z);
+    vxn.x = xc.z * vx.x + (xc.w * bx.x) * ex0;
+    vxn.y = xc.z * vx.y + (xc.w * bx.y) * ex1;
+    vxn.z = xc.z * vx.z + (xc.w * bx.z) * ex2;
+    vxn.w = xc.z * vx.w + (xc.w * bx.w) * ex3;
+    vzn.x = ln.zc[0].z * vz.x + (ln.zc[0].w * bz.x) * ez0;
+    vzn.y = ln.zc[1].z * vz.y + (ln.zc[1].w * bz.y) * ez1;
+    vzn.z = ln.zc[2].z * vz.z + (ln.zc[2].w * bz.z) * ez2;
+    vzn.w = ln.zc[3].z * vz.w + (ln.zc[3].w * bz.w) * ez3;
+}
+
+// Map a flat task index to (shot, strip, first column, segment length).
+// Order 0 runs the shots of one (strip, segment) on consecutive warps, so they
+// share that tile of the model through L2.  Order 1 runs the strips of one
+// (shot, segment) on consecutive warps, so the warps of a block read adjacent
+// pieces of each column (contiguous DRAM rows); the shots of one segment still
+// run close together and share the segment's materials in L2.
+__device__ __forceinline__ const ShotDev &task_of(const StepArgs &a, int t, int &strip, int &xa, int &seg_len) {
+    int g = 0;
+    while (g + 1 < a.ngroups && __ldg(&a.groups[g + 1].task_begin) <= t) ++g;
+    const GroupDev &G = a.groups[g];
+    int tl = t - G.task_begin;
+    int s;
+    if (a.task_order == 0) {
+        s = G.shot0 + tl % G.nshots;
+        tl /= G.nshots;
+        strip = tl % G.nstrips;
+        xa = (tl / G.nstrips) * G.seg_len;
+    } else {
+        strip = tl % G.nstrips;
+        tl /= G.nstrips;
+        s = G.shot0 + tl % G.nshots;
+        xa = (tl / G.nshots) * G.seg_len;
+    }
+    seg_len = G.seg_len;
+    return a.shots[s];
+}
+
+// ---------------------------------------------------------------- LDG variant
+
+__global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -207,19 +204,237 @@ __global__ void __launch_bounds__(128) step_kernel(const StepArgs *__restrict__ 
     const int kt = a.kt_base + kt_off;
     if (kt >= a.fd_nt) return;
     const int par = kt & 1;
-    const bool rec = ((kt + 1) % a.dt_factor) == 0;
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
-        int g = 0;
-        while (g + 1 < a.ngroups && __ldg(&a.groups[g + 1].task_begin) <= t) ++g;
-        const GroupDev &G = a.groups[g];
-        int tl = t - G.task_begin;
-        const int s = G.shot0 + tl % G.nshots;
-        tl /= G.nshots;
-        const int strip = tl % G.nstrips;
-        const int seg = tl / G.nstrips;
-        const ShotDev &S = a.shots[s];
-        run_task(S, strip, seg * G.seg_len, G.seg_len, kt, par, rec && slot < S.real_nt, slot, lane);
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const int xb = min(S.nnx, xa + seg_len);
+        const size_t ld = (size_t)S.ld;
+        const int c = strip * S2D_STRIP_OUT - 4;
+        Lane ln;
+        lane_setup(ln, S, c, lane, kt);
+        const bool rec = rec_step && slot < S.real_nt;
+        const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+        const float *pxi = S.st[par][0] + off, *pzi = S.st[par][1] + off;
+        const float *vxi = S.st[par][2] + off, *vzi = S.st[par][3] + off;
+        float *pxo = S.st[par ^ 1][0] + off, *pzo = S.st[par ^ 1][1] + off;
+        float *vxo = S.st[par ^ 1][2] + off, *vzo = S.st[par ^ 1][3] + off;
+        const float *kap = S.kappa + off, *bxp = S.bx + off, *bzp = S.bz + off;
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 vq0 = zero, vq1, vq2, vq3;
+        float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+        float4 zq0 = zero, zq1 = zero, zq2 = zero;
+        vq1 = ld4(vxi + (ptrdiff_t)(xa - 3) * (ptrdiff_t)ld);
+        vq2 = ld4(vxi + (ptrdiff_t)(xa - 2) * (ptrdiff_t)ld);
+        vq3 = ld4(vxi + (ptrdiff_t)(xa - 1) * (ptrdiff_t)ld);
+        for (int L = xa; L <= xb + 2; ++L) {
+            const int P = L - 1;
+            const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+            vq0 = vq1; vq1 = vq2; vq2 = vq3;
+            vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
+            const float4 vz = ld4(vzi + colP);
+            float4 pxn, pzn;
+            const float4 pn = p_update(ln, S, P, vq0, vq1, vq2, vq3, ld4(pxi + colP), ld4(pzi + colP),
+                                       ld4(kap + colP), vz, pxn, pzn);
+            const bool in_seg = P >= xa && P < xb;
+            if (in_seg && ln.owner) {
+                st4(pxo + colP, pxn);
+                st4(pzo + colP, pzn);
+            }
+            if (rec && in_seg) record(ln, S, P, pn, slot);
+            pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+            zq0 = zq1; zq1 = zq2; zq2 = vz;
+            if (L >= xa + 3) {
+                const int V = L - 3;
+                const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+                float4 vxn, vzn;
+                v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+                if (ln.owner) {
+                    st4(vxo + colV, vxn);
+                    st4(vzo + colV, vzn);
+                }
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------- bulk variant
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Bounded wait: every lane polls; the warp agrees on the outcome.
+__device__ __forceinline__ bool wait_stage(uint64_t *bar, unsigned parity, int limit) {
+    bool ok = false;
+    for (int i = 0; i < limit && !ok; ++i) ok = mbar_try_wait(bar, parity);
+    return __all_sync(kFull, ok);
+}
+
+constexpr int kDrainLimit = 1 << 20;
+
+// MINB = 1 lets the compiler use the registers it wants (about 160, 3 blocks
+// per SM); MINB = 4 caps it at 128 (4 blocks per SM, a few bytes of spill).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base + kt_off;
+    if (kt >= a.fd_nt) return;
+    // an earlier launch of this sequence gave up: its wavefields are not valid
+    if (*reinterpret_cast<volatile int *>(a.err) != 0) return;
+    const int S = a.stages;
+    const int drain_limit = a.spin_limit < kDrainLimit / 64 ? a.spin_limit * 64 : kDrainLimit;
+    unsigned char *ring = smem + (size_t)wib * S * kStageBytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)wpb * S * kStageBytes) + wib * S;
+    if (lane == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    const int par = kt & 1;
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    unsigned it0 = 0;  // pipeline iterations consumed by this warp so far
+
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S_ = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &Sh = S_;
+        const int xb = min(Sh.nnx, xa + seg_len);
+        const size_t ld = (size_t)Sh.ld;
+        const int c = strip * S2D_STRIP_OUT - 4;
+        Lane ln;
+        lane_setup(ln, Sh, c, lane, kt);
+        const bool rec = rec_step && slot < Sh.real_nt;
+        // column 0 of the warp's strip in each field (row c), and this lane's rows
+        const size_t wofs = (size_t)(c + S2D_GZ) + (size_t)S2D_GX * ld;
+        const size_t lofs = wofs + (size_t)(S2D_ZPT * lane);
+        const float *src_vx = Sh.st[par][2] + wofs, *src_px = Sh.st[par][0] + wofs;
+        const float *src_pz = Sh.st[par][1] + wofs, *src_vz = Sh.st[par][3] + wofs;
+        const float *src_k = Sh.kappa + wofs, *src_bx = Sh.bx + wofs, *src_bz = Sh.bz + wofs;
+        float *pxo = Sh.st[par ^ 1][0] + lofs, *pzo = Sh.st[par ^ 1][1] + lofs;
+        float *vxo = Sh.st[par ^ 1][2] + lofs, *vzo = Sh.st[par ^ 1][3] + lofs;
+        const int n_it = xb - xa + 6;  // columns L = xa-3 .. xb+2
+
+        // Producer (lane 0): bring iteration j's columns into stage (it0+j) % S.
+        auto issue = [&](int j) {
+            const unsigned itj = it0 + (unsigned)j;
+            const int s = (int)(itj % (unsigned)S);
+            unsigned char *st = ring + (size_t)s * kStageBytes;
+            const int L = xa - 3 + j;
+            const bool pp = L >= xa, vv = L >= xa + 3;
+            mbar_expect_tx(&bars[s], (unsigned)kSlotBytes * (1u + (pp ? 4u : 0u) + (vv ? 2u : 0u)));
+            if (j == a.fault_iter) return;  // test knob: the stage's bytes never arrive
+            bulk_copy(st, src_vx + (ptrdiff_t)L * (ptrdiff_t)ld, kSlotBytes, &bars[s]);
+            if (pp) {
+                const ptrdiff_t cp = (ptrdiff_t)(L - 1) * (ptrdiff_t)ld;
+                bulk_copy(st + 1 * kSlotBytes, src_px + cp, kSlotBytes, &bars[s]);
+                bulk_copy(st + 2 * kSlotBytes, src_pz + cp, kSlotBytes, &bars[s]);
+                bulk_copy(st + 3 * kSlotBytes, src_k + cp, kSlotBytes, &bars[s]);
+                bulk_copy(st + 4 * kSlotBytes, src_vz + cp, kSlotBytes, &bars[s]);
+            }
+            if (vv) {
+                const ptrdiff_t cv = (ptrdiff_t)(L - 3) * (ptrdiff_t)ld;
+                bulk_copy(st + 5 * kSlotBytes, src_bx + cv, kSlotBytes, &bars[s]);
+                bulk_copy(st + 6 * kSlotBytes, src_bz + cv, kSlotBytes, &bars[s]);
+            }
+        };
+        if (lane == 0) {
+            const int pre = min(S, n_it);
+            for (int j = 0; j < pre; ++j) issue(j);
+        }
+
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 vq0 = zero, vq1 = zero, vq2 = zero, vq3 = zero;
+        float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+        float4 zq0 = zero, zq1 = zero, zq2 = zero;
+        for (int j = 0; j < n_it; ++j) {
+            const unsigned itj = it0 + (unsigned)j;
+            const int s = (int)(itj % (unsigned)S);
+            if (!wait_stage(&bars[s], (itj / (unsigned)S) & 1u, a.spin_limit)) {
+                // Give up: record the error, let the copies already issued
+                // land (bounded), and leave without touching global state.
+                if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_WAIT);
+                const int last = min(n_it, j + S);
+                for (int k = j; k < last; ++k) {
+                    const unsigned itk = it0 + (unsigned)k;
+                    if (!wait_stage(&bars[itk % (unsigned)S], (itk / (unsigned)S) & 1u, drain_limit)) {
+                        if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_DRAIN);
+                    }
+                }
+                return;
+            }
+            const float4 *st = reinterpret_cast<const float4 *>(ring + (size_t)s * kStageBytes) + lane;
+            const int L = xa - 3 + j;
+            vq0 = vq1; vq1 = vq2; vq2 = vq3;
+            vq3 = st[0 * 32];
+            if (L >= xa) {
+                const int P = L - 1;
+                const float4 vz = st[4 * 32];
+                float4 pxn, pzn;
+                const float4 pn = p_update(ln, Sh, P, vq0, vq1, vq2, vq3, st[1 * 32], st[2 * 32], st[3 * 32], vz,
+                                           pxn, pzn);
+                const bool in_seg = P >= xa && P < xb;
+                const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+                if (in_seg && ln.owner) {
+                    st4(pxo + colP, pxn);
+                    st4(pzo + colP, pzn);
+                }
+                if (rec && in_seg) record(ln, Sh, P, pn, slot);
+                pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+                zq0 = zq1; zq1 = zq2; zq2 = vz;
+                if (L >= xa + 3) {
+                    const int V = L - 3;
+                    const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+                    float4 vxn, vzn;
+                    v_update(ln, Sh, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn);
+                    if (ln.owner) {
+                        st4(vxo + colV, vxn);
+                        st4(vzo + colV, vzn);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && j + S < n_it) {
+                fence_proxy_async();
+                issue(j + S);
+            }
+        }
+        it0 += (unsigned)n_it;
     }
 }
 
@@ -266,8 +481,14 @@ __global__ void set_args_kernel(StepArgs v, StepArgs *dst) { *dst = v; }
 
 }  // namespace
 
-int launch_step(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream) {
-    step_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int block, size_t smem,
+                void *stream) {
+    if (variant == kVariantBulk)
+        step_kernel_bulk<1><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantBulk128)
+        step_kernel_bulk<4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else
+        step_kernel_ldg<<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
@@ -285,13 +506,30 @@ int launch_prepare_model(const float *vp, const float *rho, int nx, int nz, int 
     return (int)cudaGetLastError();
 }
 
-int step_kernel_occupancy(int block, int *blocks_per_sm) {
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel, block, 0);
+namespace {
+const void *kernel_of(int variant) {
+    if (variant == kVariantBulk) return (const void *)step_kernel_bulk<1>;
+    if (variant == kVariantBulk128) return (const void *)step_kernel_bulk<4>;
+    return (const void *)step_kernel_ldg;
+}
+}  // namespace
+
+int step_kernel_prepare(int variant, size_t smem) {
+    if (variant == kVariantLdg) return 0;
+    const void *k = kernel_of(variant);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return (int)e;
 }
 
-int step_kernel_attributes(int *regs, int *local_bytes) {
+int step_kernel_occupancy(int variant, int block, size_t smem, int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block,
+                                                              variant == kVariantLdg ? 0 : smem);
+}
+
+int step_kernel_attributes(int variant, int *regs, int *local_bytes) {
     cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, step_kernel);
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel_of(variant));
     if (e != cudaSuccess) return (int)e;
     *regs = fa.numRegs;
     *local_bytes = (int)fa.localSizeBytes;

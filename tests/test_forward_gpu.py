@@ -40,12 +40,20 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_golden_parity(ctx, name):
+def test_golden_parity(ctx, name, variant):
     from seis2d_b200 import Shot
     z, c, vp, rho = _golden(name)
+    ctx.set_option("variant", VARIANTS[variant])
     m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
-    seis = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
+    try:
+        seis = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
+    finally:
+        ctx.set_option("variant", 1)
     ref = z["seis"]
     assert seis.shape == ref.shape
     err = O.rel_l2(seis, ref)
@@ -170,3 +178,61 @@ def test_errors_are_statuses(ctx):
     # context still usable after errors
     s = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
     assert O.rel_l2(s, z["seis"]) <= TOL
+
+
+@pytest.mark.parametrize("stages,block,seg_len,order", [(2, 32, 16, 0), (3, 64, 24, 1), (8, 128, 0, 0),
+                                                        (4, 96, 37, 1)])
+def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
+    """Pipeline depth, block size and segment length change the schedule,
+    never the numbers."""
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("layers_endonright_near_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    shot = [Shot(m, tuple(z["src"]), z["rec"])]
+    base = ctx.forward(shot, _wave(c))[0]
+    try:
+        ctx.set_option("stages", stages)
+        ctx.set_option("block", block)
+        ctx.set_option("seg_len", seg_len)
+        ctx.set_option("task_order", order)
+        got = ctx.forward(shot, _wave(c))[0]
+    finally:
+        ctx.set_option("stages", 5)
+        ctx.set_option("block", 128)
+        ctx.set_option("seg_len", 0)
+        ctx.set_option("task_order", 1)
+    np.testing.assert_array_equal(got, base)
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(ctx):
+    """A pipeline barrier whose bytes never arrive: every wait is bounded, the
+    kernel records the error and returns, the call reports S2D_ERR_TIMEOUT and
+    the next call on the same context is correct."""
+    from seis2d_b200 import Shot
+    from seis2d_b200._lib import Seis2dError, S2D_ERR_TIMEOUT
+    z, c, vp, rho = _golden("edges_explicit_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    shot = [Shot(m, tuple(z["src"]), z["rec"])]
+    ctx.set_option("variant", 0)
+    ctx.set_option("spin_limit", 256)
+    ctx.set_option("inject_wait_fault", 1)
+    try:
+        with pytest.raises(Seis2dError) as e:
+            ctx.forward(shot, _wave(c))
+        assert e.value.code == S2D_ERR_TIMEOUT
+    finally:
+        ctx.set_option("inject_wait_fault", -1)
+        ctx.set_option("spin_limit", 1 << 20)
+        ctx.set_option("variant", 1)
+    good = ctx.forward(shot, _wave(c))[0]
+    assert O.rel_l2(good, z["seis"]) <= TOL
+
+
+def test_unknown_option_rejected(ctx):
+    from seis2d_b200._lib import Seis2dError
+    with pytest.raises(Seis2dError):
+        ctx.set_option("no_such_knob", 1)
+    with pytest.raises(Seis2dError):
+        ctx.set_option("stages", 1)
+    with pytest.raises(Seis2dError):
+        ctx.set_option("block", 256)
