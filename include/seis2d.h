@@ -190,6 +190,47 @@ S2D_API int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_
                 const double *wavelet, int nwavelet, int kt_begin, int kt_count,
                 float *seis_out, unsigned flags, s2d_stats *stats);
 
+/* ---- forward modelling without device allocation ----------------------------- */
+
+/* Size of the device scratch s2d_forward_static works in (32 MiB). */
+#define S2D_STATIC_SCRATCH_BYTES (32u << 20)
+
+/*
+ * One shot of forward modelling that allocates no device memory.  No
+ * counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc when they want a shot modelled: a
+ * service that reserves its device memory at start-up and forbids allocation
+ * afterwards, a program whose own allocator already holds the device memory,
+ * or a latency-critical loop that cannot afford the device-wide
+ * synchronisation cudaMalloc/cudaFree cause.  The wavefields, materials,
+ * tables and staging copies live in a static device array of
+ * S2D_STATIC_SCRATCH_BYTES that every GPU loading this library holds until the
+ * process exits -- enough for a padded grid of roughly 800 x 800 cells.  A job
+ * that needs more returns S2D_ERR_NOMEM with the size it needs in errbuf.
+ *
+ * Same scheme, numbers and output layout as s2d_forward for one shot with the
+ * reference Ricker wavelet: model [nx][nz] (vp, rho), sponge width nb, wave,
+ * shot->src and shot->rec (shot->model_id is ignored), seis_out
+ * [nrec][real_nt].  flags: S2D_MODEL_DEVICE (vp, rho are device pointers),
+ * S2D_SEIS_DEVICE (seis_out is a device pointer); otherwise host pointers.
+ * stream: a cudaStream_t, NULL for the legacy default stream; the call returns
+ * when the shot is done.  errbuf (optional, errlen bytes) receives a message
+ * on failure.
+ *
+ * Every call on a device shares the one scratch array, which keeps the last
+ * call's contents; each call clears what must start at zero.  Calls whose
+ * device work overlaps on one GPU (several threads or streams at once) race
+ * on the array: serialise them.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress, with that device current)
+ * and may load the library's device code; make it before starting any stream
+ * capture on that device.
+ */
+S2D_API int s2d_forward_static(int device, int nx, int nz, float dx, float dz, int nb,
+                               const float *vp, const float *rho, const s2d_wave *wave,
+                               const s2d_shot *shot, float *seis_out, unsigned flags,
+                               void *stream, char *errbuf, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,9 @@ SIGNATURES = {
     "s2d_model_destroy": ([C.c_void_p, C.c_int], C.c_int),
     "s2d_forward": ([C.c_void_p, C.POINTER(Shot), C.c_int, C.POINTER(Wave), C.POINTER(C.c_double), C.c_int,
                      C.c_int, C.c_int, C.c_void_p, C.c_uint, C.POINTER(Stats)], C.c_int),
+    "s2d_forward_static": ([C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p,
+                            C.POINTER(Wave), C.POINTER(Shot), C.c_void_p, C.c_uint, C.c_void_p, C.c_char_p,
+                            C.c_size_t], C.c_int),
 }
 
 _lib = None
