@@ -190,6 +190,64 @@ S2D_API int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_
                 const double *wavelet, int nwavelet, int kt_begin, int kt_count,
                 float *seis_out, unsigned flags, s2d_stats *stats);
 
+/* ---- host driver: the reference's files ----------------------------------------- */
+
+/* Parsed job card: the fields of mod_t, wave_t and job_t the reference fills
+ * from it (src/src_cpu/modelling.h:13-61, json_parser.cpp:122-300). */
+typedef struct {
+    char velfile[224], densfile[224];
+    int nx, nz;
+    float dx, dz;
+    s2d_wave wave;
+    int geomflag;          /* 0: explicit geometry file, 1: shot file */
+    int frsf;              /* free-surface flag (parsed, not implemented, as in the reference) */
+    int fdop;              /* FD order (only 4 exists) */
+    char jbtype[8];        /* "New" or "Restart" */
+    char shotfile[224], geomfile[224];
+    char jobname[256];     /* card basename without extension + "_" */
+    char tmppath[512];     /* output directory, with trailing '/' */
+} s2d_jobcard;
+
+/* Source/receiver geometry of all shots (geo2d_t, src/src_cpu/modelling.h:40-45). */
+typedef struct {
+    int nsrc;
+    int *nrec;             /* [nsrc] */
+    s2d_coord *src;        /* [nsrc] */
+    s2d_coord **rec;       /* [nsrc][nrec[s]] */
+} s2d_geometry;
+
+/* Read a job card (json_parser.cpp:13-300).  Host only.  On failure errbuf
+ * (errlen bytes, optional) names the problem and the reference's abort code. */
+S2D_API int s2d_jobcard_read(const char *path, s2d_jobcard *out, char *errbuf, size_t errlen);
+
+/* Build the geometry the card names: shot file with split / end-on-left /
+ * end-on-right spreads (create_geometry.cpp:15-444) or explicit sx,sz,gx,gz
+ * file (read_receiver.cpp:14-306).  Host only.  Free with s2d_geometry_free. */
+S2D_API int s2d_geometry_read(const s2d_jobcard *job, s2d_geometry *out, char *errbuf, size_t errlen);
+S2D_API void s2d_geometry_free(s2d_geometry *geometry);
+
+/* Stability (dt <= 0.606 h_min / v_max) and dispersion (2 f <= v_min / (5 h_max))
+ * criteria of check_stability.cpp:8-72.  Host only. */
+S2D_API int s2d_check_stability(const s2d_jobcard *job, float vmin, float vmax, char *errbuf, size_t errlen);
+
+/*
+ * Run the whole job of a card on `device`: read card, geometry and models
+ * (model.cpp:12-64), check stability (skipped when check_stability == 0),
+ * model every shot (batched, as many per launch as fit in device memory) and
+ * write each seismogram, [nrec][real_nt] float32.  Replaces Modelling_master +
+ * modelling_module (modelling_master.cpp:10-92, cpumodelling.cpp:158-383).
+ *   nb      sponge width (32 in the reference)
+ *   naming  0: <outdir>/<jobname>seismogram.bin, the CPU backend's single file
+ *              (cpumodelling.cpp:370-374; every shot writes it, the last wins)
+ *           1: <outdir>/<jobname>sx<%.2f>_seismogram.bin per shot, the CUDA
+ *              backend's names (gpumodelling.cu:471-477)
+ * "Job type" Restart skips the shots before the index in
+ * <outdir>/<jobname>checkpoint_rank0.txt (cpumodelling.cpp:294-321); unlike
+ * the reference, this driver writes that file after every completed shot.
+ */
+S2D_API int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming,
+                            int check_stability, int verbose, char *errbuf, size_t errlen);
+
 /* ---- forward modelling without device allocation ----------------------------- */
 
 /* Size of the device scratch s2d_forward_static works in (32 MiB). */

@@ -46,6 +46,19 @@ class Steps(C.Structure):
     _fields_ = [("fd_nt", C.c_int), ("real_nt", C.c_int), ("dt_factor", C.c_int), ("nts", C.c_int)]
 
 
+class JobCard(C.Structure):
+    """s2d_jobcard: the fields the reference fills from a job card."""
+    _fields_ = [("velfile", C.c_char * 224), ("densfile", C.c_char * 224), ("nx", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_float), ("dz", C.c_float), ("wave", Wave), ("geomflag", C.c_int), ("frsf", C.c_int),
+                ("fdop", C.c_int), ("jbtype", C.c_char * 8), ("shotfile", C.c_char * 224),
+                ("geomfile", C.c_char * 224), ("jobname", C.c_char * 256), ("tmppath", C.c_char * 512)]
+
+
+class Geometry(C.Structure):
+    _fields_ = [("nsrc", C.c_int), ("nrec", C.POINTER(C.c_int)), ("src", C.POINTER(Coord)),
+                ("rec", C.POINTER(C.POINTER(Coord)))]
+
+
 class Stats(C.Structure):
     _fields_ = [("loop_ms", C.c_double), ("cell_updates", C.c_double), ("gcells_per_s", C.c_double),
                 ("kernel_launches", C.c_int), ("graph_used", C.c_int)]
@@ -64,6 +77,12 @@ SIGNATURES = {
     "s2d_model_destroy": ([C.c_void_p, C.c_int], C.c_int),
     "s2d_forward": ([C.c_void_p, C.POINTER(Shot), C.c_int, C.POINTER(Wave), C.POINTER(C.c_double), C.c_int,
                      C.c_int, C.c_int, C.c_void_p, C.c_uint, C.POINTER(Stats)], C.c_int),
+    "s2d_jobcard_read": ([C.c_char_p, C.POINTER(JobCard), C.c_char_p, C.c_size_t], C.c_int),
+    "s2d_geometry_read": ([C.POINTER(JobCard), C.POINTER(Geometry), C.c_char_p, C.c_size_t], C.c_int),
+    "s2d_geometry_free": ([C.POINTER(Geometry)], None),
+    "s2d_check_stability": ([C.POINTER(JobCard), C.c_float, C.c_float, C.c_char_p, C.c_size_t], C.c_int),
+    "s2d_run_jobcard": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
+                        C.c_int),
     "s2d_forward_static": ([C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p,
                             C.POINTER(Wave), C.POINTER(Shot), C.c_void_p, C.c_uint, C.c_void_p, C.c_char_p,
                             C.c_size_t], C.c_int),

@@ -18,6 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libseis2d.so")
+CLI_SRC = os.path.join(HERE, "cli", "seis2d_run.cpp")
+CLI = os.path.join(HERE, "bin", "seis2d_run")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,10 +40,10 @@ def sources():
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    deps = sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h")) + [CLI_SRC]
     return any(os.path.getmtime(p) > t for p in deps)
 
 
@@ -73,6 +75,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(LIB + ".tmp", LIB)
+    # command-line driver, linked against the library by rpath
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    cmd = [_host_cxx(), "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI,
+           "-L", HERE, "-lseis2d", "-Wl,-rpath,$ORIGIN/.."]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"seis2d_run link failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

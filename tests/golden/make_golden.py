@@ -15,6 +15,7 @@ NB=<nb>`` whose only change is the npml constant) on each case of
 Needs the reference tree (to build the binary), so it runs in the development
 container; the committed .npz files are what the tests use everywhere.
 Usage: python tests/golden/make_golden.py [case ...]
+       python tests/golden/make_golden.py --geometry   (geometry_cases.json)
 """
 from __future__ import annotations
 
@@ -83,7 +84,58 @@ def run_case(name: str, c: dict) -> dict:
             "max_abs": float(np.abs(seis).max()), "bytes": os.path.getsize(out)}
 
 
+# Shot-file spreads whose receiver lists the reference builds
+# (create_geometry.cpp:237-444), each run as a one-shot job of one FD step so
+# that print_single_source_geometry (create_geometry.cpp:446-459) writes them.
+# Split spreads with a near offset are left out: the reference writes one
+# receiver past the end of its array for every such shot.
+GEOMETRY_CASES = [
+    # (nx, nz, dx, dz, sx, sz, nrec, nearoff, spacing, type)
+    (200, 40, 10.0, 10.0, 1000.0, 20.0, 81, 0, 10.0, 1),     # split, room on both sides
+    (200, 40, 10.0, 10.0, 100.0, 20.0, 80, 0, 10.0, 1),      # split, short on the left
+    (200, 40, 10.0, 10.0, 1900.0, 0.0, 80, 0, 20.0, 1),      # split, short on the right
+    (200, 40, 10.0, 10.0, 1500.0, 10.0, 100, 0, 10.0, 2),    # end-on left
+    (200, 40, 10.0, 10.0, 1500.0, 10.0, 60, 30.0, 20.0, 2),  # end-on left, near offset
+    (200, 40, 10.0, 10.0, 200.0, 30.0, 120, 0, 10.0, 3),     # end-on right
+    (200, 40, 10.0, 10.0, 200.0, 30.0, 50, 10.0, 30.0, 3),   # end-on right, near offset
+    (600, 40, 7.62, 7.62, 2286.0, 15.24, 101, 0, 15.24, 1),  # non-integer spacing (float drift)
+    (600, 40, 7.62, 7.62, 3048.0, 7.62, 151, 0, 7.62, 2),
+    (600, 40, 7.62, 7.62, 762.0, 0.0, 151, 0, 22.86, 3),
+]
+
+
+def run_geometry_cases():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref")
+    out = []
+    for (nx, nz, dx, dz, sx, sz, nrec, near, sp, gt) in GEOMETRY_CASES:
+        with tempfile.TemporaryDirectory() as wd:
+            m = np.full((nx, nz), 2000.0, np.float32)
+            F.write_model(os.path.join(wd, "vp.bin"), m)
+            F.write_model(os.path.join(wd, "rho.bin"), m)
+            F.write_shotfile(os.path.join(wd, "shots.txt"), [(sx, sz, nrec, near, sp, gt)])
+            F.write_jobcard(os.path.join(wd, "g.json"), {
+                "Velocity": "vp.bin", "Density": "rho.bin", "NX": nx, "NZ": nz, "DX": dx, "DZ": dz,
+                "Time": 0.001, "FD DT": 0.001, "DATA DT": 0.001, "Frequency": 5.0,
+                "Read source receiver flag": 1, "if choice=0, Geometry file": "NA",
+                "if choice=1, Shot file": "shots.txt", "Output Directory": "out", "Free surface": 0,
+                "Job type New or Restart": "New", "Order of FD Operator": 4})
+            os.makedirs(os.path.join(wd, "out"))
+            r = subprocess.run([binary, "--no-stability", "g.json"], cwd=wd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"geometry case {sx},{gt}: reference exited {r.returncode}")
+            shotfile = open(os.path.join(wd, "shots.txt")).read()
+            printed = open(os.path.join(wd, "test_geometry.txt")).read()
+        out.append({"nx": nx, "nz": nz, "dx": dx, "dz": dz, "shotfile": shotfile, "test_geometry": printed})
+    with open(os.path.join(HERE, "geometry_cases.json"), "w") as f:
+        json.dump(out, f, indent=0)
+    return len(out)
+
+
 def main(argv):
+    if argv == ["--geometry"]:
+        print(json.dumps({"geometry_cases": run_geometry_cases()}))
+        return
     names = argv or list(CASES)
     for n in names:
         print(json.dumps(run_case(n, CASES[n])))
