@@ -63,6 +63,10 @@ extern "C" {
 #define S2D_NO_GRAPH 0x4u      /* launch the time loop step by step            */
 #define S2D_SYNC 0x8u          /* return only when device work has finished    */
 
+/* flags for s2d_gradient (with S2D_SEIS_DEVICE for data / seis_out, S2D_NO_GRAPH) */
+#define S2D_GRAD_MISFIT 0x10u  /* data is observed seismograms: adjoint source = d - data  */
+#define S2D_GRAD_DEVICE 0x20u  /* grad_vp, grad_rho are device pointers                    */
+
 /* flags for s2d_model_create */
 #define S2D_MODEL_DEVICE 0x1u  /* vp and rho are device pointers               */
 
@@ -104,6 +108,7 @@ typedef struct {
     double gcells_per_s;     /* cell_updates / loop_ms                        */
     int kernel_launches;     /* launches of the library's own kernels         */
     int graph_used;          /* 1 if the loop ran as a CUDA graph             */
+    int grad_segment;        /* s2d_gradient: checkpoint interval used (steps) */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */
@@ -132,6 +137,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *   "seg_len"     columns per x-segment of a warp task, 0 = automatic
  *   "spin_limit"  polls of a pipeline barrier before the wait gives up and the
  *                 call returns S2D_ERR_TIMEOUT (default 2^20)
+ *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
+ *                 longest that fits in free device memory (default)
  *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of
  *                 that pipeline iteration of its first task, so its bounded
  *                 wait runs out (no fault, no hang); -1 (default) disables
@@ -189,6 +196,36 @@ S2D_API int s2d_model_destroy(void *ctx, int model_id);
 S2D_API int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wave,
                 const double *wavelet, int nwavelet, int kt_begin, int kt_count,
                 float *seis_out, unsigned flags, s2d_stats *stats);
+
+/* ---- FWI gradient ----------------------------------------------------------------- */
+
+/*
+ * Gradient of a seismogram objective with respect to vp and rho of one model,
+ * summed over `nshots` shots that all use that model.  No counterpart in the
+ * reference (its job_t::adj flag is declared and never used,
+ * src/src_cpu/modelling.h:51).  It is the exact discrete adjoint of the FP32
+ * forward of s2d_forward: a forward sweep saving the wavefields every
+ * `grad_segment` steps, then, segment by segment backwards, a forward
+ * recompute that keeps the step derivatives and the adjoint time steps
+ * (transposed 4th-order operators, sponge and edge rows included) with the
+ * imaging terms for kappa = vp^2 rho, the staggered buoyancies and the
+ * kappa-scaled source; the chain rule to vp, rho and the fold of the sponge onto
+ * the model edge cells it replicates finish it.
+ *
+ *   data      without S2D_GRAD_MISFIT: dJ/d(seis), the adjoint source, same
+ *             layout as s2d_forward's seis_out (nshots blocks [nrec][real_nt]);
+ *             with S2D_GRAD_MISFIT: observed seismograms, J = 0.5 ||d - data||^2
+ *   grad_vp, grad_rho   [nx][nz] of the model, overwritten
+ *   seis_out  optional: the forward seismograms
+ *   misfit    optional: J (S2D_GRAD_MISFIT)
+ *   grad_wavelet  optional host array [nshots][fd_nt]: dJ/dw[kt], the gradient
+ *             with respect to the source samples (0 where no sample is injected)
+ *   flags     S2D_GRAD_MISFIT, S2D_GRAD_DEVICE, S2D_SEIS_DEVICE, S2D_NO_GRAPH
+ */
+S2D_API int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wave,
+                         const double *wavelet, int nwavelet, const float *data,
+                         float *grad_vp, float *grad_rho, float *seis_out, double *misfit,
+                         double *grad_wavelet, unsigned flags, s2d_stats *stats);
 
 /* ---- host driver: the reference's files ----------------------------------------- */
 

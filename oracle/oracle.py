@@ -60,6 +60,11 @@ def lib():
             C.c_float, C.c_float, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
             C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]
         L.orc_forward.restype = C.c_int
+        dp = C.POINTER(C.c_double)
+        L.orc_gradient.argtypes = [
+            C.POINTER(_Params), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int,
+            C.POINTER(C.c_float), C.POINTER(C.c_float), dp, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.orc_gradient.restype = C.c_int
         _lib = L
     return _lib
 
@@ -133,6 +138,38 @@ def forward(p: Params, vp: np.ndarray, rho: np.ndarray, src: Sequence[float],
     if want_state:
         return seis, tuple(state[i] for i in range(5))
     return seis
+
+
+def gradient(p: Params, vp: np.ndarray, rho: np.ndarray, src, rec_x, rec_z, adj: Optional[np.ndarray],
+             wavelet: Optional[np.ndarray] = None):
+    """FP64 discrete adjoint of the FP64 forward.  Returns a dict with
+    grad_vp, grad_rho ([nx][nz]), grad_kappa, grad_bx, grad_bz ([nnx][nnz]),
+    src_adj ([fd_nt]) and seis64 ([nrec][real_nt])."""
+    vp = np.ascontiguousarray(vp, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    gx = np.ascontiguousarray(rec_x, np.float32)
+    gz = np.ascontiguousarray(rec_z, np.float32)
+    d = derive(p)
+    nnx, nnz, nt = d["nnx"], d["nnz"], d["fd_nt"]
+    out = {"grad_vp": np.zeros((p.nx, p.nz)), "grad_rho": np.zeros((p.nx, p.nz)),
+           "grad_kappa": np.zeros((nnx, nnz)), "grad_bx": np.zeros((nnx, nnz)), "grad_bz": np.zeros((nnx, nnz)),
+           "src_adj": np.zeros(nt), "seis64": np.zeros((gx.size, d["real_nt"]))}
+    dpp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    wp, nw = None, 0
+    if wavelet is not None:
+        wavelet = np.ascontiguousarray(wavelet, np.float64)
+        wp, nw = dpp(wavelet), wavelet.size
+    a = None
+    if adj is not None:
+        a = np.ascontiguousarray(adj, np.float64)
+        assert a.shape == (gx.size, d["real_nt"])
+    rc = lib().orc_gradient(C.byref(p.c()), _fp(vp), _fp(rho), float(src[0]), float(src[1]), gx.size, _fp(gx),
+                            _fp(gz), wp, nw, dpp(a) if a is not None else None,
+                            *(dpp(out[k]) for k in ("grad_vp", "grad_rho", "grad_kappa", "grad_bx", "grad_bz",
+                                                    "src_adj", "seis64")))
+    if rc != 0:
+        raise ValueError(f"orc_gradient failed with status {rc}")
+    return out
 
 
 def ref_binary(nb: int = 32) -> str:

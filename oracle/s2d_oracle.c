@@ -447,3 +447,322 @@ bad_pos:
     free(damp1a); free(damp1a1); free(damp1b); free(damp1b1);
     return -3;
 }
+
+/* ------------------------- FP64 discrete adjoint -------------------------
+ *
+ * The forward step of f64_step, written with its intermediate derivatives
+ *   a = Gx vx, c = Gz vz                  (CK:201-258, old velocities)
+ *   px' = damp2a px + kw2 a (+ source), pz' = damp1a pz + kw1 c
+ *   p' = px' + pz',  g = Hx p', h = Hz p'  (CK:260-316)
+ *   vx' = damp2b vx + bw2 g,  vz' = damp1b vz + bw1 h
+ * is linear in the state, so its adjoint runs the same stages backwards with
+ * every operator transposed.  The transposes below scatter each row of the
+ * forward operator exactly as the forward code defines that row, so they are
+ * the transposes of the reference's operators including its edge rows. */
+
+/* out += Gx^T mu, Gx = D-x of CK:201-229 */
+static void gxT_add(const double *mu, double *out, int nnz, int nnx) {
+    for (int i2 = 2; i2 < nnx - 1; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            double m = mu[id];
+            out[id] += ORC_A0 * m;
+            out[id - nnz] -= ORC_A0 * m;
+            out[id + nnz] += ORC_A1 * m;
+            out[id - 2 * nnz] -= ORC_A1 * m;
+        }
+    for (int i1 = 0; i1 < nnz; i1++) {
+        size_t id = (size_t)i1 + (size_t)1 * nnz;
+        out[id] += mu[id];
+        out[id - nnz] -= mu[id];
+        id = (size_t)i1 + (size_t)(nnx - 1) * nnz;
+        out[id] += mu[id];
+        out[id - nnz] -= mu[id];
+    }
+}
+/* out += Gz^T mu, Gz = D-z of CK:231-258 */
+static void gzT_add(const double *mu, double *out, int nnz, int nnx) {
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 2; i1 < nnz - 1; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            double m = mu[id];
+            out[id] += ORC_A0 * m;
+            out[id - 1] -= ORC_A0 * m;
+            out[id + 1] += ORC_A1 * m;
+            out[id - 2] -= ORC_A1 * m;
+        }
+    for (int i2 = 0; i2 < nnx; i2++) {
+        size_t id = (size_t)(nnz - 1) + (size_t)i2 * nnz;
+        out[id] += mu[id];
+        out[id - 1] -= mu[id];
+        id = (size_t)1 + (size_t)i2 * nnz;
+        out[id] += mu[id];
+        out[id - 1] -= mu[id];
+    }
+}
+/* out += Hx^T mu, Hx = D+x of CK:260-287 */
+static void hxT_add(const double *mu, double *out, int nnz, int nnx) {
+    for (int i2 = 1; i2 < nnx - 2; i2++)
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            double m = mu[id];
+            out[id + nnz] += ORC_A0 * m;
+            out[id] -= ORC_A0 * m;
+            out[id + 2 * nnz] += ORC_A1 * m;
+            out[id - nnz] -= ORC_A1 * m;
+        }
+    for (int i1 = 0; i1 < nnz; i1++) {
+        size_t id = (size_t)i1;
+        out[id + nnz] += mu[id];
+        out[id] -= mu[id];
+        id = (size_t)i1 + (size_t)(nnx - 2) * nnz;
+        out[id + nnz] += mu[id];
+        out[id] -= mu[id];
+    }
+}
+/* out += Hz^T mu, Hz = D+z of CK:289-316 */
+static void hzT_add(const double *mu, double *out, int nnz, int nnx) {
+    for (int i2 = 0; i2 < nnx; i2++)
+        for (int i1 = 1; i1 < nnz - 2; i1++) {
+            size_t id = (size_t)i1 + (size_t)i2 * nnz;
+            double m = mu[id];
+            out[id + 1] += ORC_A0 * m;
+            out[id] -= ORC_A0 * m;
+            out[id + 2] += ORC_A1 * m;
+            out[id - 1] -= ORC_A1 * m;
+        }
+    for (int i2 = 0; i2 < nnx; i2++) {
+        size_t id = (size_t)(nnz - 2) + (size_t)i2 * nnz;
+        out[id + 1] += mu[id];
+        out[id] -= mu[id];
+        id = (size_t)i2 * nnz;
+        out[id + 1] += mu[id];
+        out[id] -= mu[id];
+    }
+}
+
+/* d = G f for the four forward operators (same code as f64_step). */
+static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
+    size_t N = (size_t)nnz * nnx;
+    memset(d, 0, N * sizeof(double));
+    if (which == 0) { /* Gx */
+        for (int i2 = 2; i2 < nnx - 1; i2++)
+            for (int i1 = 0; i1 < nnz; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                d[id] = ORC_A0 * (f[id] - f[id - nnz]) + ORC_A1 * (f[id + nnz] - f[id - 2 * nnz]);
+            }
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1 + (size_t)nnz;
+            d[id] = f[id] - f[id - nnz];
+            id = (size_t)i1 + (size_t)(nnx - 1) * nnz;
+            d[id] = f[id] - f[id - nnz];
+        }
+    } else if (which == 1) { /* Gz */
+        for (int i2 = 0; i2 < nnx; i2++)
+            for (int i1 = 2; i1 < nnz - 1; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                d[id] = ORC_A0 * (f[id] - f[id - 1]) + ORC_A1 * (f[id + 1] - f[id - 2]);
+            }
+        for (int i2 = 0; i2 < nnx; i2++) {
+            size_t id = (size_t)(nnz - 1) + (size_t)i2 * nnz;
+            d[id] = f[id] - f[id - 1];
+            id = (size_t)1 + (size_t)i2 * nnz;
+            d[id] = f[id] - f[id - 1];
+        }
+    } else if (which == 2) { /* Hx */
+        for (int i2 = 1; i2 < nnx - 2; i2++)
+            for (int i1 = 0; i1 < nnz; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                d[id] = ORC_A0 * (f[id + nnz] - f[id]) + ORC_A1 * (f[id + 2 * nnz] - f[id - nnz]);
+            }
+        for (int i1 = 0; i1 < nnz; i1++) {
+            size_t id = (size_t)i1;
+            d[id] = f[id + nnz] - f[id];
+            id = (size_t)i1 + (size_t)(nnx - 2) * nnz;
+            d[id] = f[id + nnz] - f[id];
+        }
+    } else { /* Hz */
+        for (int i2 = 0; i2 < nnx; i2++)
+            for (int i1 = 1; i1 < nnz - 2; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                d[id] = ORC_A0 * (f[id + 1] - f[id]) + ORC_A1 * (f[id + 2] - f[id - 1]);
+            }
+        for (int i2 = 0; i2 < nnx; i2++) {
+            size_t id = (size_t)(nnz - 2) + (size_t)i2 * nnz;
+            d[id] = f[id + 1] - f[id];
+            id = (size_t)i2 * nnz;
+            d[id] = f[id + 1] - f[id];
+        }
+    }
+}
+
+int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
+                 float sx, float sz, int nrec, const float *gx, const float *gz,
+                 const double *wavelet, int nwav, const double *adj,
+                 double *grad_vp, double *grad_rho,
+                 double *grad_kappa, double *grad_bx, double *grad_bz,
+                 double *src_adj, double *seis64) {
+    if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz))) return -1;
+    orc_derived d;
+    orc_derive(prm, &d);
+    if (d.dt_factor < 1 || d.fd_nt < 1) return -2;
+    const int nnx = d.nnx, nnz = d.nnz, nb = prm->nb, nt = d.fd_nt;
+    const size_t N = (size_t)nnx * nnz;
+    float *vel = calloc(N, sizeof(float)), *den = calloc(N, sizeof(float));
+    float *bue = calloc(N, sizeof(float)), *bx = calloc(N, sizeof(float)), *bz = calloc(N, sizeof(float));
+    double *kappa = calloc(N, sizeof(double));
+    expand(vel, vp, nb, nnz, nnx, prm->nz, prm->nx);
+    expand(den, rho, nb, nnz, nnx, prm->nz, prm->nx);
+    stagger(vel, den, bue, bx, bz, kappa, nnz, nnx);
+    int nw = wavelet ? nwav : d.nts;
+    double *w = calloc((size_t)(nw > 0 ? nw : 0) + 1, sizeof(double));
+    if (wavelet) memcpy(w, wavelet, (size_t)nw * sizeof(double));
+    else orc_ricker(prm, &d, w);
+    float *damp2a = calloc(nnx, 4), *damp2a1 = calloc(nnx, 4), *damp2b = calloc(nnx, 4), *damp2b1 = calloc(nnx, 4);
+    float *damp1a = calloc(nnz, 4), *damp1a1 = calloc(nnz, 4), *damp1b = calloc(nnz, 4), *damp1b1 = calloc(nnz, 4);
+    sponge_a(0.05f, damp2a, damp2a1, nb, prm->nx);
+    sponge_b(0.05f, damp2b, damp2b1, nb, prm->nx);
+    sponge_a(0.05f, damp1a, damp1a1, nb, prm->nz);
+    sponge_b(0.05f, damp1b, damp1b1, nb, prm->nz);
+    int isrc = orc_cell(prm, sx, sz);
+    int *gcell = calloc((size_t)nrec + 1, sizeof(int));
+    for (int g = 0; g < nrec; g++) gcell[g] = orc_cell(prm, gx[g], gz[g]);
+    double *kw1 = malloc(N * 8), *kw2 = malloc(N * 8), *bw1 = malloc(N * 8), *bw2 = malloc(N * 8);
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            kw2[id] = d.dtdx * kappa[id] * damp2a1[ix];
+            kw1[id] = d.dtdz * kappa[id] * damp1a1[iz];
+            bw2[id] = d.dtdx * bx[id] * damp2b1[ix];
+            bw1[id] = d.dtdz * bz[id] * damp1b1[iz];
+        }
+    const float dxdz = prm->dx * prm->dz;
+    /* forward, storing a, c, g, h of every step */
+    double *A = malloc(N * 8 * (size_t)nt), *Cc = malloc(N * 8 * (size_t)nt);
+    double *Gg = malloc(N * 8 * (size_t)nt), *Hh = malloc(N * 8 * (size_t)nt);
+    double *px = calloc(N, 8), *pz = calloc(N, 8), *vx = calloc(N, 8), *vz = calloc(N, 8), *p = calloc(N, 8);
+    if (!A || !Cc || !Gg || !Hh) return -4;
+    for (int kt = 0; kt < nt; kt++) {
+        double *a = A + N * kt, *c = Cc + N * kt, *g = Gg + N * kt, *h = Hh + N * kt;
+        op_apply(0, vx, a, nnz, nnx);
+        op_apply(1, vz, c, nnz, nnx);
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz < nnz; iz++) {
+                size_t id = (size_t)iz + (size_t)ix * nnz;
+                px[id] = damp2a[ix] * px[id] + kw2[id] * a[id];
+                pz[id] = damp1a[iz] * pz[id] + kw1[id] * c[id];
+            }
+        if (kt <= d.nts) px[isrc] = px[isrc] + prm->fd_dt * (kt < nw ? w[kt] : 0.0) * kappa[isrc] / (dxdz);
+        for (size_t id = 0; id < N; id++) p[id] = px[id] + pz[id];
+        op_apply(2, p, g, nnz, nnx);
+        op_apply(3, p, h, nnz, nnx);
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz < nnz; iz++) {
+                size_t id = (size_t)iz + (size_t)ix * nnz;
+                vx[id] = damp2b[ix] * vx[id] + bw2[id] * g[id];
+                vz[id] = damp1b[iz] * vz[id] + bw1[id] * h[id];
+            }
+        if (seis64 && (kt + 1) % d.dt_factor == 0) {
+            int it = (kt + 1) / d.dt_factor - 1;
+            if (it < d.real_nt)
+                for (int r = 0; r < nrec; r++) seis64[(size_t)r * d.real_nt + it] = p[gcell[r]];
+        }
+    }
+    /* adjoint, backwards in time */
+    double *mpx = calloc(N, 8), *mpz = calloc(N, 8), *mvx = calloc(N, 8), *mvz = calloc(N, 8);
+    double *mg = malloc(N * 8), *mh = malloc(N * 8), *q = malloc(N * 8), *mPX = malloc(N * 8), *mPZ = malloc(N * 8);
+    double *ma = malloc(N * 8), *mc = malloc(N * 8), *nvx = malloc(N * 8), *nvz = malloc(N * 8);
+    double *gk = calloc(N, 8), *gbx = calloc(N, 8), *gbz = calloc(N, 8);
+    double gk_src = 0.0;
+    for (int kt = nt - 1; kt >= 0; kt--) {
+        double *a = A + N * kt, *c = Cc + N * kt, *g = Gg + N * kt, *h = Hh + N * kt;
+        /* vx' = damp2b vx + bw2 g ; vz' = damp1b vz + bw1 h */
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz < nnz; iz++) {
+                size_t id = (size_t)iz + (size_t)ix * nnz;
+                mg[id] = bw2[id] * mvx[id];
+                mh[id] = bw1[id] * mvz[id];
+                gbx[id] += d.dtdx * damp2b1[ix] * g[id] * mvx[id];
+                gbz[id] += d.dtdz * damp1b1[iz] * h[id] * mvz[id];
+                nvx[id] = damp2b[ix] * mvx[id];
+                nvz[id] = damp1b[iz] * mvz[id];
+            }
+        /* g = Hx p', h = Hz p' ; record */
+        memset(q, 0, N * 8);
+        hxT_add(mg, q, nnz, nnx);
+        hzT_add(mh, q, nnz, nnx);
+        if (adj && (kt + 1) % d.dt_factor == 0) {
+            int it = (kt + 1) / d.dt_factor - 1;
+            if (it < d.real_nt)
+                for (int r = 0; r < nrec; r++) q[gcell[r]] += adj[(size_t)r * d.real_nt + it];
+        }
+        /* p' = px' + pz' */
+        for (size_t id = 0; id < N; id++) {
+            mPX[id] = mpx[id] + q[id];
+            mPZ[id] = mpz[id] + q[id];
+        }
+        /* source term: d/dkappa_src and the injection's transpose */
+        if (src_adj) src_adj[kt] = mPX[isrc];
+        if (kt <= d.nts) gk_src += mPX[isrc] * (prm->fd_dt * (kt < nw ? w[kt] : 0.0) / (dxdz));
+        /* px' = damp2a px + kw2 a ; pz' = damp1a pz + kw1 c */
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz < nnz; iz++) {
+                size_t id = (size_t)iz + (size_t)ix * nnz;
+                gk[id] += d.dtdx * damp2a1[ix] * a[id] * mPX[id] + d.dtdz * damp1a1[iz] * c[id] * mPZ[id];
+                mpx[id] = damp2a[ix] * mPX[id];
+                mpz[id] = damp1a[iz] * mPZ[id];
+                ma[id] = kw2[id] * mPX[id];
+                mc[id] = kw1[id] * mPZ[id];
+            }
+        /* a = Gx vx, c = Gz vz */
+        gxT_add(ma, nvx, nnz, nnx);
+        gzT_add(mc, nvz, nnz, nnx);
+        memcpy(mvx, nvx, N * 8);
+        memcpy(mvz, nvz, N * 8);
+    }
+    gk[isrc] += gk_src;
+    if (grad_kappa) memcpy(grad_kappa, gk, N * 8);
+    if (grad_bx) memcpy(grad_bx, gbx, N * 8);
+    if (grad_bz) memcpy(grad_bz, gbz, N * 8);
+    /* materials -> buoyancy: bz = 0.5 (b[z] + b[z+1]) (last row 0), bx = 0.5 (b[x] + b[x+1]),
+     * bx last column = bz of column nnx-2 (CK:89-119) */
+    double *gb = calloc(N, 8);
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz - 1; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            gb[id] += 0.5 * gbz[id];
+            gb[id + 1] += 0.5 * gbz[id];
+        }
+    for (int ix = 0; ix < nnx - 1; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            gb[id] += 0.5 * gbx[id];
+            gb[id + nnz] += 0.5 * gbx[id];
+        }
+    for (int iz = 0; iz < nnz - 1; iz++) {
+        size_t last = (size_t)iz + (size_t)(nnx - 1) * nnz, id = (size_t)iz + (size_t)(nnx - 2) * nnz;
+        gb[id] += 0.5 * gbx[last];
+        gb[id + 1] += 0.5 * gbx[last];
+    }
+    /* kappa = vp^2 rho, b = 1/rho (rho > 0), then fold the sponge onto the model */
+    if (grad_vp) memset(grad_vp, 0, (size_t)prm->nx * prm->nz * 8);
+    if (grad_rho) memset(grad_rho, 0, (size_t)prm->nx * prm->nz * 8);
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            int mx = ix - nb < 0 ? 0 : (ix - nb > prm->nx - 1 ? prm->nx - 1 : ix - nb);
+            int mz = iz - nb < 0 ? 0 : (iz - nb > prm->nz - 1 ? prm->nz - 1 : iz - nb);
+            double v = vel[id], r = den[id];
+            size_t m = (size_t)mx * prm->nz + mz;
+            if (grad_vp) grad_vp[m] += 2.0 * v * r * gk[id];
+            if (grad_rho) grad_rho[m] += v * v * gk[id] + (r > 0 ? -gb[id] / (r * r) : 0.0);
+        }
+    free(gb);
+    free(A); free(Cc); free(Gg); free(Hh); free(px); free(pz); free(vx); free(vz); free(p);
+    free(mpx); free(mpz); free(mvx); free(mvz); free(mg); free(mh); free(q); free(mPX); free(mPZ);
+    free(ma); free(mc); free(nvx); free(nvz); free(gk); free(gbx); free(gbz);
+    free(kw1); free(kw2); free(bw1); free(bw2); free(gcell); free(w);
+    free(vel); free(den); free(bue); free(bx); free(bz); free(kappa);
+    free(damp2a); free(damp2a1); free(damp2b); free(damp2b1); free(damp1a); free(damp1a1); free(damp1b); free(damp1b1);
+    return 0;
+}

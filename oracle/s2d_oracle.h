@@ -67,6 +67,26 @@ int orc_forward(const orc_params *p, int precision,
                 const double *wavelet, int nwav, int kt_stop,
                 float *seis, double *state_out);
 
+/*
+ * FP64 discrete adjoint of the ORC_F64 forward of one shot (test reference for
+ * the CUDA gradient).  adj: the adjoint source dJ/d(seis), [nrec][real_nt]
+ * (for the L2 misfit, the residual).  Returns, each optional:
+ *   grad_vp, grad_rho  [nx][nz]  dJ/dvp, dJ/drho on the physical grid (the
+ *                                 sponge cells fold onto the edge cells they
+ *                                 replicate)
+ *   grad_kappa, grad_bx, grad_bz [nnx][nnz] dJ/d of the padded materials
+ *   src_adj            [fd_nt]   adjoint pressure at the source after each
+ *                                 step's source term (the transpose of the
+ *                                 injection: d seis / d w is its dot product)
+ *   seis64             [nrec][real_nt] the forward traces in double
+ */
+int orc_gradient(const orc_params *p, const float *vp, const float *rho,
+                 float sx, float sz, int nrec, const float *gx, const float *gz,
+                 const double *wavelet, int nwav, const double *adj,
+                 double *grad_vp, double *grad_rho,
+                 double *grad_kappa, double *grad_bx, double *grad_bz,
+                 double *src_adj, double *seis64);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,8 @@ S2D_PLAIN = 0x2
 S2D_NO_GRAPH = 0x4
 S2D_SYNC = 0x8
 S2D_MODEL_DEVICE = 0x1
+S2D_GRAD_MISFIT = 0x10
+S2D_GRAD_DEVICE = 0x20
 
 
 class Coord(C.Structure):
@@ -61,7 +63,7 @@ class Geometry(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("loop_ms", C.c_double), ("cell_updates", C.c_double), ("gcells_per_s", C.c_double),
-                ("kernel_launches", C.c_int), ("graph_used", C.c_int)]
+                ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int)]
 
 
 # Every symbol include/seis2d.h declares, with its ctypes signature.
@@ -77,6 +79,9 @@ SIGNATURES = {
     "s2d_model_destroy": ([C.c_void_p, C.c_int], C.c_int),
     "s2d_forward": ([C.c_void_p, C.POINTER(Shot), C.c_int, C.POINTER(Wave), C.POINTER(C.c_double), C.c_int,
                      C.c_int, C.c_int, C.c_void_p, C.c_uint, C.POINTER(Stats)], C.c_int),
+    "s2d_gradient": ([C.c_void_p, C.POINTER(Shot), C.c_int, C.POINTER(Wave), C.POINTER(C.c_double), C.c_int,
+                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                      C.POINTER(C.c_double), C.c_uint, C.POINTER(Stats)], C.c_int),
     "s2d_jobcard_read": ([C.c_char_p, C.POINTER(JobCard), C.c_char_p, C.c_size_t], C.c_int),
     "s2d_geometry_read": ([C.POINTER(JobCard), C.POINTER(Geometry), C.c_char_p, C.c_size_t], C.c_int),
     "s2d_geometry_free": ([C.POINTER(Geometry)], None),

@@ -187,6 +187,82 @@ class Context:
         return res
 
 
+class GradientResult:
+    """Result of Context.gradient: dJ/dvp and dJ/drho ([nx][nz]), the
+    misfit (misfit mode), the forward seismograms (if asked) and dJ/dw per
+    shot and FD step."""
+
+    def __init__(self, grad_vp, grad_rho, misfit, seis, grad_wavelet, stats):
+        self.grad_vp, self.grad_rho, self.misfit = grad_vp, grad_rho, misfit
+        self.seis, self.grad_wavelet, self.stats = seis, grad_wavelet, stats
+
+
+def _gradient(self: "Context", shots: Sequence[Shot], wave: Wave, data, misfit: bool = False,
+              wavelet: Optional[np.ndarray] = None, grad_vp=None, grad_rho=None, want_seis: bool = False,
+              graph: bool = True) -> GradientResult:
+    """FWI gradient of the shots (one model).  ``data`` is dJ/d(seis) or, with
+    ``misfit=True``, the observed seismograms (J = 0.5 ||d - data||^2); same
+    flat layout as ``forward``'s output.  numpy arrays are host buffers; CUDA
+    tensors are device buffers (``grad_vp``/``grad_rho`` given as CUDA tensors
+    receive the gradient in place)."""
+    steps = derive_steps(wave)
+    nt, fd_nt = steps["real_nt"], steps["fd_nt"]
+    m = shots[0].model
+    cshots = (L.Shot * len(shots))()
+    keep = []
+    total = 0
+    for i, s in enumerate(shots):
+        rec = np.ascontiguousarray(s.rec, np.float32).reshape(-1, 2)
+        keep.append(rec)
+        cshots[i] = L.Shot(s.model.id, L.Coord(float(s.src[0]), float(s.src[1])), rec.shape[0],
+                           rec.ctypes.data_as(C.POINTER(L.Coord)))
+        total += rec.shape[0]
+    flags = L.S2D_GRAD_MISFIT if misfit else 0
+    if not graph:
+        flags |= L.S2D_NO_GRAPH
+    if _is_torch(data):
+        assert data.is_cuda and data.numel() >= total * nt
+        flags |= L.S2D_SEIS_DEVICE
+        dptr = C.c_void_p(data.data_ptr())
+        seis = None
+        if want_seis:
+            import torch
+            seis = torch.empty(total * nt, dtype=torch.float32, device=data.device)
+    else:
+        data = np.ascontiguousarray(data, np.float32).reshape(-1)
+        assert data.size >= total * nt
+        keep.append(data)
+        dptr = C.c_void_p(data.ctypes.data)
+        seis = np.zeros(total * nt, np.float32) if want_seis else None
+    sptr = None
+    if seis is not None:
+        sptr = C.c_void_p(seis.data_ptr() if _is_torch(seis) else seis.ctypes.data)
+    if grad_vp is not None and _is_torch(grad_vp):
+        flags |= L.S2D_GRAD_DEVICE
+        gv, gr = grad_vp, grad_rho
+        gvp, grp = C.c_void_p(gv.data_ptr()), C.c_void_p(gr.data_ptr())
+    else:
+        gv = np.zeros((m.nx, m.nz), np.float32)
+        gr = np.zeros((m.nx, m.nz), np.float32)
+        gvp, grp = C.c_void_p(gv.ctypes.data), C.c_void_p(gr.ctypes.data)
+    wp, nw = None, 0
+    if wavelet is not None:
+        wavelet = np.ascontiguousarray(wavelet, np.float64)
+        keep.append(wavelet)
+        wp, nw = wavelet.ctypes.data_as(C.POINTER(C.c_double)), wavelet.size
+    gw = np.zeros((len(shots), fd_nt), np.float64)
+    mis = C.c_double(0.0)
+    st = L.Stats()
+    self._check(L.lib().s2d_gradient(self._h, cshots, len(shots), C.byref(wave.c()), wp, nw, dptr, gvp, grp,
+                                     sptr, C.byref(mis), gw.ctypes.data_as(C.POINTER(C.c_double)), flags,
+                                     C.byref(st)))
+    self.last_stats = st
+    return GradientResult(gv, gr, mis.value if misfit else None, seis, gw, st)
+
+
+Context.gradient = _gradient
+
+
 def modelling_module(vp: np.ndarray, rho: np.ndarray, dx: float, dz: float, wave: Wave,
                      geometry: Sequence[Tuple[Tuple[float, float], np.ndarray]], nb: int = 32,
                      device: int = 0, plain: bool = False) -> List[np.ndarray]:

@@ -54,6 +54,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = _nvcc()
     common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
               "-ccbin", _host_cxx(), "-I", os.path.join(ROOT, "include")]
+    if os.environ.get("S2D_DEVICE_CHECKS") == "1":
+        # debug build: per-task range checks in the step kernels (see s2d_device.cuh)
+        common += ["-DS2D_DEVICE_CHECKS"]
     objs = []
     for src in sources():
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")

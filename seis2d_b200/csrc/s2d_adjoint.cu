@@ -1,0 +1,370 @@
+// Adjoint FD step and gradient finalisation of libseis2d (sm_100a).
+//
+// The forward step (cpumodelling.cpp:115-156) written with its derivatives
+//   a = Gx vx, c = Gz vz                      (D-, cpu_modelling_kernels.cpp:201-258)
+//   px' = Dax px + Kx kappa a (+ source),  pz' = Daz pz + Kz kappa c
+//   p' = px' + pz',  g = Hx p', h = Hz p'    (D+, :260-316)
+//   vx' = Dbx vx + Lx bx g,  vz' = Dbz vz + Lz bz h
+// is linear in the state.  One adjoint step maps the adjoint state after step
+// kt, (mpx', mpz', mvx', mvz'), to the one before it:
+//   mg = Lx bx mvx',  mh = Lz bz mvz'
+//   q  = Hx^T mg + Hz^T mh (+ the adjoint source at the receivers)
+//   mPX = mpx' + q,  mPZ = mpz' + q
+//   mpx = Dax mPX,  mpz = Daz mPZ
+//   mvx = Dbx mvx' + Gx^T (Kx kappa mPX),  mvz = Dbz mvz' + Gz^T (Kz kappa mPZ)
+// and accumulates the imaging terms
+//   dJ/dkappa += Kx a mPX + Kz c mPZ,  dJ/dbx += Lx g mvx',  dJ/dbz += Lz h mvz'
+// with a, c, g, h of step kt saved by the forward (S2D_STEP_PRODUCTS).
+//
+// The transposes are the gather forms of the reference's operators, edge rows
+// included: with (c0(j), c1(j)) the coefficient pair of forward row j,
+//   (G^T m)[i] = c0(i) m[i] - c0(i+1) m[i+1] + c1(i-1) m[i-1] - c1(i+2) m[i+2]
+//   (H^T m)[i] = c0(i-1) m[i-1] - c0(i) m[i] + c1(i-2) m[i-2] - c1(i+1) m[i+1]
+// The kernel streams like the forward: a warp owns a 128-row strip, q and the
+// pressure adjoint at column L-1, the velocity adjoint at column L-3.
+#include <cuda_runtime.h>
+
+#include "s2d_device.cuh"
+
+namespace s2d {
+
+namespace {
+
+// Coefficient pair of forward row i along z; interior strips use constants.
+template <bool EDGE>
+__device__ __forceinline__ float zc0m(int i, int n) {
+    if (!EDGE) return kA0;
+    float c0, c1;
+    dm_coef(i, n, c0, c1);
+    return c0;
+}
+template <bool EDGE>
+__device__ __forceinline__ float zc1m(int i, int n) {
+    if (!EDGE) return kA1;
+    float c0, c1;
+    dm_coef(i, n, c0, c1);
+    return c1;
+}
+template <bool EDGE>
+__device__ __forceinline__ float zc0p(int i, int n) {
+    if (!EDGE) return kA0;
+    float c0, c1;
+    dp_coef(i, n, c0, c1);
+    return c0;
+}
+template <bool EDGE>
+__device__ __forceinline__ float zc1p(int i, int n) {
+    if (!EDGE) return kA1;
+    float c0, c1;
+    dp_coef(i, n, c0, c1);
+    return c1;
+}
+__device__ __forceinline__ float xc0m(int i, int n) { float c0, c1; dm_coef(i, n, c0, c1); return c0; }
+__device__ __forceinline__ float xc1m(int i, int n) { float c0, c1; dm_coef(i, n, c0, c1); return c1; }
+__device__ __forceinline__ float xc0p(int i, int n) { float c0, c1; dp_coef(i, n, c0, c1); return c0; }
+__device__ __forceinline__ float xc1p(int i, int n) { float c0, c1; dp_coef(i, n, c0, c1); return c1; }
+
+__device__ __forceinline__ float4 ldrw(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+template <bool EDGE>
+__device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                             int kt, int lane) {
+    const int nnx = S.nnx, nnz = S.nnz;
+    const size_t ld = (size_t)S.ld;
+    const int xb = min(nnx, xa + seg_len);
+    const int c = strip * S2D_STRIP_OUT - 4;
+    const int z0 = c + S2D_ZPT * lane;
+    const bool owner = lane >= 1 && lane <= 30;
+    const int pin = (kt + 1) & 1, pout = kt & 1;
+    const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
+    const float *mpxi = S.st[pin][0] + off, *mpzi = S.st[pin][1] + off;
+    const float *mvxi = S.st[pin][2] + off, *mvzi = S.st[pin][3] + off;
+    float *mpxo = S.st[pout][0] + off, *mpzo = S.st[pout][1] + off;
+    float *mvxo = S.st[pout][2] + off, *mvzo = S.st[pout][3] + off;
+    const float *kap = S.kappa + off, *bxp = S.bx + off, *bzp = S.bz + off;
+    const float *pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
+    float *gk = S.grad[0] + off, *gbx = S.grad[1] + off, *gbz = S.grad[2] + off;
+    float4 zc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) zc[i] = __ldg(S.zcoef + (z0 + S2D_GZ + i));
+    const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
+                     (kt + 1) / a.dt_factor - 1 < S.real_nt;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    const int sdz = S.src_z - z0;
+
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 mv0 = zero, mv1 = zero, mv2 = zero, mv3 = zero;  // mvx' at L-3 .. L
+    float4 mg0 = zero, mg1 = zero, mg2 = zero, mg3 = zero;  // Lx bx mvx' at L-3 .. L
+    float4 ma0 = zero, ma1 = zero, ma2 = zero, ma3 = zero;  // Kx kappa mPX at L-4 .. L-1
+    float4 mc0 = zero, mc1 = zero, mc2 = zero;              // Kz kappa mPZ at L-3 .. L-1
+    float4 mz0 = zero, mz1 = zero, mz2 = zero;              // mvz' at L-3 .. L-1
+
+    for (int L = xa - 3; L <= xb + 2; ++L) {
+        {
+            const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
+            const float4 m = ld4(mvxi + colL), b = ld4(bxp + colL);
+            const float lx = __ldg(S.xcoef + (L + S2D_GX)).w;
+            mv0 = mv1; mv1 = mv2; mv2 = mv3; mv3 = m;
+            mg0 = mg1; mg1 = mg2; mg2 = mg3;
+            mg3 = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z, (lx * b.w) * m.w);
+        }
+        if (L < xa) continue;
+        // ---- pressure adjoint at column Q = L - 1 ----
+        const int Q = L - 1;
+        const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
+        const float4 mpx = ld4(mpxi + colQ), mpz = ld4(mpzi + colQ), mvz = ld4(mvzi + colQ);
+        const float4 bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
+        const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
+        const float4 h = make_float4((zc[0].w * bz.x) * mvz.x, (zc[1].w * bz.y) * mvz.y,
+                                     (zc[2].w * bz.z) * mvz.z, (zc[3].w * bz.w) * mvz.w);
+        const float h_up_z = __shfl_up_sync(kFull, h.z, 1);
+        const float h_up_w = __shfl_up_sync(kFull, h.w, 1);
+        const float h_dn_x = __shfl_down_sync(kFull, h.x, 1);
+        float4 q;
+        {
+            const float p0a = xc0p(Q - 1, nnx), p0b = xc0p(Q, nnx), p1a = xc1p(Q - 2, nnx), p1b = xc1p(Q + 1, nnx);
+            q.x = p0a * mg1.x - p0b * mg2.x + p1a * mg0.x - p1b * mg3.x;
+            q.y = p0a * mg1.y - p0b * mg2.y + p1a * mg0.y - p1b * mg3.y;
+            q.z = p0a * mg1.z - p0b * mg2.z + p1a * mg0.z - p1b * mg3.z;
+            q.w = p0a * mg1.w - p0b * mg2.w + p1a * mg0.w - p1b * mg3.w;
+        }
+        q.x += zc0p<EDGE>(z0 - 1, nnz) * h_up_w - zc0p<EDGE>(z0, nnz) * h.x + zc1p<EDGE>(z0 - 2, nnz) * h_up_z -
+               zc1p<EDGE>(z0 + 1, nnz) * h.y;
+        q.y += zc0p<EDGE>(z0, nnz) * h.x - zc0p<EDGE>(z0 + 1, nnz) * h.y + zc1p<EDGE>(z0 - 1, nnz) * h_up_w -
+               zc1p<EDGE>(z0 + 2, nnz) * h.z;
+        q.z += zc0p<EDGE>(z0 + 1, nnz) * h.y - zc0p<EDGE>(z0 + 2, nnz) * h.z + zc1p<EDGE>(z0, nnz) * h.x -
+               zc1p<EDGE>(z0 + 3, nnz) * h.w;
+        q.w += zc0p<EDGE>(z0 + 2, nnz) * h.z - zc0p<EDGE>(z0 + 3, nnz) * h.w + zc1p<EDGE>(z0 + 1, nnz) * h.y -
+               zc1p<EDGE>(z0 + 4, nnz) * h_dn_x;
+        // Transpose of the receiver sampling (cpumodelling.cpp:356-360).  Every
+        // warp computing column Q adds it (halo columns included, they feed the
+        // neighbours' velocity adjoint); the receiver table covers columns
+        // [0, nnx) only.
+        if (inj && Q >= 0 && Q < nnx) {
+            const int j1 = __ldg(S.rec_ptr + Q + 1);
+            for (int j = __ldg(S.rec_ptr + Q); j < j1; ++j) {
+                const int d = __ldg(S.rec_z + j) - z0;
+                if (d >= 0 && d < 4) {
+                    const float r = __ldg(S.seis + (size_t)__ldg(S.rec_id + j) * S.real_nt + slot);
+                    if (d == 0) q.x += r;
+                    else if (d == 1) q.y += r;
+                    else if (d == 2) q.z += r;
+                    else q.w += r;
+                }
+            }
+        }
+        const float4 mPX = make_float4(mpx.x + q.x, mpx.y + q.y, mpx.z + q.z, mpx.w + q.w);
+        const float4 mPZ = make_float4(mpz.x + q.x, mpz.y + q.y, mpz.z + q.z, mpz.w + q.w);
+        const bool in_seg = Q >= xa && Q < xb;
+        if (in_seg && owner) {
+            st4(mpxo + colQ, make_float4(xq.x * mPX.x, xq.x * mPX.y, xq.x * mPX.z, xq.x * mPX.w));
+            st4(mpzo + colQ, make_float4(zc[0].x * mPZ.x, zc[1].x * mPZ.y, zc[2].x * mPZ.z, zc[3].x * mPZ.w));
+            const float4 pa = ld4(pr + colQ), pc = ld4(pr + F + colQ);
+            const float4 pg = ld4(pr + 2 * F + colQ), ph = ld4(pr + 3 * F + colQ);
+            float4 t = ldrw(gk + colQ);
+            t.x += (xq.y * pa.x) * mPX.x + (zc[0].y * pc.x) * mPZ.x;
+            t.y += (xq.y * pa.y) * mPX.y + (zc[1].y * pc.y) * mPZ.y;
+            t.z += (xq.y * pa.z) * mPX.z + (zc[2].y * pc.z) * mPZ.z;
+            t.w += (xq.y * pa.w) * mPX.w + (zc[3].y * pc.w) * mPZ.w;
+            st4(gk + colQ, t);
+            t = ldrw(gbx + colQ);
+            t.x += (xq.w * pg.x) * mv2.x;
+            t.y += (xq.w * pg.y) * mv2.y;
+            t.z += (xq.w * pg.z) * mv2.z;
+            t.w += (xq.w * pg.w) * mv2.w;
+            st4(gbx + colQ, t);
+            t = ldrw(gbz + colQ);
+            t.x += (zc[0].w * ph.x) * mvz.x;
+            t.y += (zc[1].w * ph.y) * mvz.y;
+            t.z += (zc[2].w * ph.z) * mvz.z;
+            t.w += (zc[3].w * ph.w) * mvz.w;
+            st4(gbz + colQ, t);
+            if (Q == S.src_x && sdz >= 0 && sdz < 4) S.srcadj[kt] = comp(mPX, sdz);
+        }
+        ma0 = ma1; ma1 = ma2; ma2 = ma3;
+        ma3 = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
+                          (xq.y * kk.w) * mPX.w);
+        mc0 = mc1; mc1 = mc2;
+        mc2 = make_float4((zc[0].y * kk.x) * mPZ.x, (zc[1].y * kk.y) * mPZ.y, (zc[2].y * kk.z) * mPZ.z,
+                          (zc[3].y * kk.w) * mPZ.w);
+        mz0 = mz1; mz1 = mz2; mz2 = mvz;
+        if (L < xa + 3) continue;
+        // ---- velocity adjoint at column W = L - 3 ----
+        const int W = L - 3;
+        const ptrdiff_t colW = (ptrdiff_t)W * (ptrdiff_t)ld;
+        const float dbx = __ldg(S.xcoef + (W + S2D_GX)).z;
+        const float m0a = xc0m(W, nnx), m0b = xc0m(W + 1, nnx), m1a = xc1m(W - 1, nnx), m1b = xc1m(W + 2, nnx);
+        float4 ovx;
+        ovx.x = dbx * mv0.x + (m0a * ma1.x - m0b * ma2.x + m1a * ma0.x - m1b * ma3.x);
+        ovx.y = dbx * mv0.y + (m0a * ma1.y - m0b * ma2.y + m1a * ma0.y - m1b * ma3.y);
+        ovx.z = dbx * mv0.z + (m0a * ma1.z - m0b * ma2.z + m1a * ma0.z - m1b * ma3.z);
+        ovx.w = dbx * mv0.w + (m0a * ma1.w - m0b * ma2.w + m1a * ma0.w - m1b * ma3.w);
+        const float4 cc = mc0;
+        const float c_up_w = __shfl_up_sync(kFull, cc.w, 1);
+        const float c_dn_x = __shfl_down_sync(kFull, cc.x, 1);
+        const float c_dn_y = __shfl_down_sync(kFull, cc.y, 1);
+        float4 ovz;
+        ovz.x = zc[0].z * mz0.x + (zc0m<EDGE>(z0, nnz) * cc.x - zc0m<EDGE>(z0 + 1, nnz) * cc.y +
+                                   zc1m<EDGE>(z0 - 1, nnz) * c_up_w - zc1m<EDGE>(z0 + 2, nnz) * cc.z);
+        ovz.y = zc[1].z * mz0.y + (zc0m<EDGE>(z0 + 1, nnz) * cc.y - zc0m<EDGE>(z0 + 2, nnz) * cc.z +
+                                   zc1m<EDGE>(z0, nnz) * cc.x - zc1m<EDGE>(z0 + 3, nnz) * cc.w);
+        ovz.z = zc[2].z * mz0.z + (zc0m<EDGE>(z0 + 2, nnz) * cc.z - zc0m<EDGE>(z0 + 3, nnz) * cc.w +
+                                   zc1m<EDGE>(z0 + 1, nnz) * cc.y - zc1m<EDGE>(z0 + 4, nnz) * c_dn_x);
+        ovz.w = zc[3].z * mz0.w + (zc0m<EDGE>(z0 + 3, nnz) * cc.w - zc0m<EDGE>(z0 + 4, nnz) * c_dn_x +
+                                   zc1m<EDGE>(z0 + 2, nnz) * cc.z - zc1m<EDGE>(z0 + 5, nnz) * c_dn_y);
+        if (owner) {
+            st4(mvxo + colW, ovx);
+            st4(mvzo + colW, ovz);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base - kt_off;
+    if (kt < 0 || kt >= a.fd_nt) return;
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        if (!task_in_bounds(a, S, strip, xa, seg_len, kt, true, 2)) continue;
+        const int c = strip * S2D_STRIP_OUT - 4;
+        // rows c-2 .. c+129 all carry the interior coefficient pairs
+        if (strip >= 1 && c + 132 <= S.nnz)
+            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane);
+        else
+            adjoint_task<true>(a, S, strip, xa, seg_len, kt, lane);
+    }
+}
+
+// ---- gradient finalisation ----
+
+__device__ __forceinline__ size_t pad_id(int x, int z, int ld) {
+    return (size_t)(x + S2D_GX) * ld + (z + S2D_GZ);
+}
+
+// Source term of dJ/dkappa (the amplitude fd_dt w kappa_src / (dx dz) depends
+// on kappa at the source cell), added in shot order.
+__global__ void add_source_terms(float *const *gk, const int *cells, const double *vals, int nshots) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int s = 0; s < nshots; ++s) gk[s][cells[s]] = (float)((double)gk[s][cells[s]] + vals[s]);
+}
+
+__global__ void sum_shots(float *const *gk, float *const *gbx, float *const *gbz, int nshots, int nnx, int nnz,
+                          int ld, float *tk, float *tbx, float *tbz) {
+    const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
+    if (z >= nnz || x >= nnx) return;
+    const size_t id = pad_id(x, z, ld);
+    double a = 0, b = 0, c = 0;
+    for (int s = 0; s < nshots; ++s) {
+        a += gk[s][id];
+        b += gbx[s][id];
+        c += gbz[s][id];
+    }
+    tk[id] = (float)a;
+    tbx[id] = (float)b;
+    tbz[id] = (float)c;
+}
+
+// dJ/db from dJ/dbx, dJ/dbz (transpose of cpu_modelling_kernels.cpp:89-119),
+// then kappa = vp^2 rho and b = 1/rho.
+__global__ void chain_rule(const float *tk, const float *tbx, const float *tbz, const float *vp, const float *rho,
+                           int nx, int nz, int nb, int ld, float *gvp, float *grho) {
+    const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
+    const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
+    if (z >= nnz || x >= nnx) return;
+    const size_t id = pad_id(x, z, ld);
+    double gb = 0;
+    if (z < nnz - 1) gb += 0.5 * tbz[id];
+    if (z >= 1) gb += 0.5 * tbz[id - 1];
+    if (x < nnx - 1) gb += 0.5 * tbx[id];
+    if (x >= 1) gb += 0.5 * tbx[id - ld];
+    if (x == nnx - 2) {
+        const size_t last = id + ld;
+        if (z < nnz - 1) gb += 0.5 * tbx[last];
+        if (z >= 1) gb += 0.5 * tbx[last - 1];
+    }
+    const int mx = min(max(x - nb, 0), nx - 1), mz = min(max(z - nb, 0), nz - 1);
+    const double v = vp[(size_t)mx * nz + mz], r = rho[(size_t)mx * nz + mz];
+    gvp[id] = (float)(2.0 * v * r * (double)tk[id]);
+    grho[id] = (float)(v * v * (double)tk[id] + (r > 0 ? -gb / (r * r) : 0.0));
+}
+
+// Fold the sponge onto the model cells it replicates (transpose of
+// cpumodelling.cpp:39-60).
+__global__ void fold_sponge(const float *gvp, const float *grho, int nx, int nz, int nb, int ld, float *out_vp,
+                            float *out_rho) {
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x, ix = blockIdx.y;
+    if (iz >= nz || ix >= nx) return;
+    const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
+    const int x0 = ix == 0 ? 0 : ix + nb, x1 = ix == nx - 1 ? nnx - 1 : ix + nb;
+    const int z0 = iz == 0 ? 0 : iz + nb, z1 = iz == nz - 1 ? nnz - 1 : iz + nb;
+    double a = 0, b = 0;
+    for (int x = x0; x <= x1; ++x)
+        for (int z = z0; z <= z1; ++z) {
+            const size_t id = pad_id(x, z, ld);
+            a += gvp[id];
+            b += grho[id];
+        }
+    out_vp[(size_t)ix * nz + iz] = (float)a;
+    out_rho[(size_t)ix * nz + iz] = (float)b;
+}
+
+__global__ void residual_kernel(const float *seis, const float *obs, float *res, size_t n, double *sumsq) {
+    __shared__ double part[256];
+#ifdef S2D_DEVICE_CHECKS
+    if (blockDim.x != 256) return;
+#endif
+    double acc = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float r = seis[i] - obs[i];
+        res[i] = r;
+        acc += (double)r * r;
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(sumsq, part[0]);
+}
+
+}  // namespace
+
+int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream) {
+    adjoint_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    return (int)cudaGetLastError();
+}
+
+int adjoint_kernel_occupancy(int block, int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint_kernel, block, 0);
+}
+
+int launch_gradient_finalize(float *const *gk, float *const *gbx, float *const *gbz, int nshots,
+                             const int *src_cells, const double *src_vals, const float *vp, const float *rho,
+                             int nx, int nz, int nb, int ld, float *tmp3, float *gvp_pad, float *grho_pad,
+                             float *grad_vp, float *grad_rho, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
+    const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
+    add_source_terms<<<1, 1, 0, st>>>(gk, src_cells, src_vals, nshots);
+    dim3 blk(256), grd((nnz + 255) / 256, nnx);
+    sum_shots<<<grd, blk, 0, st>>>(gk, gbx, gbz, nshots, nnx, nnz, ld, tmp3, tmp3 + F, tmp3 + 2 * F);
+    chain_rule<<<grd, blk, 0, st>>>(tmp3, tmp3 + F, tmp3 + 2 * F, vp, rho, nx, nz, nb, ld, gvp_pad, grho_pad);
+    dim3 grd2((nz + 255) / 256, nx);
+    fold_sponge<<<grd2, blk, 0, st>>>(gvp_pad, grho_pad, nx, nz, nb, ld, grad_vp, grad_rho);
+    return (int)cudaGetLastError();
+}
+
+int launch_residual(const float *seis, const float *obs, float *res, size_t n, double *sumsq, void *stream) {
+    int grid = (int)std::min<size_t>(4096, (n + 255) / 256);
+    if (grid < 1) grid = 1;
+    residual_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(seis, obs, res, n, sumsq);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace s2d

@@ -134,6 +134,8 @@ struct Ctx {
     int opt_spin_limit = 1 << 20;
     int opt_fault_iter = -1;  // test knob, see s2d_set_option
     int opt_order = 1;        // task order (StepArgs::task_order)
+    int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
+    int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -204,12 +206,14 @@ int build_coef(Ctx *c, Model &m, float fd_dt) {
 // Launch configuration from the context's options: block size, ring depth,
 // shared memory and a grid of exactly the resident blocks (the kernels loop
 // over tasks), capped by the work available.
-int launch_config(Ctx *c, long max_tasks, LaunchCfg *out) {
+int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant = -1) {
     LaunchCfg lc;
-    lc.variant = c->opt_variant;
+    lc.variant = variant >= 0 ? variant : c->opt_variant;
     lc.block = std::max(32, std::min(128, c->opt_block / 32 * 32));
     lc.stages = std::max(2, std::min(16, c->opt_stages));
-    lc.smem = lc.variant == kVariantLdg ? 0 : bulk_smem_bytes(lc.block / 32, lc.stages);
+    const bool ldg = lc.variant == kVariantLdg || lc.variant == kVariantLdgProducts;
+    if (ldg) lc.block = 128;
+    lc.smem = ldg ? 0 : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
     if (e) return fail(c, S2D_ERR_ARG, "step kernel does not accept %zu B of shared memory: %s", lc.smem,
                        cudaGetErrorString((cudaError_t)e));
@@ -359,6 +363,9 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         d.src_z = h.src_z;
         d.real_nt = rs.real_nt;
         d.seis = b.seis_d + h.seis_off;
+        d.nfield = m.field_elems;
+        d.nrec = h.nrec;
+        d.nseis = (size_t)h.nrec * rs.real_nt;
         // source amplitude per step: fd_dt * w[kt] * kappa[src] / (dx*dz)
         // (cpumodelling.cpp:136-140), kappa = vp^2 rho in double at the source
         const int mx = std::min(std::max(h.src_x - m.nb, 0), m.nx - 1);
@@ -533,6 +540,9 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "grad_segment") {
+        if (value < 0) return fail(c, S2D_ERR_ARG, "grad_segment must be >= 0");
+        c->opt_grad_segment = (int)value;
     } else if (k == "task_order") {
         if (value != 0 && value != 1) return fail(c, S2D_ERR_ARG, "task_order must be 0 or 1");
         c->opt_order = (int)value;
@@ -753,8 +763,363 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         stats->gcells_per_s = ms > 0 ? stats->cell_updates / (ms * 1e6) : 0.0;
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;
+        stats->grad_segment = 0;
     }
     return S2D_OK;
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Gradient (adjoint state with checkpointed forward recompute)
+
+namespace {
+
+struct GradRun {
+    std::vector<std::unique_ptr<DevBuf>> bufs;
+    std::map<int, cudaGraphExec_t> adj_graphs;  // by step count
+    ~GradRun() {
+        for (auto &kv : adj_graphs) cudaGraphExecDestroy(kv.second);
+    }
+};
+
+int grad_alloc(Ctx *c, GradRun &g, size_t bytes, void **out) {
+    cudaError_t e;
+    g.bufs.push_back(c->pool.take(bytes, &e));
+    CK(e);
+    *out = g.bufs.back()->p;
+    return S2D_OK;
+}
+
+// Adjoint launches for steps kt_top, kt_top-1, ..., kt_top-n+1 (one graph per length).
+int run_adjoint(Ctx *c, Batch &b, GradRun &g, StepArgs args, int kt_top, int n, int grid, bool use_graph,
+                int *launches) {
+    if (n <= 0) return S2D_OK;
+    args.kt_base = kt_top;
+    StepArgs *args_d = b.args_d.as<StepArgs>();
+    int e = launch_set_args(args, args_d, c->stream);
+    if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+    *launches += 1 + n;
+    if (!use_graph) {
+        for (int k = 0; k < n; ++k) {
+            e = launch_adjoint(args_d, k, grid, 128, c->stream);
+            if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
+        }
+        return S2D_OK;
+    }
+    auto it = g.adj_graphs.find(n);
+    if (it == g.adj_graphs.end()) {
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < n; ++k) {
+            e = launch_adjoint(args_d, k, grid, 128, c->stream);
+            if (e) {
+                cudaStreamEndCapture(c->stream, &gr);
+                if (gr) cudaGraphDestroy(gr);
+                return fail(c, S2D_ERR_CUDA, "adjoint capture: %s", cudaGetErrorString((cudaError_t)e));
+            }
+        }
+        CK(cudaStreamEndCapture(c->stream, &gr));
+        cudaGraphExec_t ge;
+        cudaError_t ce = cudaGraphInstantiate(&ge, gr, 0);
+        cudaGraphDestroy(gr);
+        CK(ce);
+        it = g.adj_graphs.emplace(n, ge).first;
+    }
+    CK(cudaGraphLaunch(it->second, c->stream));
+    return S2D_OK;
+}
+
+}  // namespace
+
+extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wave,
+                            const double *wavelet, int nwavelet, const float *data, float *grad_vp,
+                            float *grad_rho, float *seis_out, double *misfit, double *grad_wavelet,
+                            unsigned flags, s2d_stats *stats) {
+    Ctx *c = static_cast<Ctx *>(ctx);
+    if (!c) return S2D_ERR_ARG;
+    if (!shots || nshots < 1 || !wave || !data || !grad_vp || !grad_rho)
+        return fail(c, S2D_ERR_ARG, "null argument");
+    for (int s = 1; s < nshots; ++s)
+        if (shots[s].model_id != shots[0].model_id)
+            return fail(c, S2D_ERR_ARG, "all shots of a gradient call must use one model");
+    if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0))
+        return fail(c, S2D_ERR_ARG, "wave parameters must be positive");
+    CK(cudaSetDevice(c->device));
+    const bool dev_seis = (flags & S2D_SEIS_DEVICE) != 0;
+    const bool dev_grad = (flags & S2D_GRAD_DEVICE) != 0;
+    const bool use_graph = !(flags & S2D_NO_GRAPH);
+    // forward batch: record into the caller's device buffer when there is one
+    unsigned fflags = (dev_seis && seis_out) ? S2D_SEIS_DEVICE : 0u;
+    {
+        int e = setup_batch(c, shots, nshots, *wave, wavelet, nwavelet, seis_out, fflags);
+        if (e) {
+            c->drop_batch();
+            return e;
+        }
+    }
+    Batch &b = *c->batch;
+    const RunSteps rs = b.steps;
+    Model &m = *c->models[shots[0].model_id];
+    const size_t F = m.field_elems, fb = F * sizeof(float);
+    GradRun g;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int launches = 0;
+
+    // per-shot adjoint state, accumulators and source-adjoint trace
+    std::vector<ShotDev> adj = b.shot_dev;
+    std::vector<float *> gk(nshots), gbx(nshots), gbz(nshots), sadj(nshots);
+    for (int s = 0; s < nshots; ++s) {
+        for (int par = 0; par < 2; ++par)
+            for (int f = 0; f < 4; ++f) {
+                void *p;
+                int e = grad_alloc(c, g, fb, &p);
+                if (e) return e;
+                CK(cudaMemsetAsync(p, 0, fb, c->stream));
+                adj[s].st[par][f] = static_cast<float *>(p);
+            }
+        void *p;
+        for (int f = 0; f < 3; ++f) {
+            int e = grad_alloc(c, g, fb, &p);
+            if (e) return e;
+            CK(cudaMemsetAsync(p, 0, fb, c->stream));
+            adj[s].grad[f] = static_cast<float *>(p);
+        }
+        gk[s] = adj[s].grad[0];
+        gbx[s] = adj[s].grad[1];
+        gbz[s] = adj[s].grad[2];
+        int e = grad_alloc(c, g, sizeof(float) * rs.fd_nt, &p);
+        if (e) return e;
+        CK(cudaMemsetAsync(p, 0, sizeof(float) * rs.fd_nt, c->stream));
+        sadj[s] = static_cast<float *>(p);
+        adj[s].srcadj = sadj[s];
+    }
+    // adjoint source: the caller's, or the residual d - d_obs after the forward
+    const size_t nseis = b.seis_elems;
+    float *adj_src = nullptr;
+    {
+        void *p;
+        int e = grad_alloc(c, g, std::max<size_t>(nseis, 1) * sizeof(float), &p);
+        if (e) return e;
+        adj_src = static_cast<float *>(p);
+    }
+    // segment length: the largest whose products and checkpoints fit
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const double budget = 0.85 * (double)free_b - 4.0 * fb - 64e6;
+    const double per_step_all = (double)nshots * 4.0 * fb;
+    int C = rs.fd_nt;
+    if (c->opt_grad_segment > 0) C = std::min(C, c->opt_grad_segment);
+    while (C > 1) {
+        const int nseg = (rs.fd_nt + C - 1) / C;
+        if (per_step_all * (C + nseg - 1) <= budget) break;
+        C = std::max(1, C * 3 / 4);
+    }
+    const int nseg = (rs.fd_nt + C - 1) / C;
+    if (per_step_all * (C + nseg - 1) > budget)
+        return fail(c, S2D_ERR_NOMEM, "gradient needs %.1f GB of products/checkpoints, %.1f GB free",
+                    per_step_all * (C + nseg - 1) / 1e9, (double)free_b / 1e9);
+    std::vector<float *> prod(nshots), ckpt(nshots);
+    for (int s = 0; s < nshots; ++s) {
+        void *p;
+        int e = grad_alloc(c, g, (size_t)C * 4 * fb, &p);
+        if (e) return e;
+        prod[s] = static_cast<float *>(p);
+        ckpt[s] = nullptr;
+        if (nseg > 1) {
+            e = grad_alloc(c, g, (size_t)(nseg - 1) * 4 * fb, &p);
+            if (e) return e;
+            ckpt[s] = static_cast<float *>(p);
+        }
+        adj[s].prod = prod[s];
+        adj[s].nprod = (size_t)C * 4 * F;
+        adj[s].seis = adj_src + b.shots[s].seis_off;
+        b.shot_dev[s].prod = prod[s];
+        b.shot_dev[s].nprod = (size_t)C * 4 * F;
+    }
+    DevBuf adj_table;
+    CK(adj_table.alloc(sizeof(ShotDev) * nshots));
+    CK(cudaMemcpyAsync(adj_table.p, adj.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(b.shots_d.p, b.shot_dev.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice,
+                       c->stream));
+
+    LaunchCfg lc_fwd, lc_prod;
+    {
+        int e = launch_config(c, b.max_tasks, &lc_fwd);
+        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts);
+        if (e) return e;
+    }
+    StepArgs fa{};
+    fa.shots = b.shots_d.as<ShotDev>();
+    fa.groups = b.groups_d.as<GroupDev>();
+    fa.ngroups = (int)b.groups.size();
+    fa.total_tasks = 0;
+    for (auto &gr : b.groups) fa.total_tasks += gr.nshots * gr.nstrips * gr.nsegs;
+    fa.dt_factor = rs.dt_factor;
+    fa.fd_nt = rs.fd_nt;
+    bool graph_used = false;
+    // ---- forward sweep, saving the state at each segment start ----
+    auto save_ckpt = [&](int j) -> int {
+        const int par = (j * C) & 1;
+        for (int s = 0; s < nshots; ++s)
+            for (int f = 0; f < 4; ++f)
+                CK(cudaMemcpyAsync(ckpt[s] + ((size_t)j * 4 + f) * F, b.shot_dev[s].st[par][f], fb,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+        return S2D_OK;
+    };
+    for (int j = 0; j < nseg; ++j) {
+        const int k0 = j * C, n = std::min(C, rs.fd_nt - k0);
+        StepArgs a = fa;
+        if (j < nseg - 1) {
+            int e = save_ckpt(j);
+            if (!e) e = run_loop(c, b, lc_fwd, a, k0, n, use_graph, &launches, &graph_used);
+            if (e) return e;
+        } else {
+            a.flags = S2D_STEP_PRODUCTS;
+            a.prod_kt0 = k0;
+            int e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
+            if (e) return e;
+        }
+    }
+    // ---- adjoint source ----
+    DevBuf sumsq;
+    CK(sumsq.alloc(sizeof(double)));
+    CK(cudaMemsetAsync(sumsq.p, 0, sizeof(double), c->stream));
+    const cudaMemcpyKind dk = dev_seis ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (flags & S2D_GRAD_MISFIT) {
+        const float *obs = data;
+        if (!dev_seis) {
+            CK(cudaMemcpyAsync(adj_src, data, nseis * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+            obs = adj_src;
+        }
+        int e = launch_residual(b.seis_d, obs, adj_src, nseis, sumsq.as<double>(), c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "residual launch: %s", cudaGetErrorString((cudaError_t)e));
+    } else {
+        CK(cudaMemcpyAsync(adj_src, data, nseis * sizeof(float), dk, c->stream));
+    }
+    // ---- backward over the segments ----
+    int agrid = 1;
+    {
+        int bps = 0;
+        if (adjoint_kernel_occupancy(128, &bps) || bps < 1) bps = 1;
+        agrid = (int)std::max<long>(1, std::min<long>((long)c->sm_count * bps, (b.max_tasks * 32 + 127) / 128));
+    }
+    StepArgs aa = fa;
+    aa.shots = adj_table.as<ShotDev>();
+    aa.err = c->dev_err.as<int>();
+    for (int j = nseg - 1; j >= 0; --j) {
+        const int k0 = j * C, n = std::min(C, rs.fd_nt - k0);
+        if (j < nseg - 1) {
+            const int par = k0 & 1;
+            for (int s = 0; s < nshots; ++s)
+                for (int f = 0; f < 4; ++f)
+                    CK(cudaMemcpyAsync(b.shot_dev[s].st[par][f], ckpt[s] + ((size_t)j * 4 + f) * F, fb,
+                                       cudaMemcpyDeviceToDevice, c->stream));
+            StepArgs a = fa;
+            a.flags = S2D_STEP_PRODUCTS | S2D_STEP_NO_RECORD;
+            a.prod_kt0 = k0;
+            int e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
+            if (e) return e;
+        }
+        StepArgs a = aa;
+        a.prod_kt0 = k0;
+        int e = run_adjoint(c, b, g, a, k0 + n - 1, n, agrid, use_graph, &launches);
+        if (e) return e;
+    }
+    // ---- source term, chain rule, fold ----
+    std::vector<double> wv;
+    int inject_last;
+    if (wavelet) {
+        wv.assign(wavelet, wavelet + std::max(nwavelet, 0));
+        inject_last = nwavelet - 1;
+    } else {
+        wv = ricker(*wave, rs.nts);
+        inject_last = rs.nts;
+    }
+    std::vector<float> sa(rs.fd_nt);
+    std::vector<int> cells(nshots);
+    std::vector<double> vals(nshots);
+    const double sfac = (double)wave->fd_dt / (double)(m.dx * m.dz);
+    for (int s = 0; s < nshots; ++s) {
+        CK(cudaMemcpyAsync(sa.data(), sadj[s], sizeof(float) * rs.fd_nt, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        // kappa at the source, in double as the amplitude uses it (cpumodelling.cpp:136-140)
+        const int mx = std::min(std::max(b.shots[s].src_x - m.nb, 0), m.nx - 1);
+        const int mz = std::min(std::max(b.shots[s].src_z - m.nb, 0), m.nz - 1);
+        float vr[2];
+        CK(cudaMemcpy(&vr[0], m.vp.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&vr[1], m.rho.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
+        const double ksrc = ((double)vr[0] * (double)vr[0]) * (double)vr[1];
+        double v = 0;
+        for (int kt = 0; kt < rs.fd_nt; ++kt) {
+            const bool injected = kt <= inject_last;
+            const double wk = injected && kt < (int)wv.size() ? wv[kt] : 0.0;
+            if (injected) v += (double)sa[kt] * (wave->fd_dt * wk / (double)(m.dx * m.dz));
+            if (grad_wavelet)
+                grad_wavelet[(size_t)s * rs.fd_nt + kt] = injected ? (double)sa[kt] * sfac * ksrc : 0.0;
+        }
+        vals[s] = v;
+        cells[s] = (int)((size_t)(b.shots[s].src_x + S2D_GX) * m.ld + (b.shots[s].src_z + S2D_GZ));
+    }
+    void *p_cells, *p_vals, *p_ptrs, *p_tmp, *p_pad, *p_out = nullptr;
+    {
+        int e = grad_alloc(c, g, sizeof(int) * nshots, &p_cells);
+        if (!e) e = grad_alloc(c, g, sizeof(double) * nshots, &p_vals);
+        if (!e) e = grad_alloc(c, g, sizeof(float *) * 3 * nshots, &p_ptrs);
+        if (!e) e = grad_alloc(c, g, 3 * fb, &p_tmp);
+        if (!e) e = grad_alloc(c, g, 2 * fb, &p_pad);
+        if (!e && !dev_grad) e = grad_alloc(c, g, 2 * sizeof(float) * m.nx * m.nz, &p_out);
+        if (e) return e;
+    }
+    std::vector<float *> ptrs;
+    ptrs.insert(ptrs.end(), gk.begin(), gk.end());
+    ptrs.insert(ptrs.end(), gbx.begin(), gbx.end());
+    ptrs.insert(ptrs.end(), gbz.begin(), gbz.end());
+    CK(cudaMemcpyAsync(p_cells, cells.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(p_vals, vals.data(), sizeof(double) * nshots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(p_ptrs, ptrs.data(), sizeof(float *) * 3 * nshots, cudaMemcpyHostToDevice, c->stream));
+    float **dptrs = static_cast<float **>(p_ptrs);
+    float *out_vp = dev_grad ? grad_vp : static_cast<float *>(p_out);
+    float *out_rho = dev_grad ? grad_rho : static_cast<float *>(p_out) + (size_t)m.nx * m.nz;
+    {
+        int e = launch_gradient_finalize(dptrs, dptrs + nshots, dptrs + 2 * nshots, nshots,
+                                         static_cast<int *>(p_cells), static_cast<double *>(p_vals),
+                                         m.vp.as<float>(), m.rho.as<float>(), m.nx, m.nz, m.nb, m.ld,
+                                         static_cast<float *>(p_tmp), static_cast<float *>(p_pad),
+                                         static_cast<float *>(p_pad) + F, out_vp, out_rho, c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "gradient finalize: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    launches += 5;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    if (!dev_grad) {
+        CK(cudaMemcpyAsync(grad_vp, out_vp, sizeof(float) * m.nx * m.nz, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(grad_rho, out_rho, sizeof(float) * m.nx * m.nz, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (seis_out && !(fflags & S2D_SEIS_DEVICE))
+        CK(cudaMemcpyAsync(seis_out, b.seis_d, nseis * sizeof(float),
+                           dev_seis ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+    double ss = 0;
+    CK(cudaMemcpyAsync(&ss, sumsq.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (misfit) *misfit = 0.5 * ss;
+    // the forward state buffers now hold recomputed states: no continuation
+    b.kt_next = -1;
+    {
+        int e = check_device_error(c);
+        if (e) return e;
+    }
+    for (auto &bp : g.bufs) c->pool.give(std::move(bp));
+    g.bufs.clear();
+    if (stats) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        stats->loop_ms = ms;
+        stats->cell_updates = (double)m.nnx * m.nnz * nshots * rs.fd_nt;
+        stats->gcells_per_s = ms > 0 ? stats->cell_updates / (ms * 1e6) : 0.0;
+        stats->kernel_launches = launches;
+        stats->graph_used = graph_used ? 1 : 0;
+        stats->grad_segment = C;
+    }
+    c->last_segment = C;
+    return S2D_OK;
+}

@@ -1,0 +1,119 @@
+// Device helpers shared by the forward and adjoint step kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "s2d_internal.h"
+
+namespace s2d {
+
+static constexpr unsigned kFull = 0xffffffffu;
+
+static __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+static __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+
+// Coefficients (c0, c1) of a0*(f[i]-f[i-1]) + a1*(f[i+1]-f[i-2]) per row of
+// the backward operators: 4th order on rows [2, n-2], plain difference on
+// rows 1 and n-1, zero on row 0 and outside the grid
+// (cpu_modelling_kernels.cpp:201-258).
+static __device__ __forceinline__ void dm_coef(int i, int n, float &c0, float &c1) {
+    if (i >= 2 && i <= n - 2) { c0 = kA0; c1 = kA1; }
+    else if (i == 1 || i == n - 1) { c0 = 1.0f; c1 = 0.0f; }
+    else { c0 = 0.0f; c1 = 0.0f; }
+}
+// Forward operators a0*(f[i+1]-f[i]) + a1*(f[i+2]-f[i-1]): 4th order on rows
+// [1, n-3], plain difference on rows 0 and n-2, zero on row n-1
+// (cpu_modelling_kernels.cpp:260-316).
+static __device__ __forceinline__ void dp_coef(int i, int n, float &c0, float &c1) {
+    if (i >= 1 && i <= n - 3) { c0 = kA0; c1 = kA1; }
+    else if (i == 0 || i == n - 2) { c0 = 1.0f; c1 = 0.0f; }
+    else { c0 = 0.0f; c1 = 0.0f; }
+}
+
+static __device__ __forceinline__ float comp(const float4 &v, int i) {
+    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
+// Per-lane constants of one task: the lane's four rows and the shot data.
+struct Lane {
+    float4 zc[4];                 // damp1a, kz*damp1a1, damp1b, kz*damp1b1 per row
+    float cm0[4], cm1[4], cp0[4], cp1[4];
+    int z0;                       // first row of the lane
+    bool owner;                   // writes its rows (lanes 1..30)
+    int sdz;                      // source row - z0
+    float amp;                    // source term of this step
+};
+
+static __device__ __forceinline__ void lane_setup(Lane &ln, const ShotDev &S, int c, int lane, int kt) {
+    ln.z0 = c + S2D_ZPT * lane;
+    const float4 *zc = S.zcoef + (ln.z0 + S2D_GZ);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        ln.zc[i] = __ldg(zc + i);
+        dm_coef(ln.z0 + i, S.nnz, ln.cm0[i], ln.cm1[i]);
+        dp_coef(ln.z0 + i, S.nnz, ln.cp0[i], ln.cp1[i]);
+    }
+    ln.owner = lane >= 1 && lane <= 30;
+    ln.sdz = S.src_z - ln.z0;
+    ln.amp = __ldg(S.amp + kt);
+}
+
+// Map a flat task index to (shot, strip, first column, segment length).
+// Order 0 runs the shots of one (strip, segment) on consecutive warps, so they
+// share that tile of the model through L2.  Order 1 runs the strips of one
+// (shot, segment) on consecutive warps, so the warps of a block read adjacent
+// pieces of each column (contiguous DRAM rows); the shots of one segment still
+// run close together and share the segment's materials in L2.
+static __device__ __forceinline__ const ShotDev &task_of(const StepArgs &a, int t, int &strip, int &xa, int &seg_len) {
+    int g = 0;
+    while (g + 1 < a.ngroups && __ldg(&a.groups[g + 1].task_begin) <= t) ++g;
+    const GroupDev &G = a.groups[g];
+    int tl = t - G.task_begin;
+    int s;
+    if (a.task_order == 0) {
+        s = G.shot0 + tl % G.nshots;
+        tl /= G.nshots;
+        strip = tl % G.nstrips;
+        xa = (tl / G.nstrips) * G.seg_len;
+    } else {
+        strip = tl % G.nstrips;
+        tl /= G.nstrips;
+        s = G.shot0 + tl % G.nshots;
+        xa = (tl / G.nshots) * G.seg_len;
+    }
+    seg_len = G.seg_len;
+    return a.shots[s];
+}
+
+
+// Debug self-check (built with -DS2D_DEVICE_CHECKS): the ranges every access
+// of one task touches, from the runtime tables.  A failed check records a
+// code in the error word and the task is skipped.
+static __device__ __forceinline__ bool task_in_bounds(const StepArgs &a, const ShotDev &S, int strip, int xa,
+                                                      int seg_len, int kt, bool prod, int code) {
+#ifdef S2D_DEVICE_CHECKS
+    const size_t ld = (size_t)S.ld;
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+    const long c = (long)strip * S2D_STRIP_OUT - 4;
+    const long lo = (long)(xa - 3 + S2D_GX) * (long)ld + (c + S2D_GZ);
+    const long hi = (long)(xb + 2 + S2D_GX) * (long)ld + (c + S2D_GZ) + 127;
+    int bad = 0;
+    if (ld % 4 || (c + S2D_GZ) % 4) bad = 1;
+    else if (F > S.nfield) bad = 2;
+    else if (lo < 0 || hi >= (long)F) bad = 3;
+    else if (c + 127 + S2D_GZ >= (long)ld) bad = 4;
+    else if (kt < 0 || kt >= a.fd_nt) bad = 5;
+    else if (prod && ((long)(kt - a.prod_kt0) < 0 || (size_t)(kt - a.prod_kt0 + 1) * 4 * F > S.nprod)) bad = 6;
+    else if ((size_t)S.nrec * S.real_nt > S.nseis) bad = 7;
+    else if (S.src_x < 0 || S.src_x >= S.nnx || S.src_z < 0 || S.src_z >= S.nnz) bad = 8;
+    if (bad) {
+        if (a.err) atomicCAS(a.err, 0, (code << 8) | bad);
+        return false;
+    }
+#endif
+    return true;
+}
+
+}  // namespace s2d

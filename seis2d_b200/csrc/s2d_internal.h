@@ -42,9 +42,19 @@ struct ShotDev {
     const int *rec_ptr;            // [nnx + 1] receivers grouped by column (CSR)
     const int *rec_z;              // padded row of each receiver entry
     const int *rec_id;             // index of the entry's trace in seis
-    float *seis;                   // [nrec][real_nt]
+    float *seis;                   // [nrec][real_nt]; the adjoint reads its source here
     int real_nt;
     int pad_;
+    // gradient runs only
+    float *prod;                   // [steps][4][field]: D-x vx, D-z vz, D+x p, D+z p of each step
+    float *grad[3];                // accumulators dJ/dkappa, dJ/dbx, dJ/dbz (padded layout)
+    float *srcadj;                 // [fd_nt] adjoint pressure at the source after each step
+    // element counts of the buffers above (device self-checks, S2D_DEVICE_CHECKS)
+    size_t nfield;                 // every per-cell field
+    size_t nprod;                  // prod
+    size_t nseis;                  // seis (this shot's block)
+    int nrec;
+    int pad3_;
 };
 
 // Shots that share one grid shape; their tasks are interleaved so that the
@@ -76,15 +86,21 @@ struct StepArgs {
     int spin_limit;       // polls of an mbarrier before a wait counts as timed out
     int fault_iter;       // test knob: pipeline iteration whose copies are not issued (-1: none)
     int task_order;       // 0: shot fastest, 1: strip fastest (see task_of)
-    int pad_;
+    int flags;            // S2D_STEP_* bits
+    int prod_kt0;         // FD step stored in plane 0 of ShotDev::prod
+    int pad2_;
 };
+
+#define S2D_STEP_NO_RECORD 1  // forward: do not sample receivers; adjoint: do not inject the adjoint source
+#define S2D_STEP_PRODUCTS 2   // forward also writes its four derivatives to ShotDev::prod
 
 // Device error bits reported through StepArgs::err.
 #define S2D_DEV_ERR_WAIT 1    // a pipeline wait gave up (bounded spin ran out)
 #define S2D_DEV_ERR_DRAIN 2   // copies still in flight after the bounded drain
 
 // Step kernel variants.
-enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2 };
+enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
+                   kVariantLdgProducts = 3 /* plain loads + S2D_STEP_PRODUCTS, gradient runs */ };
 
 // Shared memory of one pipeline stage: 7 slots of one 128-row column each
 // (vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3).
@@ -99,6 +115,17 @@ inline size_t bulk_smem_bytes(int warps_per_block, int stages) {
 int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int block, size_t smem,
                 void *stream);
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
+// Adjoint FD step (step kt = args.kt_base - kt_off) and the gradient finalisation.
+int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream);
+int adjoint_kernel_occupancy(int block, int *blocks_per_sm);
+// Sum the shots' accumulators, apply the buoyancy averaging transpose and the
+// kappa = vp^2 rho, b = 1/rho chain rule, fold the sponge onto the model.
+int launch_gradient_finalize(float *const *gk, float *const *gbx, float *const *gbz, int nshots,
+                             const int *src_cells, const double *src_vals, const float *vp, const float *rho,
+                             int nx, int nz, int nb, int ld, float *tmp3, float *gvp_pad, float *grho_pad,
+                             float *grad_vp, float *grad_rho, void *stream);
+// Residual d - d_obs in place of d_obs... : res[i] = seis[i] - obs[i]; partial sums of res^2.
+int launch_residual(const float *seis, const float *obs, float *res, size_t n, double *sumsq, void *stream);
 int launch_prepare_model(const float *vp, const float *rho, int nx, int nz, int nb, int ld,
                          float *kappa, float *bue_scratch, float *bx, float *bz, void *stream);
 int step_kernel_prepare(int variant, size_t smem);

@@ -32,62 +32,11 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
-#include "s2d_internal.h"
+#include "s2d_device.cuh"
 
 namespace s2d {
 
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
-__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
-
-// Coefficients (c0, c1) of a0*(f[i]-f[i-1]) + a1*(f[i+1]-f[i-2]) per row of
-// the backward operators: 4th order on rows [2, n-2], plain difference on
-// rows 1 and n-1, zero on row 0 and outside the grid
-// (cpu_modelling_kernels.cpp:201-258).
-__device__ __forceinline__ void dm_coef(int i, int n, float &c0, float &c1) {
-    if (i >= 2 && i <= n - 2) { c0 = kA0; c1 = kA1; }
-    else if (i == 1 || i == n - 1) { c0 = 1.0f; c1 = 0.0f; }
-    else { c0 = 0.0f; c1 = 0.0f; }
-}
-// Forward operators a0*(f[i+1]-f[i]) + a1*(f[i+2]-f[i-1]): 4th order on rows
-// [1, n-3], plain difference on rows 0 and n-2, zero on row n-1
-// (cpu_modelling_kernels.cpp:260-316).
-__device__ __forceinline__ void dp_coef(int i, int n, float &c0, float &c1) {
-    if (i >= 1 && i <= n - 3) { c0 = kA0; c1 = kA1; }
-    else if (i == 0 || i == n - 2) { c0 = 1.0f; c1 = 0.0f; }
-    else { c0 = 0.0f; c1 = 0.0f; }
-}
-
-__device__ __forceinline__ float comp(const float4 &v, int i) {
-    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
-}
-
-// Per-lane constants of one task: the lane's four rows and the shot data.
-struct Lane {
-    float4 zc[4];                 // damp1a, kz*damp1a1, damp1b, kz*damp1b1 per row
-    float cm0[4], cm1[4], cp0[4], cp1[4];
-    int z0;                       // first row of the lane
-    bool owner;                   // writes its rows (lanes 1..30)
-    int sdz;                      // source row - z0
-    float amp;                    // source term of this step
-};
-
-__device__ __forceinline__ void lane_setup(Lane &ln, const ShotDev &S, int c, int lane, int kt) {
-    ln.z0 = c + S2D_ZPT * lane;
-    const float4 *zc = S.zcoef + (ln.z0 + S2D_GZ);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        ln.zc[i] = __ldg(zc + i);
-        dm_coef(ln.z0 + i, S.nnz, ln.cm0[i], ln.cm1[i]);
-        dp_coef(ln.z0 + i, S.nnz, ln.cp0[i], ln.cp1[i]);
-    }
-    ln.owner = lane >= 1 && lane <= 30;
-    ln.sdz = S.src_z - ln.z0;
-    ln.amp = __ldg(S.amp + kt);
-}
 
 // Pressure at column P from vx at P-2..P+1 (q0..q3), old px, pz, kappa and vz
 // at P (cpu_modelling_kernels.cpp:201-258 and 335-351, cpumodelling.cpp:136-142).
@@ -95,7 +44,7 @@ __device__ __forceinline__ void lane_setup(Lane &ln, const ShotDev &S, int c, in
 __device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int P, const float4 &q0,
                                            const float4 &q1, const float4 &q2, const float4 &q3, const float4 &px,
                                            const float4 &pz, const float4 &kk, const float4 &vz, float4 &pxn,
-                                           float4 &pzn) {
+                                           float4 &pzn, float4 &dxv, float4 &dzv) {
     const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
     float cx0, cx1;
     dm_coef(P, S.nnx, cx0, cx1);
@@ -110,6 +59,8 @@ __device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int
     const float dx1 = cx0 * (q2.y - q1.y) + cx1 * (q3.y - q0.y);
     const float dx2 = cx0 * (q2.z - q1.z) + cx1 * (q3.z - q0.z);
     const float dx3 = cx0 * (q2.w - q1.w) + cx1 * (q3.w - q0.w);
+    dxv = make_float4(dx0, dx1, dx2, dx3);
+    dzv = make_float4(dz0, dz1, dz2, dz3);
     pxn.x = xc.x * px.x + (xc.y * kk.x) * dx0;
     pxn.y = xc.x * px.y + (xc.y * kk.y) * dx1;
     pxn.z = xc.x * px.z + (xc.y * kk.z) * dx2;
@@ -141,7 +92,7 @@ __device__ __forceinline__ void record(const Lane &ln, const ShotDev &S, int P, 
 __device__ __forceinline__ void v_update(const Lane &ln, const ShotDev &S, int V, const float4 &p0,
                                          const float4 &p1, const float4 &p2, const float4 &p3, const float4 &vx,
                                          const float4 &vz, const float4 &bx, const float4 &bz, float4 &vxn,
-                                         float4 &vzn) {
+                                         float4 &vzn, float4 &dxp, float4 &dzp) {
     const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
     float ux0, ux1;
     dp_coef(V, S.nnx, ux0, ux1);
@@ -157,6 +108,8 @@ __device__ __forceinline__ void v_update(const Lane &ln, const ShotDev &S, int V
     const float ez1 = ln.cp0[1] * (q.z - q.y) + ln.cp1[1] * (q.w - q.x);
     const float ez2 = ln.cp0[2] * (q.w - q.z) + ln.cp1[2] * (dn_x - q.y);
     const float ez3 = ln.cp0[3] * (dn_x - q.w) + ln.cp1[3] * (dn_y - q.z);
+    dxp = make_float4(ex0, ex1, ex2, ex3);
+    dzp = make_float4(ez0, ez1, ez2, ez3);
     vxn.x = xc.z * vx.x + (xc.w * bx.x) * ex0;
     vxn.y = xc.z * vx.y + (xc.w * bx.y) * ex1;
     vxn.z = xc.z * vx.z + (xc.w * bx.z) * ex2;
@@ -167,35 +120,10 @@ __device__ __forceinline__ void v_update(const Lane &ln, const ShotDev &S, int V
     vzn.w = ln.zc[3].z * vz.w + (ln.zc[3].w * bz.w) * ez3;
 }
 
-// Map a flat task index to (shot, strip, first column, segment length).
-// Order 0 runs the shots of one (strip, segment) on consecutive warps, so they
-// share that tile of the model through L2.  Order 1 runs the strips of one
-// (shot, segment) on consecutive warps, so the warps of a block read adjacent
-// pieces of each column (contiguous DRAM rows); the shots of one segment still
-// run close together and share the segment's materials in L2.
-__device__ __forceinline__ const ShotDev &task_of(const StepArgs &a, int t, int &strip, int &xa, int &seg_len) {
-    int g = 0;
-    while (g + 1 < a.ngroups && __ldg(&a.groups[g + 1].task_begin) <= t) ++g;
-    const GroupDev &G = a.groups[g];
-    int tl = t - G.task_begin;
-    int s;
-    if (a.task_order == 0) {
-        s = G.shot0 + tl % G.nshots;
-        tl /= G.nshots;
-        strip = tl % G.nstrips;
-        xa = (tl / G.nstrips) * G.seg_len;
-    } else {
-        strip = tl % G.nstrips;
-        tl /= G.nstrips;
-        s = G.shot0 + tl % G.nshots;
-        xa = (tl / G.nshots) * G.seg_len;
-    }
-    seg_len = G.seg_len;
-    return a.shots[s];
-}
-
 // ---------------------------------------------------------------- LDG variant
 
+// PROD: also write the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).
+template <bool PROD>
 __global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
@@ -209,13 +137,16 @@ __global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restric
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
         const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
         const int xb = min(S.nnx, xa + seg_len);
         const size_t ld = (size_t)S.ld;
         const int c = strip * S2D_STRIP_OUT - 4;
         Lane ln;
         lane_setup(ln, S, c, lane, kt);
-        const bool rec = rec_step && slot < S.real_nt;
+        const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
         const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+        const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+        float *pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
         const float *pxi = S.st[par][0] + off, *pzi = S.st[par][1] + off;
         const float *vxi = S.st[par][2] + off, *vzi = S.st[par][3] + off;
         float *pxo = S.st[par ^ 1][0] + off, *pzo = S.st[par ^ 1][1] + off;
@@ -234,13 +165,17 @@ __global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restric
             vq0 = vq1; vq1 = vq2; vq2 = vq3;
             vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
             const float4 vz = ld4(vzi + colP);
-            float4 pxn, pzn;
+            float4 pxn, pzn, dxv, dzv;
             const float4 pn = p_update(ln, S, P, vq0, vq1, vq2, vq3, ld4(pxi + colP), ld4(pzi + colP),
-                                       ld4(kap + colP), vz, pxn, pzn);
+                                       ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
             const bool in_seg = P >= xa && P < xb;
             if (in_seg && ln.owner) {
                 st4(pxo + colP, pxn);
                 st4(pzo + colP, pzn);
+                if (PROD) {
+                    st4(pr + colP, dxv);
+                    st4(pr + F + colP, dzv);
+                }
             }
             if (rec && in_seg) record(ln, S, P, pn, slot);
             pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
@@ -248,11 +183,16 @@ __global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restric
             if (L >= xa + 3) {
                 const int V = L - 3;
                 const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-                float4 vxn, vzn;
-                v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+                float4 vxn, vzn, dxp, dzp;
+                v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp,
+                         dzp);
                 if (ln.owner) {
                     st4(vxo + colV, vxn);
                     st4(vzo + colV, vzn);
+                    if (PROD) {
+                        st4(pr + 2 * F + colV, dxp);
+                        st4(pr + 3 * F + colV, dzp);
+                    }
                 }
             }
         }
@@ -339,7 +279,7 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
         const int c = strip * S2D_STRIP_OUT - 4;
         Lane ln;
         lane_setup(ln, Sh, c, lane, kt);
-        const bool rec = rec_step && slot < Sh.real_nt;
+        const bool rec = rec_step && slot < Sh.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
         // column 0 of the warp's strip in each field (row c), and this lane's rows
         const size_t wofs = (size_t)(c + S2D_GZ) + (size_t)S2D_GX * ld;
         const size_t lofs = wofs + (size_t)(S2D_ZPT * lane);
@@ -405,9 +345,9 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
             if (L >= xa) {
                 const int P = L - 1;
                 const float4 vz = st[4 * 32];
-                float4 pxn, pzn;
+                float4 pxn, pzn, dxv, dzv;
                 const float4 pn = p_update(ln, Sh, P, vq0, vq1, vq2, vq3, st[1 * 32], st[2 * 32], st[3 * 32], vz,
-                                           pxn, pzn);
+                                           pxn, pzn, dxv, dzv);
                 const bool in_seg = P >= xa && P < xb;
                 const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
                 if (in_seg && ln.owner) {
@@ -420,8 +360,8 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
                 if (L >= xa + 3) {
                     const int V = L - 3;
                     const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-                    float4 vxn, vzn;
-                    v_update(ln, Sh, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn);
+                    float4 vxn, vzn, dxp, dzp;
+                    v_update(ln, Sh, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn, dxp, dzp);
                     if (ln.owner) {
                         st4(vxo + colV, vxn);
                         st4(vzo + colV, vzn);
@@ -487,8 +427,10 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_bulk<1><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantBulk128)
         step_kernel_bulk<4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgProducts)
+        step_kernel_ldg<true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
-        step_kernel_ldg<<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        step_kernel_ldg<false><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
@@ -510,12 +452,13 @@ namespace {
 const void *kernel_of(int variant) {
     if (variant == kVariantBulk) return (const void *)step_kernel_bulk<1>;
     if (variant == kVariantBulk128) return (const void *)step_kernel_bulk<4>;
-    return (const void *)step_kernel_ldg;
+    if (variant == kVariantLdgProducts) return (const void *)step_kernel_ldg<true>;
+    return (const void *)step_kernel_ldg<false>;
 }
 }  // namespace
 
 int step_kernel_prepare(int variant, size_t smem) {
-    if (variant == kVariantLdg) return 0;
+    if (variant == kVariantLdg || variant == kVariantLdgProducts) return 0;
     const void *k = kernel_of(variant);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -523,8 +466,8 @@ int step_kernel_prepare(int variant, size_t smem) {
 }
 
 int step_kernel_occupancy(int variant, int block, size_t smem, int *blocks_per_sm) {
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block,
-                                                              variant == kVariantLdg ? 0 : smem);
+    const bool ldg = variant == kVariantLdg || variant == kVariantLdgProducts;
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block, ldg ? 0 : smem);
 }
 
 int step_kernel_attributes(int variant, int *regs, int *local_bytes) {
