@@ -50,6 +50,71 @@ WORKLOADS = {
 }
 
 
+# ---------------------------------------------------------------------------
+# Seeded synthetic models of the other workload configurations (the
+# reference's own model files are not distributed).
+
+def gardner(vp):
+    return (310.0 * np.power(vp.astype(np.float64), 0.25)).astype(np.float32)
+
+
+def salt_model(seed=20261203 + 3):
+    """3201 x 1201, d = 7.62 m: 60 cells of water (1500 m/s), then 1600 -> 4000 m/s
+    with a +-5% smoothed Gaussian perturbation, and a 12-vertex salt polygon
+    (4500 m/s) in the middle third; Gardner density."""
+    from scipy.ndimage import gaussian_filter
+    nx, nz = 3201, 1201
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz, dtype=np.float64)[None, :]
+    base = 1600.0 + 2400.0 * (z - 60) / (nz - 1 - 60)
+    g = gaussian_filter(rng.standard_normal((nx, nz)), 10.0)
+    g /= g.std()
+    vp = base * (1.0 + 0.05 * g)
+    vp[:, :60] = 1500.0
+    cx, cz, R = rng.uniform(nx / 3, 2 * nx / 3), rng.uniform(400, 800), 300.0
+    ang = np.sort(rng.uniform(0, 2 * np.pi, 12))
+    rad = rng.uniform(0.5, 1.0, 12) * R
+    px, pz = cx + rad * np.cos(ang), cz + rad * np.sin(ang)
+    X, Z = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(nz, dtype=np.float64), indexing="ij")
+    inside = np.zeros((nx, nz), bool)
+    for k in range(12):  # even-odd rule
+        x1, z1, x2, z2 = px[k], pz[k], px[(k + 1) % 12], pz[(k + 1) % 12]
+        cross = ((z1 > Z) != (z2 > Z)) & (X < (x2 - x1) * (Z - z1) / (z2 - z1 + 1e-300) + x1)
+        inside ^= cross
+    vp[inside & (Z >= 60)] = 4500.0
+    vp = vp.astype(np.float32)
+    return vp, gardner(vp)
+
+
+def layered_model(nx, nz, seed):
+    """4-8 seeded layers, vp ~ U[1500, 4500], Gardner density."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(4, 9))
+    depths = np.sort(rng.uniform(0.1, 0.95, n - 1)) * nz
+    vels = rng.uniform(1500.0, 4500.0, n)
+    z = np.arange(nz)[None, :].repeat(nx, 0)
+    vp = np.full((nx, nz), vels[0], np.float32)
+    for k, d in enumerate(depths):
+        vp[z >= d] = vels[k + 1]
+    return vp, gardner(vp)
+
+
+def fwi_models(seed=20261203 + 5):
+    """1201 x 401, d = 10 m: true = 1500 -> 3500 m/s gradient + two Gaussian
+    anomalies of +-300 m/s (sigma 20 cells, seeded centres); start = the
+    gradient alone; constant density 2000 kg/m^3 in both."""
+    nx, nz = 1201, 401
+    rng = np.random.default_rng(seed)
+    X, Z = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(nz, dtype=np.float64), indexing="ij")
+    start = 1500.0 + 2000.0 * Z / (nz - 1)
+    true = start.copy()
+    for amp in (300.0, -300.0):
+        cx, cz = rng.uniform(200, 1000), rng.uniform(100, 300)
+        true += amp * np.exp(-((X - cx) ** 2 + (Z - cz) ** 2) / (2 * 20.0 ** 2))
+    rho = np.full((nx, nz), 2000.0, np.float32)
+    return true.astype(np.float32), start.astype(np.float32), rho
+
+
 def build_workload(w, rank=0, world=1):
     nx, nz = w["nx"], w["nz"]
     vp = np.empty((nx, nz), np.float32)
@@ -136,6 +201,120 @@ def traffic_per_launch(workload):
         if t:
             return float(t["dram_bytes_per_launch"])
     return None
+
+
+# ---------------------------------------------------------------------------
+# Other configurations: single-shot c1/c3, uneven batch c4, gradient c5
+
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, out
+
+
+def surface_shots(nx, d, nshots, nrec=None):
+    src = [(float(int(round((k + 0.5) * nx / nshots)) * d), 2 * d) for k in range(nshots)]
+    n = nrec or nx
+    rec = np.stack([np.arange(n, dtype=np.float32) * d, np.full(n, 2 * d, np.float32)], 1)
+    return src, rec
+
+
+def extra_legs(device):
+    """Rates of the other BASELINE configurations (each a bounded part of its job)."""
+    import torch
+    from seis2d_b200 import Context, Shot, Wave, derive_steps
+    peak, _ = measured_peak()
+    out = {}
+    with Context(device) as ctx:
+        # c1: 1000x1000, nb 40, 15 Hz, dt 1 ms, nt 2000, 1 shot, full job
+        w1 = WORKLOADS["c1"]
+        vp, rho, src, rec = build_workload(w1)
+        m = ctx.model(vp, rho, w1["d"], w1["d"], w1["nb"])
+        wave = Wave(w1["T"], w1["dt"], w1["dt"], w1["f"])
+        st = derive_steps(wave)
+        buf = torch.zeros(rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
+        shots = [Shot(m, src[0], rec)]
+        ctx.forward(shots, wave, kt_count=50, out=buf)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
+        cells = m.padded_cells * st["fd_nt"]
+        out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
+                     "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": 44 * cells / t / 1e9 / peak,
+                     "note": "whole job ~37 MB of state: L2-resident"}
+        m.release()
+        # c3: salt 3201x1201, d 7.62, nb 50, 20 Hz, dt 0.6 ms, nt 10000, 1 shot; 1000 of the 10000 steps
+        vp, rho = salt_model()
+        m = ctx.model(vp, rho, 7.62, 7.62, 50)
+        wave = Wave(6.0, 0.0006, 0.0006, 20.0)
+        st = derive_steps(wave)
+        src = (float(1600 * np.float32(7.62)), 2 * 7.62)
+        rec = np.stack([np.arange(3201, dtype=np.float32) * np.float32(7.62), np.full(3201, 2 * 7.62, np.float32)], 1)
+        buf = torch.zeros(3201 * st["real_nt"], dtype=torch.float32, device="cuda")
+        shots = [Shot(m, src, rec)]
+        ctx.forward(shots, wave, kt_count=100, out=buf)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=1000, out=buf, sync=False))
+        cells = m.padded_cells * 1000
+        rate = cells / t / 1e9
+        out["c3"] = {"workload": "3201x1201 salt (seeded), d 7.62, nb 50, 1 shot, 1000 of 10000 steps",
+                     "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (m.padded_cells * st["fd_nt"]),
+                     "roofline_frac": 44 * rate / peak}
+        m.release()
+        # c4: 48 shots on three layered models of uneven size, one launch sequence; 300 of 3000 steps
+        wave = Wave(2.3996, 0.0008, 0.0008, 15.0)
+        st = derive_steps(wave)
+        shots, cells_step, total_rec = [], 0, 0
+        models = []
+        for k, (nx, nz) in enumerate([(601, 301), (1201, 601), (2401, 801)]):
+            vp, rho = layered_model(nx, nz, 20261203 + 40 + k)
+            mm = ctx.model(vp, rho, 10.0, 10.0, 50)
+            models.append(mm)
+            src, rec = surface_shots(nx, 10.0, 16)
+            shots += [Shot(mm, s_, rec) for s_ in src]
+            cells_step += 16 * mm.padded_cells
+            total_rec += 16 * rec.shape[0]
+        buf = torch.zeros(total_rec * st["real_nt"], dtype=torch.float32, device="cuda")
+        ctx.forward(shots, wave, kt_count=30, out=buf)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=30, kt_count=300, out=buf, sync=False))
+        rate = cells_step * 300 / t / 1e9
+        tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
+        prate = cells_step * 60 / tp / 1e9
+        out["c4"] = {"workload": "48 shots on 601x301 / 1201x601 / 2401x801 layered models (16 each), nb 50, "
+                                 "one launch per step for all; 300 of 3000 steps",
+                     "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (cells_step / 48 * st["fd_nt"]),
+                     "plain_gcells_per_s": prate, "roofline_frac": 44 * rate / peak}
+        for mm in models:
+            mm.release()
+        # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
+        true, start, rho = fwi_models()
+        wave = Wave(3.0, 0.001, 0.001, 10.0)
+        st = derive_steps(wave)
+        src, rec = surface_shots(1201, 10.0, 32)
+        mt = ctx.model(true, rho, 10.0, 10.0, 50)
+        dobs = torch.zeros(32 * rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
+        ctx.forward([Shot(mt, s_, rec) for s_ in src], wave, out=dobs)
+        mt.release()
+        ms = ctx.model(start, rho, 10.0, 10.0, 50)
+        shots = [Shot(ms, s_, rec) for s_ in src]
+        fbuf = torch.zeros_like(dobs)
+        ctx.forward(shots, wave, kt_count=20, out=fbuf)
+        tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
+        gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
+        grho = torch.zeros_like(gvp)
+        ctx.gradient(shots[:2], wave, dobs[: 2 * rec.shape[0] * st["real_nt"]], misfit=True, grad_vp=gvp,
+                     grad_rho=grho)
+        tg, g = _timed(lambda: ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho))
+        out["c5_gradient"] = {"workload": "FWI gradient, 1201x401 (seeded gradient + two +-300 m/s anomalies; "
+                                          "start = gradient), rho 2000, nb 50, 32 shots x 1201 receivers, nt 3000",
+                              "gradient_s_per_shot": tg / 32, "forward_s_per_shot": tf / 32,
+                              "gradient_over_forward": tg / tf, "misfit": g.misfit,
+                              "checkpoint_interval": int(g.stats.grad_segment),
+                              "forward_gcells_per_s": ms.padded_cells * 32 * st["fd_nt"] / tf / 1e9}
+        ms.release()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -229,6 +408,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the c1/c3/c4/c5 legs")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -370,6 +550,10 @@ def main():
             cpu = {"unavailable": err}
 
     ctx.close()
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        torch.cuda.empty_cache()
+        extras = extra_legs(local)
     if rank == 0:
         line = {
             "metric": "padded-grid cell-updates per second, batched forward modelling",
@@ -382,7 +566,7 @@ def main():
                        "parallelism": f"shots sharded over {world} GPU(s), no collective"},
             "shots_per_s": value * 1e9 / (cells_shot * fd_nt),
             "plain": plain, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": launches,
+            "gpu_launches": launches, "other_configs": extras,
         }
         print(json.dumps(line))
     if dist is not None:

@@ -137,6 +137,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *   "seg_len"     columns per x-segment of a warp task, 0 = automatic
  *   "spin_limit"  polls of a pipeline barrier before the wait gives up and the
  *                 call returns S2D_ERR_TIMEOUT (default 2^20)
+ *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
+ *                 run needs (default 64)
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
  *                 longest that fits in free device memory (default)
  *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of

@@ -76,15 +76,11 @@ struct Batch {
     std::vector<GroupDev> groups;    // batched mode
     std::vector<std::unique_ptr<DevBuf>> state;   // 8 per shot
     std::vector<std::unique_ptr<DevBuf>> aux;     // amp tables, receiver tables
-    DevBuf shots_d, groups_d, args_d;
+    DevBuf shots_d, groups_d;
     DevBuf seis_int;                 // internal seismogram buffer (host output)
     float *seis_d = nullptr;         // where the kernels record
     size_t seis_elems = 0;
     long max_tasks = 0;              // largest task count of one launch sequence
-    std::map<std::vector<long>, cudaGraphExec_t> graphs;  // by (steps, launch config)
-    ~Batch() {
-        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
-    }
 };
 
 // Device buffers of finished batches, kept for reuse by the next batch of
@@ -135,8 +131,19 @@ struct Ctx {
     int opt_fault_iter = -1;  // test knob, see s2d_set_option
     int opt_order = 1;        // task order (StepArgs::task_order)
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
+    int opt_graph_chunk = 64; // FD steps per captured graph
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
+    // Launch-argument block read by every step launch, and the graphs of step
+    // launches captured against it (by step count and launch configuration);
+    // kept for the context's lifetime, so later runs replay them.
+    DevBuf args_d;
+    std::map<std::vector<long>, cudaGraphExec_t> graphs;
+    std::map<std::vector<long>, cudaGraphExec_t> adj_graphs;  // by (step count, grid)
+    ~Ctx() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        for (auto &kv : adj_graphs) cudaGraphExecDestroy(kv.second);
+    }
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err = "no error";
@@ -170,15 +177,26 @@ int fail(Ctx *c, int code, const char *fmt, ...) {
                         "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
     } while (0)
 
-// Columns per x-segment for a group: long segments amortise the 3-column
-// warm-up of the streaming window; enough tasks must exist to fill the GPU.
+// Columns per x-segment for a group.  Each task streams L + 6 columns (3 of
+// warm-up, 3 of halo); warps loop over tasks, so a launch takes about
+// ceil(tasks / resident warps) rounds of the longest task.  Pick the L with
+// the fewest round-columns (longer segments on ties).
 int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps) {
-    static const int cand[] = {1024, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16};
+    static const int cand[] = {1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16};
+    int best = 16;
+    double best_cost = 1e300;
     for (int L : cand) {
-        long nsegs = (nnx + L - 1) / L;
-        if (tasks_per_seg * nsegs >= 24 * resident_warps) return std::min(L, nnx);
+        const int Lc = std::min(L, nnx);
+        const long nsegs = (nnx + Lc - 1) / Lc;
+        const long tasks = tasks_per_seg * nsegs;
+        const long rounds = (tasks + resident_warps - 1) / std::max(1L, resident_warps);
+        const double cost = (double)rounds * (Lc + 6);
+        if (cost < best_cost * 0.999) {
+            best_cost = cost;
+            best = Lc;
+        }
     }
-    return 16;
+    return best;
 }
 
 int build_coef(Ctx *c, Model &m, float fd_dt) {
@@ -229,36 +247,18 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant = -1) {
     return S2D_OK;
 }
 
-// One pass over `nsteps` FD steps starting at kt_begin, for the launch
-// arguments `args` (a whole batch, or one shot of a plain run).
-int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin, int nsteps, bool use_graph,
-             int *launches, bool *graph_used) {
-    if (nsteps <= 0) return S2D_OK;
-    args.kt_base = kt_begin;
-    args.stages = lc.stages;
-    args.err = c->dev_err.as<int>();
-    args.spin_limit = c->opt_spin_limit;
-    args.fault_iter = c->opt_fault_iter;
-    args.task_order = c->opt_order;
-    StepArgs *args_d = b.args_d.as<StepArgs>();
-    int e = launch_set_args(args, args_d, c->stream);
-    if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
-    *launches += 1;
-    if (!use_graph) {
-        for (int k = 0; k < nsteps; ++k) {
-            e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
-            if (e) return fail(c, S2D_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)e));
-        }
-        *launches += nsteps;
-        return S2D_OK;
-    }
-    const std::vector<long> key = {nsteps, lc.variant, lc.block, lc.stages, (long)lc.smem, lc.grid};
-    auto it = b.graphs.find(key);
-    if (it == b.graphs.end()) {
+// Graph of `n` step launches (kt_off = 0..n-1) for one launch configuration,
+// captured once per (n, configuration) and replayed; the launches read their
+// step base from the device argument block written just before each replay.
+int step_graph(Ctx *c, const LaunchCfg &lc, int n, cudaGraphExec_t *out) {
+    StepArgs *args_d = c->args_d.as<StepArgs>();
+    const std::vector<long> key = {n, lc.variant, lc.block, lc.stages, (long)lc.smem, lc.grid};
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < nsteps; ++k) {
-            e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
+        for (int k = 0; k < n; ++k) {
+            int e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
             if (e) {
                 cudaStreamEndCapture(c->stream, &g);
                 if (g) cudaGraphDestroy(g);
@@ -270,11 +270,44 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
         cudaError_t ce = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         CK(ce);
-        it = b.graphs.emplace(key, ge).first;
+        it = c->graphs.emplace(key, ge).first;
     }
-    CK(cudaGraphLaunch(it->second, c->stream));
-    *launches += nsteps;
-    *graph_used = true;
+    *out = it->second;
+    return S2D_OK;
+}
+
+// One pass over `nsteps` FD steps starting at kt_begin, for the launch
+// arguments `args` (a whole batch, or one shot of a plain run), as replays of
+// a graph of `graph_chunk` steps.
+int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin, int nsteps, bool use_graph,
+             int *launches, bool *graph_used) {
+    if (nsteps <= 0) return S2D_OK;
+    args.stages = lc.stages;
+    args.err = c->dev_err.as<int>();
+    args.spin_limit = c->opt_spin_limit;
+    args.fault_iter = c->opt_fault_iter;
+    args.task_order = c->opt_order;
+    StepArgs *args_d = c->args_d.as<StepArgs>();
+    const int chunk = use_graph ? std::max(1, c->opt_graph_chunk) : nsteps;
+    for (int done = 0; done < nsteps; done += chunk) {
+        const int n = std::min(chunk, nsteps - done);
+        args.kt_base = kt_begin + done;
+        int e = launch_set_args(args, args_d, c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+        *launches += 1 + n;
+        if (!use_graph) {
+            for (int k = 0; k < n; ++k) {
+                e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
+                if (e) return fail(c, S2D_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)e));
+            }
+            continue;
+        }
+        cudaGraphExec_t ge;
+        e = step_graph(c, lc, n, &ge);
+        if (e) return e;
+        CK(cudaGraphLaunch(ge, c->stream));
+        *graph_used = true;
+    }
     return S2D_OK;
 }
 
@@ -420,13 +453,13 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
     }
     CK(b.shots_d.alloc(sizeof(ShotDev) * nshots));
     CK(cudaMemcpy(b.shots_d.p, b.shot_dev.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
-    CK(b.args_d.alloc(sizeof(StepArgs)));
 
     // segment lengths are chosen for the resident warp count of the current
     // launch configuration (grid = resident blocks, grid-stride over tasks)
     LaunchCfg lc;
     {
-        int e = launch_config(c, 1, &lc);
+        // a task count no launch reaches: the grid is then every resident block
+        int e = launch_config(c, 1L << 40, &lc);
         if (e) return e;
     }
     const long resident_warps = (long)lc.grid * (lc.block / 32);
@@ -540,6 +573,9 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "graph_chunk") {
+        if (value < 1 || value > 100000) return fail(c, S2D_ERR_ARG, "graph_chunk must be in [1, 100000]");
+        c->opt_graph_chunk = (int)value;
     } else if (k == "grad_segment") {
         if (value < 0) return fail(c, S2D_ERR_ARG, "grad_segment must be >= 0");
         c->opt_grad_segment = (int)value;
@@ -582,6 +618,7 @@ int s2d_create(void **ctx, int device) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = c->dev_err.alloc(sizeof(int));
+    if (e == cudaSuccess) e = c->args_d.alloc(sizeof(StepArgs));
     if (e == cudaSuccess) e = cudaMemset(c->dev_err.p, 0, sizeof(int));
     if (e != cudaSuccess) {
         delete c;
@@ -777,10 +814,6 @@ namespace {
 
 struct GradRun {
     std::vector<std::unique_ptr<DevBuf>> bufs;
-    std::map<int, cudaGraphExec_t> adj_graphs;  // by step count
-    ~GradRun() {
-        for (auto &kv : adj_graphs) cudaGraphExecDestroy(kv.second);
-    }
 };
 
 int grad_alloc(Ctx *c, GradRun &g, size_t bytes, void **out) {
@@ -791,42 +824,49 @@ int grad_alloc(Ctx *c, GradRun &g, size_t bytes, void **out) {
     return S2D_OK;
 }
 
-// Adjoint launches for steps kt_top, kt_top-1, ..., kt_top-n+1 (one graph per length).
+// Adjoint launches for steps kt_top, kt_top-1, ..., kt_top-n+1, as replays of
+// a graph of `graph_chunk` launches.
 int run_adjoint(Ctx *c, Batch &b, GradRun &g, StepArgs args, int kt_top, int n, int grid, bool use_graph,
                 int *launches) {
     if (n <= 0) return S2D_OK;
-    args.kt_base = kt_top;
-    StepArgs *args_d = b.args_d.as<StepArgs>();
-    int e = launch_set_args(args, args_d, c->stream);
-    if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
-    *launches += 1 + n;
-    if (!use_graph) {
-        for (int k = 0; k < n; ++k) {
-            e = launch_adjoint(args_d, k, grid, 128, c->stream);
-            if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
-        }
-        return S2D_OK;
-    }
-    auto it = g.adj_graphs.find(n);
-    if (it == g.adj_graphs.end()) {
-        cudaGraph_t gr;
-        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < n; ++k) {
-            e = launch_adjoint(args_d, k, grid, 128, c->stream);
-            if (e) {
-                cudaStreamEndCapture(c->stream, &gr);
-                if (gr) cudaGraphDestroy(gr);
-                return fail(c, S2D_ERR_CUDA, "adjoint capture: %s", cudaGetErrorString((cudaError_t)e));
+    StepArgs *args_d = c->args_d.as<StepArgs>();
+    const int chunk = use_graph ? std::max(1, c->opt_graph_chunk) : n;
+    for (int done = 0; done < n; done += chunk) {
+        const int m = std::min(chunk, n - done);
+        args.kt_base = kt_top - done;
+        int e = launch_set_args(args, args_d, c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+        *launches += 1 + m;
+        if (!use_graph) {
+            for (int k = 0; k < m; ++k) {
+                e = launch_adjoint(args_d, k, grid, 128, c->stream);
+                if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
             }
+            continue;
         }
-        CK(cudaStreamEndCapture(c->stream, &gr));
-        cudaGraphExec_t ge;
-        cudaError_t ce = cudaGraphInstantiate(&ge, gr, 0);
-        cudaGraphDestroy(gr);
-        CK(ce);
-        it = g.adj_graphs.emplace(n, ge).first;
+        (void)g;
+        const std::vector<long> key = {m, grid};
+        auto it = c->adj_graphs.find(key);
+        if (it == c->adj_graphs.end()) {
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < m; ++k) {
+                e = launch_adjoint(args_d, k, grid, 128, c->stream);
+                if (e) {
+                    cudaStreamEndCapture(c->stream, &gr);
+                    if (gr) cudaGraphDestroy(gr);
+                    return fail(c, S2D_ERR_CUDA, "adjoint capture: %s", cudaGetErrorString((cudaError_t)e));
+                }
+            }
+            CK(cudaStreamEndCapture(c->stream, &gr));
+            cudaGraphExec_t ge;
+            cudaError_t ce = cudaGraphInstantiate(&ge, gr, 0);
+            cudaGraphDestroy(gr);
+            CK(ce);
+            it = c->adj_graphs.emplace(key, ge).first;
+        }
+        CK(cudaGraphLaunch(it->second, c->stream));
     }
-    CK(cudaGraphLaunch(it->second, c->stream));
     return S2D_OK;
 }
 

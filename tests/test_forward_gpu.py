@@ -236,3 +236,19 @@ def test_unknown_option_rejected(ctx):
         ctx.set_option("stages", 1)
     with pytest.raises(Seis2dError):
         ctx.set_option("block", 256)
+
+
+def test_graph_chunking_is_transparent(ctx):
+    """Replaying a short captured graph many times gives the same traces as
+    step-by-step launches."""
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("gradient_endonleft_nb40")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    shot = [Shot(m, tuple(z["src"]), z["rec"])]
+    plain = ctx.forward(shot, _wave(c), graph=False)[0]
+    try:
+        for chunk in (7, 1000):
+            ctx.set_option("graph_chunk", chunk)
+            np.testing.assert_array_equal(ctx.forward(shot, _wave(c))[0], plain)
+    finally:
+        ctx.set_option("graph_chunk", 64)
