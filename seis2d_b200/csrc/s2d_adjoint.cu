@@ -78,13 +78,23 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const int pin = (kt + 1) & 1, pout = kt & 1;
     const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
-    const float *mpxi = S.st[pin][0] + off, *mpzi = S.st[pin][1] + off;
-    const float *mvxi = S.st[pin][2] + off, *mvzi = S.st[pin][3] + off;
-    float *mpxo = S.st[pout][0] + off, *mpzo = S.st[pout][1] + off;
-    float *mvxo = S.st[pout][2] + off, *mvzo = S.st[pout][3] + off;
-    const float *kap = S.kappa + off, *bxp = S.bx + off, *bzp = S.bz + off;
-    const float *pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
-    float *gk = S.grad[0] + off, *gbx = S.grad[1] + off, *gbz = S.grad[2] + off;
+    // Every buffer below is distinct: restrict lets the compiler issue the
+    // accumulator and product loads ahead of the state stores.
+    const float *__restrict__ mpxi = S.st[pin][0] + off;
+    const float *__restrict__ mpzi = S.st[pin][1] + off;
+    const float *__restrict__ mvxi = S.st[pin][2] + off;
+    const float *__restrict__ mvzi = S.st[pin][3] + off;
+    float *__restrict__ mpxo = S.st[pout][0] + off;
+    float *__restrict__ mpzo = S.st[pout][1] + off;
+    float *__restrict__ mvxo = S.st[pout][2] + off;
+    float *__restrict__ mvzo = S.st[pout][3] + off;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = S.bx + off;
+    const float *__restrict__ bzp = S.bz + off;
+    const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
+    float *__restrict__ gk = S.grad[0] + off;
+    float *__restrict__ gbx = S.grad[1] + off;
+    float *__restrict__ gbz = S.grad[2] + off;
     float4 zc[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) zc[i] = __ldg(S.zcoef + (z0 + S2D_GZ + i));
@@ -113,8 +123,21 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         // ---- pressure adjoint at column Q = L - 1 ----
         const int Q = L - 1;
         const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
+        const bool in_seg = Q >= xa && Q < xb;
+        const bool upd = in_seg && owner;  // this lane writes column Q
         const float4 mpx = ld4(mpxi + colQ), mpz = ld4(mpzi + colQ), mvz = ld4(mvzi + colQ);
         const float4 bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
+        // products of the forward step and the accumulators, loaded up front
+        float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tbx = zero, tbz = zero;
+        if (upd) {
+            pa = ld4(pr + colQ);
+            pc = ld4(pr + F + colQ);
+            pg = ld4(pr + 2 * F + colQ);
+            ph = ld4(pr + 3 * F + colQ);
+            tk = ldrw(gk + colQ);
+            tbx = ldrw(gbx + colQ);
+            tbz = ldrw(gbz + colQ);
+        }
         const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
         const float4 h = make_float4((zc[0].w * bz.x) * mvz.x, (zc[1].w * bz.y) * mvz.y,
                                      (zc[2].w * bz.z) * mvz.z, (zc[3].w * bz.w) * mvz.w);
@@ -156,30 +179,24 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         }
         const float4 mPX = make_float4(mpx.x + q.x, mpx.y + q.y, mpx.z + q.z, mpx.w + q.w);
         const float4 mPZ = make_float4(mpz.x + q.x, mpz.y + q.y, mpz.z + q.z, mpz.w + q.w);
-        const bool in_seg = Q >= xa && Q < xb;
-        if (in_seg && owner) {
+        if (upd) {
             st4(mpxo + colQ, make_float4(xq.x * mPX.x, xq.x * mPX.y, xq.x * mPX.z, xq.x * mPX.w));
             st4(mpzo + colQ, make_float4(zc[0].x * mPZ.x, zc[1].x * mPZ.y, zc[2].x * mPZ.z, zc[3].x * mPZ.w));
-            const float4 pa = ld4(pr + colQ), pc = ld4(pr + F + colQ);
-            const float4 pg = ld4(pr + 2 * F + colQ), ph = ld4(pr + 3 * F + colQ);
-            float4 t = ldrw(gk + colQ);
-            t.x += (xq.y * pa.x) * mPX.x + (zc[0].y * pc.x) * mPZ.x;
-            t.y += (xq.y * pa.y) * mPX.y + (zc[1].y * pc.y) * mPZ.y;
-            t.z += (xq.y * pa.z) * mPX.z + (zc[2].y * pc.z) * mPZ.z;
-            t.w += (xq.y * pa.w) * mPX.w + (zc[3].y * pc.w) * mPZ.w;
-            st4(gk + colQ, t);
-            t = ldrw(gbx + colQ);
-            t.x += (xq.w * pg.x) * mv2.x;
-            t.y += (xq.w * pg.y) * mv2.y;
-            t.z += (xq.w * pg.z) * mv2.z;
-            t.w += (xq.w * pg.w) * mv2.w;
-            st4(gbx + colQ, t);
-            t = ldrw(gbz + colQ);
-            t.x += (zc[0].w * ph.x) * mvz.x;
-            t.y += (zc[1].w * ph.y) * mvz.y;
-            t.z += (zc[2].w * ph.z) * mvz.z;
-            t.w += (zc[3].w * ph.w) * mvz.w;
-            st4(gbz + colQ, t);
+            tk.x += (xq.y * pa.x) * mPX.x + (zc[0].y * pc.x) * mPZ.x;
+            tk.y += (xq.y * pa.y) * mPX.y + (zc[1].y * pc.y) * mPZ.y;
+            tk.z += (xq.y * pa.z) * mPX.z + (zc[2].y * pc.z) * mPZ.z;
+            tk.w += (xq.y * pa.w) * mPX.w + (zc[3].y * pc.w) * mPZ.w;
+            st4(gk + colQ, tk);
+            tbx.x += (xq.w * pg.x) * mv2.x;
+            tbx.y += (xq.w * pg.y) * mv2.y;
+            tbx.z += (xq.w * pg.z) * mv2.z;
+            tbx.w += (xq.w * pg.w) * mv2.w;
+            st4(gbx + colQ, tbx);
+            tbz.x += (zc[0].w * ph.x) * mvz.x;
+            tbz.y += (zc[1].w * ph.y) * mvz.y;
+            tbz.z += (zc[2].w * ph.z) * mvz.z;
+            tbz.w += (zc[3].w * ph.w) * mvz.w;
+            st4(gbz + colQ, tbz);
             if (Q == S.src_x && sdz >= 0 && sdz < 4) S.srcadj[kt] = comp(mPX, sdz);
         }
         ma0 = ma1; ma1 = ma2; ma2 = ma3;

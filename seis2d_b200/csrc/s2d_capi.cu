@@ -108,6 +108,11 @@ struct Pool {
     void give(std::unique_ptr<DevBuf> b) {
         if (b && b->p) free.emplace(b->bytes, std::move(b));
     }
+    size_t held() const {
+        size_t n = 0;
+        for (auto &kv : free) n += kv.first;
+        return n;
+    }
 };
 
 // Launch configuration of the step kernel.
@@ -943,22 +948,31 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         if (e) return e;
         adj_src = static_cast<float *>(p);
     }
-    // segment length: the largest whose products and checkpoints fit
+    // checkpoint interval: the longest whose products and checkpoints fit in
+    // free memory (pooled buffers count as free: the pool releases itself when
+    // an allocation fails)
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    const double budget = 0.85 * (double)free_b - 4.0 * fb - 64e6;
+    const double budget = 0.85 * ((double)free_b + (double)c->pool.held()) - 4.0 * fb - 64e6;
     const double per_step_all = (double)nshots * 4.0 * fb;
-    int C = rs.fd_nt;
-    if (c->opt_grad_segment > 0) C = std::min(C, c->opt_grad_segment);
-    while (C > 1) {
-        const int nseg = (rs.fd_nt + C - 1) / C;
-        if (per_step_all * (C + nseg - 1) <= budget) break;
-        C = std::max(1, C * 3 / 4);
+    auto need = [&](int C) { return per_step_all * (C + (rs.fd_nt + C - 1) / C - 1); };
+    int C = -1;
+    const int cmax = c->opt_grad_segment > 0 ? std::min(rs.fd_nt, c->opt_grad_segment) : rs.fd_nt;
+    for (int t = cmax; t >= 1; --t)
+        if (need(t) <= budget) {
+            C = t;
+            break;
+        }
+    if (C < 1) {
+        int best = 1;
+        for (int t = 1; t <= rs.fd_nt; ++t)
+            if (need(t) < need(best)) best = t;
+        return fail(c, S2D_ERR_NOMEM,
+                    "gradient of %d shots needs at least %.1f GB for checkpoints and step products, %.1f GB "
+                    "available; use fewer shots per call",
+                    nshots, need(best) / 1e9, budget / 1e9);
     }
     const int nseg = (rs.fd_nt + C - 1) / C;
-    if (per_step_all * (C + nseg - 1) > budget)
-        return fail(c, S2D_ERR_NOMEM, "gradient needs %.1f GB of products/checkpoints, %.1f GB free",
-                    per_step_all * (C + nseg - 1) / 1e9, (double)free_b / 1e9);
     std::vector<float *> prod(nshots), ckpt(nshots);
     for (int s = 0; s < nshots; ++s) {
         void *p;
