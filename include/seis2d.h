@@ -42,7 +42,7 @@ extern "C" {
 #define S2D_API
 #endif
 
-#define S2D_ABI_VERSION 1
+#define S2D_ABI_VERSION 2
 
 /* status codes */
 #define S2D_OK 0
@@ -109,6 +109,9 @@ typedef struct {
     int kernel_launches;     /* launches of the library's own kernels         */
     int graph_used;          /* 1 if the loop ran as a CUDA graph             */
     int grad_segment;        /* s2d_gradient: checkpoint interval used (steps) */
+    int variant, block, stages;  /* launch configuration of the time loop     */
+    int seg_len;             /* columns per warp task (first model group)     */
+    int autotuned;           /* 1 if this call ran the autotuner's trials     */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */
@@ -128,15 +131,27 @@ S2D_API const char *s2d_last_error(const void *ctx);
 
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
- *   "variant"     0 bulk-copy pipeline, 1 plain loads (default), 2 bulk-copy
- *                 pipeline compiled for 128 registers
+ *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
+ *                 shape (models, grids, shot counts) with at least 56 steps
+ *                 spends 28 of them, 4 under each candidate configuration
+ *                 (the results do not change: every candidate computes the same
+ *                 bits), times them with events and keeps the fastest for that
+ *                 shape in the context; untuned runs use variant 2, block 128,
+ *                 stages 3.  0: use "variant", "block" and "stages".
+ *                 Setting any of those three turns autotuning off.
+ *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline
+ *                 compiled for 128 registers (default), 4 plain loads compiled
+ *                 for 128 registers
  *   "block"       threads per block: 32, 64, 96 or 128 (default 128)
  *   "task_order"  0: consecutive warps take the shots of one tile;
  *                 1: consecutive warps take adjacent strips of one shot (default)
- *   "stages"      bulk-copy ring depth per warp, 2..16 (default 5)
+ *   "stages"      bulk-copy ring depth per warp, 2..16 (default 3)
  *   "seg_len"     columns per x-segment of a warp task, 0 = automatic
  *   "spin_limit"  polls of a pipeline barrier before the wait gives up and the
  *                 call returns S2D_ERR_TIMEOUT (default 2^20)
+ *   "fast_rows"   1 (default): strips clear of the z-sponge and the edge rows
+ *                 use literal row coefficients; 0: every strip reads them
+ *                 (same results, a check of the fast path)
  *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
  *                 run needs (default 64)
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the

@@ -23,6 +23,8 @@ S2D_ERR_STABILITY = -8
 S2D_ERR_TIMEOUT = -9
 S2D_ERR_NODEV = -10
 
+ABI_VERSION = 2  # S2D_ABI_VERSION of include/seis2d.h
+
 S2D_SEIS_DEVICE = 0x1
 S2D_PLAIN = 0x2
 S2D_NO_GRAPH = 0x4
@@ -63,7 +65,9 @@ class Geometry(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("loop_ms", C.c_double), ("cell_updates", C.c_double), ("gcells_per_s", C.c_double),
-                ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int)]
+                ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int),
+                ("variant", C.c_int), ("block", C.c_int), ("stages", C.c_int), ("seg_len", C.c_int),
+                ("autotuned", C.c_int)]
 
 
 # Every symbol include/seis2d.h declares, with its ctypes signature.
@@ -115,5 +119,8 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = res
+        if L.s2d_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI {L.s2d_abi_version()}, these bindings want {ABI_VERSION}: "
+                               "rebuild it with `python -m seis2d_b200.build`")
         _lib = L
     return _lib

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -74,6 +75,8 @@ struct Batch {
     std::vector<ShotHost> shots;
     std::vector<ShotDev> shot_dev;   // host mirror
     std::vector<GroupDev> groups;    // batched mode
+    std::vector<int> group_nnx;      // padded columns of each group's model
+    std::vector<long> layout;        // launch configuration the groups are laid out for
     std::vector<std::unique_ptr<DevBuf>> state;   // 8 per shot
     std::vector<std::unique_ptr<DevBuf>> aux;     // amp tables, receiver tables
     DevBuf shots_d, groups_d;
@@ -117,9 +120,9 @@ struct Pool {
 
 // Launch configuration of the step kernel.
 struct LaunchCfg {
-    int variant = kVariantBulk;
+    int variant = kVariantBulk128;
     int block = 128;      // threads per block (whole warps)
-    int stages = 5;       // bulk-copy ring depth per warp
+    int stages = 3;       // bulk-copy ring depth per warp
     size_t smem = 0;
     int grid = 0;
 };
@@ -128,15 +131,18 @@ struct Ctx {
     int device = 0;
     int sm_count = 0;
     // tuning options (s2d_set_option)
-    int opt_variant = kVariantLdg;   // fastest on the c2 batch (see profiles/)
+    // explicit launch configuration, used when autotuning is off
+    int opt_variant = kVariantBulk128;
     int opt_block = 128;
-    int opt_stages = 5;
+    int opt_stages = 3;
+    int opt_autotune = 1;     // time candidate configurations on a new batch shape
     int opt_seg_len = 0;      // 0 = automatic
     int opt_spin_limit = 1 << 20;
     int opt_fault_iter = -1;  // test knob, see s2d_set_option
     int opt_order = 1;        // task order (StepArgs::task_order)
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
     int opt_graph_chunk = 64; // FD steps per captured graph
+    int opt_fast_rows = 1;    // 0: every strip takes the general row path
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     // Launch-argument block read by every step launch, and the graphs of step
@@ -145,6 +151,8 @@ struct Ctx {
     DevBuf args_d;
     std::map<std::vector<long>, cudaGraphExec_t> graphs;
     std::map<std::vector<long>, cudaGraphExec_t> adj_graphs;  // by (step count, grid)
+    // autotuner results: batch shape -> (variant, block, stages)
+    std::map<std::vector<long>, std::array<int, 3>> tuned;
     ~Ctx() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
         for (auto &kv : adj_graphs) cudaGraphExecDestroy(kv.second);
@@ -226,16 +234,19 @@ int build_coef(Ctx *c, Model &m, float fd_dt) {
     return S2D_OK;
 }
 
-// Launch configuration from the context's options: block size, ring depth,
-// shared memory and a grid of exactly the resident blocks (the kernels loop
-// over tasks), capped by the work available.
-int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant = -1) {
+// Launch configuration for (variant, block, stages): shared memory and a grid
+// of exactly the resident blocks (the kernels loop over tasks), capped by the
+// work available.
+int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block, int stages) {
     LaunchCfg lc;
-    lc.variant = variant >= 0 ? variant : c->opt_variant;
-    lc.block = std::max(32, std::min(128, c->opt_block / 32 * 32));
-    lc.stages = std::max(2, std::min(16, c->opt_stages));
-    const bool ldg = lc.variant == kVariantLdg || lc.variant == kVariantLdgProducts;
-    if (ldg) lc.block = 128;
+    lc.variant = variant;
+    lc.block = std::max(32, std::min(128, block / 32 * 32));
+    lc.stages = std::max(2, std::min(16, stages));
+    const bool ldg = lc.variant == kVariantLdg || lc.variant == kVariantLdgProducts || lc.variant == kVariantLdg128;
+    if (ldg) {
+        lc.block = 128;
+        lc.stages = 0;
+    }
     lc.smem = ldg ? 0 : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
     if (e) return fail(c, S2D_ERR_ARG, "step kernel does not accept %zu B of shared memory: %s", lc.smem,
@@ -249,6 +260,74 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant = -1) {
     const long needed = (max_tasks * 32 + lc.block - 1) / lc.block;
     lc.grid = (int)std::max<long>(1, std::min<long>(resident, std::max<long>(needed, 1)));
     *out = lc;
+    return S2D_OK;
+}
+
+// Key of a batch's shape for the autotuner: run mode and, per model group,
+// padded grid and shot count.
+std::vector<long> tune_key(const Ctx *c, const Batch &b) {
+    std::vector<long> k = {b.plain ? 1L : 0L, (long)c->sm_count};
+    for (size_t g = 0; g < b.groups.size(); ++g) {
+        k.push_back(b.group_nnx[g]);
+        k.push_back(b.groups[g].nstrips);
+        k.push_back(b.groups[g].nshots);
+    }
+    return k;
+}
+
+// The configuration a run of batch `b` uses when it does not tune: the
+// options when autotuning is off, else the tuned result for the batch's
+// shape, else the built-in default.
+int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
+    if (tuned) *tuned = false;
+    if (!c->opt_autotune) return launch_config(c, b.max_tasks, out, c->opt_variant, c->opt_block, c->opt_stages);
+    auto it = c->tuned.find(tune_key(c, b));
+    if (it != c->tuned.end()) {
+        if (tuned) *tuned = true;
+        return launch_config(c, b.max_tasks, out, it->second[0], it->second[1], it->second[2]);
+    }
+    const LaunchCfg d;
+    return launch_config(c, b.max_tasks, out, d.variant, d.block, d.stages);
+}
+
+// Segment lengths, segment counts and task ranges of the batch's groups for
+// the resident warps of launch configuration `lc`; uploaded when they change.
+int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
+    const std::vector<long> key = {lc.variant, lc.block, lc.stages, c->opt_seg_len};
+    if (b.layout == key) return S2D_OK;
+    // resident warps of the configuration (its grid when the work is smaller)
+    LaunchCfg full;
+    int e = launch_config(c, 1L << 40, &full, lc.variant, lc.block, lc.stages);
+    if (e) return e;
+    const long resident_warps = (long)full.grid * (full.block / 32);
+    long per_seg_total = 0;
+    for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
+    long max_tasks = 0;
+    int task = 0;
+    for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+        GroupDev &g = b.groups[gi];
+        const int nnx = b.group_nnx[gi];
+        // plain mode: every shot is a group of its own and runs alone
+        const long tasks_per_seg = b.plain ? (long)g.nstrips : per_seg_total;
+        g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, nnx)
+                                       : choose_seg_len(nnx, tasks_per_seg, resident_warps);
+        g.nsegs = (nnx + g.seg_len - 1) / g.seg_len;
+        if (b.plain) {
+            g.task_begin = 0;
+            max_tasks = std::max<long>(max_tasks, (long)g.nstrips * g.nsegs);
+        } else {
+            g.task_begin = task;
+            task += g.nshots * g.nstrips * g.nsegs;
+            max_tasks = task;
+        }
+    }
+    if (!b.groups_d.p) CK(b.groups_d.alloc(sizeof(GroupDev) * b.groups.size()));
+    CK(cudaMemcpyAsync(b.groups_d.p, b.groups.data(), sizeof(GroupDev) * b.groups.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+    // the copy reads host memory that a later layout rewrites
+    CK(cudaStreamSynchronize(c->stream));
+    b.max_tasks = max_tasks;
+    b.layout = key;
     return S2D_OK;
 }
 
@@ -279,6 +358,24 @@ int step_graph(Ctx *c, const LaunchCfg &lc, int n, cudaGraphExec_t *out) {
     }
     *out = it->second;
     return S2D_OK;
+}
+
+// Rows whose coefficients are the interior constants (see ShotDev::zfast_lo):
+// damp1a = damp1b = 1, kz*damp1a1 = kz*damp1b1 = (float)kz, rows [2, nnz-3].
+void fast_rows(const Model &m, float fd_dt, int *lo, int *hi, float *kz) {
+    const double dtdz = (double)(fd_dt * (1.0f / m.dz));  // as build_coef forms it
+    const float kzi = (float)(dtdz * 1.0f);
+    auto ok = [&](int r) {
+        return r >= 2 && r <= m.nnz - 3 && m.damp1a[r] == 1.0f && m.damp1b[r] == 1.0f &&
+               (float)(dtdz * m.damp1a1[r]) == kzi && (float)(dtdz * m.damp1b1[r]) == kzi;
+    };
+    int a = 0;
+    while (a < m.nnz && !ok(a)) ++a;
+    int b = a;
+    while (b < m.nnz && ok(b)) ++b;
+    *lo = a;
+    *hi = b;  // empty when a == b
+    *kz = kzi;
 }
 
 // One pass over `nsteps` FD steps starting at kt_begin, for the launch
@@ -404,6 +501,8 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         d.nfield = m.field_elems;
         d.nrec = h.nrec;
         d.nseis = (size_t)h.nrec * rs.real_nt;
+        fast_rows(m, wave.fd_dt, &d.zfast_lo, &d.zfast_hi, &d.kz_in);
+        if (!c->opt_fast_rows) d.zfast_lo = d.zfast_hi = 0;
         // source amplitude per step: fd_dt * w[kt] * kappa[src] / (dx*dz)
         // (cpumodelling.cpp:136-140), kappa = vp^2 rho in double at the source
         const int mx = std::min(std::max(h.src_x - m.nb, 0), m.nx - 1);
@@ -459,25 +558,14 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
     CK(b.shots_d.alloc(sizeof(ShotDev) * nshots));
     CK(cudaMemcpy(b.shots_d.p, b.shot_dev.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
 
-    // segment lengths are chosen for the resident warp count of the current
-    // launch configuration (grid = resident blocks, grid-stride over tasks)
-    LaunchCfg lc;
-    {
-        // a task count no launch reaches: the grid is then every resident block
-        int e = launch_config(c, 1L << 40, &lc);
-        if (e) return e;
-    }
-    const long resident_warps = (long)lc.grid * (lc.block / 32);
     // groups: shots sharing a model, tasks interleaved over the group's shots.
     // In plain mode every shot is a group of its own and runs alone.
-    std::vector<int> order;
-    std::map<int, std::vector<int>> by_model;
     std::vector<int> model_order;
+    std::map<int, std::vector<int>> by_model;
     for (int s = 0; s < nshots; ++s) {
         if (!by_model.count(shots[s].model_id)) model_order.push_back(shots[s].model_id);
         by_model[shots[s].model_id].push_back(s);
     }
-    long max_tasks = 0;
     if (b.plain) {
         for (int s = 0; s < nshots; ++s) {
             const Model &m = *c->models[shots[s].model_id];
@@ -485,50 +573,34 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             g.nshots = 1;
             g.shot0 = s;
             g.nstrips = num_strips(m.nnz);
-            g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, m.nnx)
-                                           : choose_seg_len(m.nnx, g.nstrips, resident_warps);
-            g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
-            g.task_begin = 0;
             b.groups.push_back(g);
-            max_tasks = std::max<long>(max_tasks, (long)g.nstrips * g.nsegs);
+            b.group_nnx.push_back(m.nnx);
         }
     } else {
         // shots of one model must be contiguous in the shot table for shot0
         // indexing; keep the caller's order inside each model and reorder the
         // device table only (seis offsets stay the caller's).
         std::vector<ShotDev> reordered;
-        int task = 0;
         for (int mid : model_order) {
             const Model &m = *c->models[mid];
             const std::vector<int> &ss = by_model[mid];
             GroupDev g{};
-            g.task_begin = task;
             g.nshots = (int)ss.size();
             g.shot0 = (int)reordered.size();
             g.nstrips = num_strips(m.nnz);
             b.groups.push_back(g);
+            b.group_nnx.push_back(m.nnx);
             for (int s : ss) reordered.push_back(b.shot_dev[s]);
         }
-        long per_seg_total = 0;
-        for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
-        for (size_t gi = 0; gi < b.groups.size(); ++gi) {
-            GroupDev &g = b.groups[gi];
-            const Model &m = *c->models[model_order[gi]];
-            g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, m.nnx)
-                                           : choose_seg_len(m.nnx, per_seg_total, resident_warps);
-            g.nsegs = (m.nnx + g.seg_len - 1) / g.seg_len;
-        }
-        task = 0;
-        for (auto &g : b.groups) {
-            g.task_begin = task;
-            task += g.nshots * g.nstrips * g.nsegs;
-        }
-        max_tasks = task;
         CK(cudaMemcpy(b.shots_d.p, reordered.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
     }
-    CK(b.groups_d.alloc(sizeof(GroupDev) * b.groups.size()));
-    CK(cudaMemcpy(b.groups_d.p, b.groups.data(), sizeof(GroupDev) * b.groups.size(), cudaMemcpyHostToDevice));
-    b.max_tasks = max_tasks;
+    // segment lengths for the configuration the run starts with
+    {
+        LaunchCfg lc;
+        int e = base_config(c, b, &lc);
+        if (!e) e = layout_groups(c, b, lc);
+        if (e) return e;
+    }
     CK(cudaStreamSynchronize(c->stream));
     c->batch = std::move(bp);
     return S2D_OK;
@@ -551,6 +623,101 @@ int check_device_error(Ctx *c) {
 
 }  // namespace
 
+// Candidate launch configurations of the autotuner: (variant, block, stages).
+constexpr int kTuneCandidates[][3] = {
+    {kVariantBulk128, 128, 3}, {kVariantBulk128, 128, 2}, {kVariantBulk128, 64, 3}, {kVariantBulk128, 64, 4},
+    {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},
+};
+constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
+constexpr int kTuneWarm = 1, kTuneTimed = 3;
+constexpr int kTuneSteps = kNumTuneCandidates * (kTuneWarm + kTuneTimed);
+
+// Sum of the task counts of a batched launch sequence.
+int batch_tasks(const Batch &b) {
+    int t = 0;
+    for (auto &g : b.groups) t += g.nshots * g.nstrips * g.nsegs;
+    return t;
+}
+
+// Autotuner: advance the batch by kTuneSteps real FD steps from kt_begin,
+// kTuneWarm + kTuneTimed under each candidate configuration (every candidate
+// computes the same bits: they share the update arithmetic and differ only in
+// how columns reach registers and how tasks map to warps), with each timed
+// step between two events.  The candidate with the lowest median step time
+// is cached for the batch's shape and returned, its segment layout in place.
+int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best) {
+    std::vector<cudaEvent_t> ev(2 * kTuneTimed * kNumTuneCandidates, nullptr);
+    for (auto &e : ev) {
+        cudaError_t ce = cudaEventCreate(&e);
+        if (ce != cudaSuccess) {
+            for (auto &x : ev)
+                if (x) cudaEventDestroy(x);
+            return fail(c, S2D_ERR_CUDA, "autotune events: %s", cudaGetErrorString(ce));
+        }
+    }
+    auto release = [&]() {
+        for (auto &x : ev) cudaEventDestroy(x);
+    };
+    std::vector<LaunchCfg> cfg(kNumTuneCandidates);
+    std::vector<bool> ok(kNumTuneCandidates, false);
+    int kt = kt_begin;
+    bool graph_used = false;
+    for (int i = 0; i < kNumTuneCandidates; ++i) {
+        const int *k = kTuneCandidates[i];
+        LaunchCfg lc;
+        if (launch_config(c, 1L << 40, &lc, k[0], k[1], k[2]) != S2D_OK) {
+            if (i == 0) {
+                release();
+                return S2D_ERR_ARG;
+            }
+            // a configuration this device cannot run: its steps run under the
+            // first candidate instead and are not timed
+            lc = cfg[0];
+        } else {
+            ok[i] = true;
+        }
+        int e = layout_groups(c, b, lc);
+        if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
+        if (e) {
+            release();
+            return e;
+        }
+        cfg[i] = lc;
+        a.total_tasks = batch_tasks(b);
+        for (int s = 0; s < kTuneWarm + kTuneTimed; ++s, ++kt) {
+            const int t = s - kTuneWarm;
+            if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t)], c->stream));
+            e = run_loop(c, b, lc, a, kt, 1, false, launches, &graph_used);
+            if (e) {
+                release();
+                return e;
+            }
+            if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t) + 1], c->stream));
+        }
+    }
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    int pick = 0;
+    float pick_ms = 0;
+    for (int i = 0; i < kNumTuneCandidates && ce == cudaSuccess; ++i) {
+        float t[kTuneTimed];
+        for (int s = 0; s < kTuneTimed && ce == cudaSuccess; ++s)
+            ce = cudaEventElapsedTime(&t[s], ev[2 * (i * kTuneTimed + s)], ev[2 * (i * kTuneTimed + s) + 1]);
+        std::sort(t, t + kTuneTimed);
+        const float med = t[kTuneTimed / 2];
+        if (ok[i] && (i == 0 || med < pick_ms)) {
+            pick = i;
+            pick_ms = med;
+        }
+    }
+    release();
+    CK(ce);
+    const int *k = kTuneCandidates[pick];
+    c->tuned[tune_key(c, b)] = {k[0], k[1], k[2]};
+    int e = layout_groups(c, b, cfg[pick]);
+    if (!e) e = launch_config(c, b.max_tasks, best, k[0], k[1], k[2]);
+    return e;
+}
+
 // ---------------------------------------------------------------------------
 
 extern "C" {
@@ -561,23 +728,32 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     Ctx *c = static_cast<Ctx *>(ctx);
     if (!c || !key) return S2D_ERR_ARG;
     const std::string k(key);
+    // an explicit launch configuration turns the autotuner off
     if (k == "variant") {
-        if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128)
+        if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
+        c->opt_autotune = 0;
     } else if (k == "block") {
         if (value < 32 || value > 128 || value % 32)
             return fail(c, S2D_ERR_ARG, "block must be 1 to 4 whole warps (the step kernels are built for <= 128 threads)");
         c->opt_block = (int)value;
+        c->opt_autotune = 0;
     } else if (k == "stages") {
         if (value < 2 || value > 16) return fail(c, S2D_ERR_ARG, "stages must be in [2, 16]");
         c->opt_stages = (int)value;
+        c->opt_autotune = 0;
     } else if (k == "seg_len") {
         if (value < 0) return fail(c, S2D_ERR_ARG, "seg_len must be >= 0");
         c->opt_seg_len = (int)value;
+    } else if (k == "autotune") {
+        if (value != 0 && value != 1) return fail(c, S2D_ERR_ARG, "autotune must be 0 or 1");
+        c->opt_autotune = (int)value;
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "fast_rows") {
+        c->opt_fast_rows = value ? 1 : 0;
     } else if (k == "graph_chunk") {
         if (value < 1 || value > 100000) return fail(c, S2D_ERR_ARG, "graph_chunk must be in [1, 100000]");
         c->opt_graph_chunk = (int)value;
@@ -743,9 +919,12 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     const bool use_graph = !(flags & S2D_NO_GRAPH);
     int launches = 0;
     bool graph_used = false;
+    bool tuned = false;
     LaunchCfg lc;
     {
-        int e = launch_config(c, b.max_tasks, &lc);
+        int e = base_config(c, b, &lc, &tuned);
+        if (!e) e = layout_groups(c, b, lc);
+        if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
         if (e) return e;
     }
     CK(cudaEventRecord(c->ev0, c->stream));
@@ -753,6 +932,18 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     a.shots = b.shots_d.as<ShotDev>();
     a.dt_factor = rs.dt_factor;
     a.fd_nt = rs.fd_nt;
+    int kt_run = kt_begin;  // first step left after tuning
+    int tuned_now = 0;
+    // Batched runs of a shape with no tuned configuration yet tune on their
+    // first steps when the call has room for the trials and a run after them.
+    if (c->opt_autotune && !tuned && !b.plain && nsteps >= 2 * kTuneSteps) {
+        a.groups = b.groups_d.as<GroupDev>();
+        a.ngroups = (int)b.groups.size();
+        int e = autotune(c, b, a, kt_begin, &launches, &lc);
+        if (e) return e;
+        kt_run += kTuneSteps;
+        tuned_now = 1;
+    }
     if (b.plain) {
         for (int s = 0; s < nshots; ++s) {
             a.groups = b.groups_d.as<GroupDev>() + s;
@@ -764,9 +955,8 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     } else {
         a.groups = b.groups_d.as<GroupDev>();
         a.ngroups = (int)b.groups.size();
-        a.total_tasks = 0;
-        for (auto &g : b.groups) a.total_tasks += g.nshots * g.nstrips * g.nsegs;
-        int e = run_loop(c, b, lc, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
+        a.total_tasks = batch_tasks(b);
+        int e = run_loop(c, b, lc, a, kt_run, kt_end - kt_run, use_graph, &launches, &graph_used);
         if (e) return e;
     }
     CK(cudaEventRecord(c->ev1, c->stream));
@@ -806,6 +996,11 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;
         stats->grad_segment = 0;
+        stats->variant = lc.variant;
+        stats->block = lc.block;
+        stats->stages = lc.stages;
+        stats->seg_len = b.groups.empty() ? 0 : b.groups[0].seg_len;
+        stats->autotuned = tuned_now;
     }
     return S2D_OK;
 }
@@ -999,16 +1194,17 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
 
     LaunchCfg lc_fwd, lc_prod;
     {
-        int e = launch_config(c, b.max_tasks, &lc_fwd);
-        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts);
+        int e = base_config(c, b, &lc_fwd);
+        if (!e) e = layout_groups(c, b, lc_fwd);
+        if (!e) e = launch_config(c, b.max_tasks, &lc_fwd, lc_fwd.variant, lc_fwd.block, lc_fwd.stages);
+        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts, 128, 0);
         if (e) return e;
     }
     StepArgs fa{};
     fa.shots = b.shots_d.as<ShotDev>();
     fa.groups = b.groups_d.as<GroupDev>();
     fa.ngroups = (int)b.groups.size();
-    fa.total_tasks = 0;
-    for (auto &gr : b.groups) fa.total_tasks += gr.nshots * gr.nstrips * gr.nsegs;
+    fa.total_tasks = batch_tasks(b);
     fa.dt_factor = rs.dt_factor;
     fa.fd_nt = rs.fd_nt;
     bool graph_used = false;

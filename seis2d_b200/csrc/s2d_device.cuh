@@ -35,28 +35,53 @@ static __device__ __forceinline__ float comp(const float4 &v, int i) {
     return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
-// Per-lane constants of one task: the lane's four rows and the shot data.
+// Per-lane constants of one task.  FAST tasks lie inside the shot's fast row
+// range (no z-sponge, no edge rows): their row coefficients are literals.
+// Other tasks read a row's coefficients when they use them (L1 hits), so that
+// neither kind holds per-row tables in registers.
+template <bool FAST>
 struct Lane {
-    float4 zc[4];                 // damp1a, kz*damp1a1, damp1b, kz*damp1b1 per row
-    float cm0[4], cm1[4], cp0[4], cp1[4];
-    int z0;                       // first row of the lane
-    bool owner;                   // writes its rows (lanes 1..30)
-    int sdz;                      // source row - z0
-    float amp;                    // source term of this step
+    int z0;          // first row of the lane
+    bool owner;      // writes its rows (lanes 1..30)
+    int sdz;         // source row - z0
+    float amp;       // source term of this step
+    float kz;        // interior kz (FAST)
+    int nnz;
+    const float4 *zc;  // zcoef + z0 + GZ (not FAST)
 };
 
-static __device__ __forceinline__ void lane_setup(Lane &ln, const ShotDev &S, int c, int lane, int kt) {
+template <bool FAST>
+static __device__ __forceinline__ void lane_setup(Lane<FAST> &ln, const ShotDev &S, int c, int lane, int kt) {
     ln.z0 = c + S2D_ZPT * lane;
-    const float4 *zc = S.zcoef + (ln.z0 + S2D_GZ);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        ln.zc[i] = __ldg(zc + i);
-        dm_coef(ln.z0 + i, S.nnz, ln.cm0[i], ln.cm1[i]);
-        dp_coef(ln.z0 + i, S.nnz, ln.cp0[i], ln.cp1[i]);
-    }
     ln.owner = lane >= 1 && lane <= 30;
     ln.sdz = S.src_z - ln.z0;
     ln.amp = __ldg(S.amp + kt);
+    ln.kz = S.kz_in;
+    ln.nnz = S.nnz;
+    ln.zc = S.zcoef + (ln.z0 + S2D_GZ);
+}
+
+// damp1a, kz*damp1a1, damp1b, kz*damp1b1 of the lane's row z0 + i
+template <bool FAST>
+static __device__ __forceinline__ float4 zrow(const Lane<FAST> &ln, int i) {
+    if (FAST) return make_float4(1.0f, ln.kz, 1.0f, ln.kz);
+    return __ldg(ln.zc + i);
+}
+// operator pairs of the lane's row z0 + i (D- and D+)
+template <bool FAST>
+static __device__ __forceinline__ void zdm(const Lane<FAST> &ln, int i, float &c0, float &c1) {
+    if (FAST) { c0 = kA0; c1 = kA1; return; }
+    dm_coef(ln.z0 + i, ln.nnz, c0, c1);
+}
+template <bool FAST>
+static __device__ __forceinline__ void zdp(const Lane<FAST> &ln, int i, float &c0, float &c1) {
+    if (FAST) { c0 = kA0; c1 = kA1; return; }
+    dp_coef(ln.z0 + i, ln.nnz, c0, c1);
+}
+
+// Rows [lo, hi] of a task all in the shot's fast range.
+static __device__ __forceinline__ bool rows_fast(const ShotDev &S, int lo, int hi) {
+    return lo >= S.zfast_lo && hi < S.zfast_hi;
 }
 
 // Map a flat task index to (shot, strip, first column, segment length).

@@ -54,7 +54,10 @@ struct ShotDev {
     size_t nprod;                  // prod
     size_t nseis;                  // seis (this shot's block)
     int nrec;
-    int pad3_;
+    // Rows [zfast_lo, zfast_hi) have the interior row constants: damp1a =
+    // damp1b = 1, kz*damp1a1 = kz*damp1b1 = kz_in, operator pair (a0, a1).
+    int zfast_lo, zfast_hi;
+    float kz_in;
 };
 
 // Shots that share one grid shape; their tasks are interleaved so that the
@@ -100,7 +103,8 @@ struct StepArgs {
 
 // Step kernel variants.
 enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
-                   kVariantLdgProducts = 3 /* plain loads + S2D_STEP_PRODUCTS, gradient runs */ };
+                   kVariantLdgProducts = 3 /* plain loads + S2D_STEP_PRODUCTS, gradient runs */,
+                   kVariantLdg128 = 4 /* plain loads, compiled for 128 registers */ };
 
 // Shared memory of one pipeline stage: 7 slots of one 128-row column each
 // (vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3).

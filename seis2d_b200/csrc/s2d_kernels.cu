@@ -38,10 +38,23 @@ namespace s2d {
 
 namespace {
 
+// The two arithmetic forms of the update, with the rounding of every
+// operation fixed (explicit fma/mul, nothing left to contraction), so that a
+// row computes the same bits whether its coefficients are literals or loads.
+//   dif: c0*d0 + c1*d1, one product rounded, then fused;
+//   upd: a*x + (b*k)*d, the coefficient product and the term rounded, then fused.
+__device__ __forceinline__ float dif(float c0, float d0, float c1, float d1) {
+    return __fmaf_rn(c0, d0, __fmul_rn(c1, d1));
+}
+__device__ __forceinline__ float upd(float a, float x, float b, float k, float d) {
+    return __fmaf_rn(a, x, __fmul_rn(__fmul_rn(b, k), d));
+}
+
 // Pressure at column P from vx at P-2..P+1 (q0..q3), old px, pz, kappa and vz
 // at P (cpu_modelling_kernels.cpp:201-258 and 335-351, cpumodelling.cpp:136-142).
-// Returns new p; new px, pz in pxn, pzn.
-__device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int P, const float4 &q0,
+// Returns new p; new px, pz in pxn, pzn; D-x vx and D-z vz in dxv, dzv.
+template <bool FAST>
+__device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &q0,
                                            const float4 &q1, const float4 &q2, const float4 &q3, const float4 &px,
                                            const float4 &pz, const float4 &kk, const float4 &vz, float4 &pxn,
                                            float4 &pzn, float4 &dxv, float4 &dzv) {
@@ -51,24 +64,33 @@ __device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int
     const float up_z = __shfl_up_sync(kFull, vz.z, 1);
     const float up_w = __shfl_up_sync(kFull, vz.w, 1);
     const float dn_x = __shfl_down_sync(kFull, vz.x, 1);
-    const float dz0 = ln.cm0[0] * (vz.x - up_w) + ln.cm1[0] * (vz.y - up_z);
-    const float dz1 = ln.cm0[1] * (vz.y - vz.x) + ln.cm1[1] * (vz.z - up_w);
-    const float dz2 = ln.cm0[2] * (vz.z - vz.y) + ln.cm1[2] * (vz.w - vz.x);
-    const float dz3 = ln.cm0[3] * (vz.w - vz.z) + ln.cm1[3] * (dn_x - vz.y);
-    const float dx0 = cx0 * (q2.x - q1.x) + cx1 * (q3.x - q0.x);
-    const float dx1 = cx0 * (q2.y - q1.y) + cx1 * (q3.y - q0.y);
-    const float dx2 = cx0 * (q2.z - q1.z) + cx1 * (q3.z - q0.z);
-    const float dx3 = cx0 * (q2.w - q1.w) + cx1 * (q3.w - q0.w);
+    float a0, a1;
+    zdm(ln, 0, a0, a1);
+    const float dz0 = dif(a0, vz.x - up_w, a1, vz.y - up_z);
+    zdm(ln, 1, a0, a1);
+    const float dz1 = dif(a0, vz.y - vz.x, a1, vz.z - up_w);
+    zdm(ln, 2, a0, a1);
+    const float dz2 = dif(a0, vz.z - vz.y, a1, vz.w - vz.x);
+    zdm(ln, 3, a0, a1);
+    const float dz3 = dif(a0, vz.w - vz.z, a1, dn_x - vz.y);
+    const float dx0 = dif(cx0, q2.x - q1.x, cx1, q3.x - q0.x);
+    const float dx1 = dif(cx0, q2.y - q1.y, cx1, q3.y - q0.y);
+    const float dx2 = dif(cx0, q2.z - q1.z, cx1, q3.z - q0.z);
+    const float dx3 = dif(cx0, q2.w - q1.w, cx1, q3.w - q0.w);
     dxv = make_float4(dx0, dx1, dx2, dx3);
     dzv = make_float4(dz0, dz1, dz2, dz3);
-    pxn.x = xc.x * px.x + (xc.y * kk.x) * dx0;
-    pxn.y = xc.x * px.y + (xc.y * kk.y) * dx1;
-    pxn.z = xc.x * px.z + (xc.y * kk.z) * dx2;
-    pxn.w = xc.x * px.w + (xc.y * kk.w) * dx3;
-    pzn.x = ln.zc[0].x * pz.x + (ln.zc[0].y * kk.x) * dz0;
-    pzn.y = ln.zc[1].x * pz.y + (ln.zc[1].y * kk.y) * dz1;
-    pzn.z = ln.zc[2].x * pz.z + (ln.zc[2].y * kk.z) * dz2;
-    pzn.w = ln.zc[3].x * pz.w + (ln.zc[3].y * kk.w) * dz3;
+    pxn.x = upd(xc.x, px.x, xc.y, kk.x, dx0);
+    pxn.y = upd(xc.x, px.y, xc.y, kk.y, dx1);
+    pxn.z = upd(xc.x, px.z, xc.y, kk.z, dx2);
+    pxn.w = upd(xc.x, px.w, xc.y, kk.w, dx3);
+    float4 r = zrow(ln, 0);
+    pzn.x = upd(r.x, pz.x, r.y, kk.x, dz0);
+    r = zrow(ln, 1);
+    pzn.y = upd(r.x, pz.y, r.y, kk.y, dz1);
+    r = zrow(ln, 2);
+    pzn.z = upd(r.x, pz.z, r.y, kk.z, dz2);
+    r = zrow(ln, 3);
+    pzn.w = upd(r.x, pz.w, r.y, kk.w, dz3);
     if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
         if (ln.sdz == 0) pxn.x += ln.amp;
         else if (ln.sdz == 1) pxn.y += ln.amp;
@@ -79,7 +101,8 @@ __device__ __forceinline__ float4 p_update(const Lane &ln, const ShotDev &S, int
 }
 
 // Receiver sampling of new p at column P (cpumodelling.cpp:356-360).
-__device__ __forceinline__ void record(const Lane &ln, const ShotDev &S, int P, const float4 &pn, int slot) {
+template <bool FAST>
+__device__ __forceinline__ void record(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &pn, int slot) {
     const int j1 = __ldg(S.rec_ptr + P + 1);
     for (int j = __ldg(S.rec_ptr + P); j < j1; ++j) {
         const int d = __ldg(S.rec_z + j) - ln.z0;
@@ -88,43 +111,125 @@ __device__ __forceinline__ void record(const Lane &ln, const ShotDev &S, int P, 
 }
 
 // Velocities at column V from new p at V-1..V+2 (p0..p3), old vx, vz at V and
-// bx, bz at V (cpu_modelling_kernels.cpp:260-316 and 353-368).
-__device__ __forceinline__ void v_update(const Lane &ln, const ShotDev &S, int V, const float4 &p0,
+// bx, bz at V (cpu_modelling_kernels.cpp:260-316 and 353-368); D+x p and D+z p
+// in dxp, dzp.
+template <bool FAST>
+__device__ __forceinline__ void v_update(const Lane<FAST> &ln, const ShotDev &S, int V, const float4 &p0,
                                          const float4 &p1, const float4 &p2, const float4 &p3, const float4 &vx,
                                          const float4 &vz, const float4 &bx, const float4 &bz, float4 &vxn,
                                          float4 &vzn, float4 &dxp, float4 &dzp) {
     const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
     float ux0, ux1;
     dp_coef(V, S.nnx, ux0, ux1);
-    const float ex0 = ux0 * (p2.x - p1.x) + ux1 * (p3.x - p0.x);
-    const float ex1 = ux0 * (p2.y - p1.y) + ux1 * (p3.y - p0.y);
-    const float ex2 = ux0 * (p2.z - p1.z) + ux1 * (p3.z - p0.z);
-    const float ex3 = ux0 * (p2.w - p1.w) + ux1 * (p3.w - p0.w);
+    const float ex0 = dif(ux0, p2.x - p1.x, ux1, p3.x - p0.x);
+    const float ex1 = dif(ux0, p2.y - p1.y, ux1, p3.y - p0.y);
+    const float ex2 = dif(ux0, p2.z - p1.z, ux1, p3.z - p0.z);
+    const float ex3 = dif(ux0, p2.w - p1.w, ux1, p3.w - p0.w);
     const float4 q = p1;
     const float up_w = __shfl_up_sync(kFull, q.w, 1);
     const float dn_x = __shfl_down_sync(kFull, q.x, 1);
     const float dn_y = __shfl_down_sync(kFull, q.y, 1);
-    const float ez0 = ln.cp0[0] * (q.y - q.x) + ln.cp1[0] * (q.z - up_w);
-    const float ez1 = ln.cp0[1] * (q.z - q.y) + ln.cp1[1] * (q.w - q.x);
-    const float ez2 = ln.cp0[2] * (q.w - q.z) + ln.cp1[2] * (dn_x - q.y);
-    const float ez3 = ln.cp0[3] * (dn_x - q.w) + ln.cp1[3] * (dn_y - q.z);
+    float b0, b1;
+    zdp(ln, 0, b0, b1);
+    const float ez0 = dif(b0, q.y - q.x, b1, q.z - up_w);
+    zdp(ln, 1, b0, b1);
+    const float ez1 = dif(b0, q.z - q.y, b1, q.w - q.x);
+    zdp(ln, 2, b0, b1);
+    const float ez2 = dif(b0, q.w - q.z, b1, dn_x - q.y);
+    zdp(ln, 3, b0, b1);
+    const float ez3 = dif(b0, dn_x - q.w, b1, dn_y - q.z);
     dxp = make_float4(ex0, ex1, ex2, ex3);
     dzp = make_float4(ez0, ez1, ez2, ez3);
-    vxn.x = xc.z * vx.x + (xc.w * bx.x) * ex0;
-    vxn.y = xc.z * vx.y + (xc.w * bx.y) * ex1;
-    vxn.z = xc.z * vx.z + (xc.w * bx.z) * ex2;
-    vxn.w = xc.z * vx.w + (xc.w * bx.w) * ex3;
-    vzn.x = ln.zc[0].z * vz.x + (ln.zc[0].w * bz.x) * ez0;
-    vzn.y = ln.zc[1].z * vz.y + (ln.zc[1].w * bz.y) * ez1;
-    vzn.z = ln.zc[2].z * vz.z + (ln.zc[2].w * bz.z) * ez2;
-    vzn.w = ln.zc[3].z * vz.w + (ln.zc[3].w * bz.w) * ez3;
+    vxn.x = upd(xc.z, vx.x, xc.w, bx.x, ex0);
+    vxn.y = upd(xc.z, vx.y, xc.w, bx.y, ex1);
+    vxn.z = upd(xc.z, vx.z, xc.w, bx.z, ex2);
+    vxn.w = upd(xc.z, vx.w, xc.w, bx.w, ex3);
+    float4 r = zrow(ln, 0);
+    vzn.x = upd(r.z, vz.x, r.w, bz.x, ez0);
+    r = zrow(ln, 1);
+    vzn.y = upd(r.z, vz.y, r.w, bz.y, ez1);
+    r = zrow(ln, 2);
+    vzn.z = upd(r.z, vz.z, r.w, bz.z, ez2);
+    r = zrow(ln, 3);
+    vzn.w = upd(r.z, vz.w, r.w, bz.w, ez3);
 }
 
 // ---------------------------------------------------------------- LDG variant
 
-// PROD: also write the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).
-template <bool PROD>
-__global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
+// One (shot, strip, segment) task of the plain-load kernel.  PROD: also write
+// the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).
+template <bool PROD, bool FAST>
+__device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                         int kt, int par, bool rec_step, int slot, int lane) {
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t ld = (size_t)S.ld;
+    const int c = strip * S2D_STRIP_OUT - 4;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+    float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
+    const float *__restrict__ pxi = S.st[par][0] + off;
+    const float *__restrict__ pzi = S.st[par][1] + off;
+    const float *__restrict__ vxi = S.st[par][2] + off;
+    const float *__restrict__ vzi = S.st[par][3] + off;
+    float *__restrict__ pxo = S.st[par ^ 1][0] + off;
+    float *__restrict__ pzo = S.st[par ^ 1][1] + off;
+    float *__restrict__ vxo = S.st[par ^ 1][2] + off;
+    float *__restrict__ vzo = S.st[par ^ 1][3] + off;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = S.bx + off;
+    const float *__restrict__ bzp = S.bz + off;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 vq0 = zero, vq1, vq2, vq3;
+    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+    float4 zq0 = zero, zq1 = zero, zq2 = zero;
+    vq1 = ld4(vxi + (ptrdiff_t)(xa - 3) * (ptrdiff_t)ld);
+    vq2 = ld4(vxi + (ptrdiff_t)(xa - 2) * (ptrdiff_t)ld);
+    vq3 = ld4(vxi + (ptrdiff_t)(xa - 1) * (ptrdiff_t)ld);
+    for (int L = xa; L <= xb + 2; ++L) {
+        const int P = L - 1;
+        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+        vq0 = vq1; vq1 = vq2; vq2 = vq3;
+        vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
+        const float4 vz = ld4(vzi + colP);
+        float4 pxn, pzn, dxv, dzv;
+        const float4 pn = p_update(ln, S, P, vq0, vq1, vq2, vq3, ld4(pxi + colP), ld4(pzi + colP),
+                                   ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
+        const bool in_seg = P >= xa && P < xb;
+        if (in_seg && ln.owner) {
+            st4(pxo + colP, pxn);
+            st4(pzo + colP, pzn);
+            if (PROD) {
+                st4(pr + colP, dxv);
+                st4(pr + F + colP, dzv);
+            }
+        }
+        if (rec && in_seg) record(ln, S, P, pn, slot);
+        pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+        zq0 = zq1; zq1 = zq2; zq2 = vz;
+        if (L >= xa + 3) {
+            const int V = L - 3;
+            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+            float4 vxn, vzn, dxp, dzp;
+            v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
+            if (ln.owner) {
+                st4(vxo + colV, vxn);
+                st4(vzo + colV, vzn);
+                if (PROD) {
+                    st4(pr + 2 * F + colV, dxp);
+                    st4(pr + 3 * F + colV, dzp);
+                }
+            }
+        }
+    }
+}
+
+// MINB = 4 caps registers at 128 (4 blocks of 4 warps per SM, some spill);
+// MINB = 3 keeps the product-writing instance at 3 blocks per SM.
+template <bool PROD, int MINB>
+__global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -138,64 +243,11 @@ __global__ void __launch_bounds__(128) step_kernel_ldg(const StepArgs *__restric
         int strip, xa, seg_len;
         const ShotDev &S = task_of(a, t, strip, xa, seg_len);
         if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
-        const int xb = min(S.nnx, xa + seg_len);
-        const size_t ld = (size_t)S.ld;
         const int c = strip * S2D_STRIP_OUT - 4;
-        Lane ln;
-        lane_setup(ln, S, c, lane, kt);
-        const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
-        const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
-        const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
-        float *pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
-        const float *pxi = S.st[par][0] + off, *pzi = S.st[par][1] + off;
-        const float *vxi = S.st[par][2] + off, *vzi = S.st[par][3] + off;
-        float *pxo = S.st[par ^ 1][0] + off, *pzo = S.st[par ^ 1][1] + off;
-        float *vxo = S.st[par ^ 1][2] + off, *vzo = S.st[par ^ 1][3] + off;
-        const float *kap = S.kappa + off, *bxp = S.bx + off, *bzp = S.bz + off;
-        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 vq0 = zero, vq1, vq2, vq3;
-        float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
-        float4 zq0 = zero, zq1 = zero, zq2 = zero;
-        vq1 = ld4(vxi + (ptrdiff_t)(xa - 3) * (ptrdiff_t)ld);
-        vq2 = ld4(vxi + (ptrdiff_t)(xa - 2) * (ptrdiff_t)ld);
-        vq3 = ld4(vxi + (ptrdiff_t)(xa - 1) * (ptrdiff_t)ld);
-        for (int L = xa; L <= xb + 2; ++L) {
-            const int P = L - 1;
-            const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
-            vq0 = vq1; vq1 = vq2; vq2 = vq3;
-            vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
-            const float4 vz = ld4(vzi + colP);
-            float4 pxn, pzn, dxv, dzv;
-            const float4 pn = p_update(ln, S, P, vq0, vq1, vq2, vq3, ld4(pxi + colP), ld4(pzi + colP),
-                                       ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
-            const bool in_seg = P >= xa && P < xb;
-            if (in_seg && ln.owner) {
-                st4(pxo + colP, pxn);
-                st4(pzo + colP, pzn);
-                if (PROD) {
-                    st4(pr + colP, dxv);
-                    st4(pr + F + colP, dzv);
-                }
-            }
-            if (rec && in_seg) record(ln, S, P, pn, slot);
-            pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
-            zq0 = zq1; zq1 = zq2; zq2 = vz;
-            if (L >= xa + 3) {
-                const int V = L - 3;
-                const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-                float4 vxn, vzn, dxp, dzp;
-                v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp,
-                         dzp);
-                if (ln.owner) {
-                    st4(vxo + colV, vxn);
-                    st4(vzo + colV, vzn);
-                    if (PROD) {
-                        st4(pr + 2 * F + colV, dxp);
-                        st4(pr + 3 * F + colV, dzp);
-                    }
-                }
-            }
-        }
+        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1))
+            ldg_task<PROD, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else
+            ldg_task<PROD, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
     }
 }
 
@@ -241,8 +293,118 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bar, unsigned parity, int l
 
 constexpr int kDrainLimit = 1 << 20;
 
-// MINB = 1 lets the compiler use the registers it wants (about 160, 3 blocks
-// per SM); MINB = 4 caps it at 128 (4 blocks per SM, a few bytes of spill).
+// One task of the bulk-copy kernel; returns false when a pipeline wait gave up
+// (the warp must then leave the kernel).
+template <bool FAST>
+__device__ __forceinline__ bool bulk_task(const StepArgs &a, const ShotDev &Sh, int strip, int xa, int seg_len,
+                                          int kt, int par, bool rec_step, int slot, int lane, unsigned char *ring,
+                                          uint64_t *bars, int S, int drain_limit, unsigned &it0) {
+    const int xb = min(Sh.nnx, xa + seg_len);
+    const size_t ld = (size_t)Sh.ld;
+    const int c = strip * S2D_STRIP_OUT - 4;
+    Lane<FAST> ln;
+    lane_setup(ln, Sh, c, lane, kt);
+    const bool rec = rec_step && slot < Sh.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    // column 0 of the warp's strip in each field (row c), and this lane's rows
+    const size_t wofs = (size_t)(c + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t lofs = wofs + (size_t)(S2D_ZPT * lane);
+    const float *src_vx = Sh.st[par][2] + wofs, *src_px = Sh.st[par][0] + wofs;
+    const float *src_pz = Sh.st[par][1] + wofs, *src_vz = Sh.st[par][3] + wofs;
+    const float *src_k = Sh.kappa + wofs, *src_bx = Sh.bx + wofs, *src_bz = Sh.bz + wofs;
+    float *pxo = Sh.st[par ^ 1][0] + lofs, *pzo = Sh.st[par ^ 1][1] + lofs;
+    float *vxo = Sh.st[par ^ 1][2] + lofs, *vzo = Sh.st[par ^ 1][3] + lofs;
+    const int n_it = xb - xa + 6;  // columns L = xa-3 .. xb+2
+
+    // Producer (lane 0): bring iteration j's columns into stage (it0+j) % S.
+    auto issue = [&](int j) {
+        const unsigned itj = it0 + (unsigned)j;
+        const int s = (int)(itj % (unsigned)S);
+        unsigned char *st = ring + (size_t)s * kStageBytes;
+        const int L = xa - 3 + j;
+        const bool pp = L >= xa, vv = L >= xa + 3;
+        mbar_expect_tx(&bars[s], (unsigned)kSlotBytes * (1u + (pp ? 4u : 0u) + (vv ? 2u : 0u)));
+        if (j == a.fault_iter) return;  // test knob: the stage's bytes never arrive
+        bulk_copy(st, src_vx + (ptrdiff_t)L * (ptrdiff_t)ld, kSlotBytes, &bars[s]);
+        if (pp) {
+            const ptrdiff_t cp = (ptrdiff_t)(L - 1) * (ptrdiff_t)ld;
+            bulk_copy(st + 1 * kSlotBytes, src_px + cp, kSlotBytes, &bars[s]);
+            bulk_copy(st + 2 * kSlotBytes, src_pz + cp, kSlotBytes, &bars[s]);
+            bulk_copy(st + 3 * kSlotBytes, src_k + cp, kSlotBytes, &bars[s]);
+            bulk_copy(st + 4 * kSlotBytes, src_vz + cp, kSlotBytes, &bars[s]);
+        }
+        if (vv) {
+            const ptrdiff_t cv = (ptrdiff_t)(L - 3) * (ptrdiff_t)ld;
+            bulk_copy(st + 5 * kSlotBytes, src_bx + cv, kSlotBytes, &bars[s]);
+            bulk_copy(st + 6 * kSlotBytes, src_bz + cv, kSlotBytes, &bars[s]);
+        }
+    };
+    if (lane == 0) {
+        const int pre = min(S, n_it);
+        for (int j = 0; j < pre; ++j) issue(j);
+    }
+
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 vq0 = zero, vq1 = zero, vq2 = zero, vq3 = zero;
+    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+    float4 zq0 = zero, zq1 = zero, zq2 = zero;
+    for (int j = 0; j < n_it; ++j) {
+        const unsigned itj = it0 + (unsigned)j;
+        const int s = (int)(itj % (unsigned)S);
+        if (!wait_stage(&bars[s], (itj / (unsigned)S) & 1u, a.spin_limit)) {
+            // Give up: record the error, let the copies already issued
+            // land (bounded), and leave without touching global state.
+            if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_WAIT);
+            const int last = min(n_it, j + S);
+            for (int k = j; k < last; ++k) {
+                const unsigned itk = it0 + (unsigned)k;
+                if (!wait_stage(&bars[itk % (unsigned)S], (itk / (unsigned)S) & 1u, drain_limit)) {
+                    if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_DRAIN);
+                }
+            }
+            return false;
+        }
+        const float4 *st = reinterpret_cast<const float4 *>(ring + (size_t)s * kStageBytes) + lane;
+        const int L = xa - 3 + j;
+        vq0 = vq1; vq1 = vq2; vq2 = vq3;
+        vq3 = st[0 * 32];
+        if (L >= xa) {
+            const int P = L - 1;
+            const float4 vz = st[4 * 32];
+            float4 pxn, pzn, dxv, dzv;
+            const float4 pn = p_update(ln, Sh, P, vq0, vq1, vq2, vq3, st[1 * 32], st[2 * 32], st[3 * 32], vz, pxn,
+                                       pzn, dxv, dzv);
+            const bool in_seg = P >= xa && P < xb;
+            const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+            if (in_seg && ln.owner) {
+                st4(pxo + colP, pxn);
+                st4(pzo + colP, pzn);
+            }
+            if (rec && in_seg) record(ln, Sh, P, pn, slot);
+            pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+            zq0 = zq1; zq1 = zq2; zq2 = vz;
+            if (L >= xa + 3) {
+                const int V = L - 3;
+                const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+                float4 vxn, vzn, dxp, dzp;
+                v_update(ln, Sh, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn, dxp, dzp);
+                if (ln.owner) {
+                    st4(vxo + colV, vxn);
+                    st4(vzo + colV, vzn);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && j + S < n_it) {
+            fence_proxy_async();
+            issue(j + S);
+        }
+    }
+    it0 += (unsigned)n_it;
+    return true;
+}
+
+// MINB = 1 lets the compiler use the registers it wants, MINB = 4 caps it at
+// 128 (4 blocks per SM).
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__restrict__ A, int kt_off) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -269,112 +431,16 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
     unsigned it0 = 0;  // pipeline iterations consumed by this warp so far
-
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S_ = task_of(a, t, strip, xa, seg_len);
-        const ShotDev &Sh = S_;
-        const int xb = min(Sh.nnx, xa + seg_len);
-        const size_t ld = (size_t)Sh.ld;
+        const ShotDev &Sh = task_of(a, t, strip, xa, seg_len);
         const int c = strip * S2D_STRIP_OUT - 4;
-        Lane ln;
-        lane_setup(ln, Sh, c, lane, kt);
-        const bool rec = rec_step && slot < Sh.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
-        // column 0 of the warp's strip in each field (row c), and this lane's rows
-        const size_t wofs = (size_t)(c + S2D_GZ) + (size_t)S2D_GX * ld;
-        const size_t lofs = wofs + (size_t)(S2D_ZPT * lane);
-        const float *src_vx = Sh.st[par][2] + wofs, *src_px = Sh.st[par][0] + wofs;
-        const float *src_pz = Sh.st[par][1] + wofs, *src_vz = Sh.st[par][3] + wofs;
-        const float *src_k = Sh.kappa + wofs, *src_bx = Sh.bx + wofs, *src_bz = Sh.bz + wofs;
-        float *pxo = Sh.st[par ^ 1][0] + lofs, *pzo = Sh.st[par ^ 1][1] + lofs;
-        float *vxo = Sh.st[par ^ 1][2] + lofs, *vzo = Sh.st[par ^ 1][3] + lofs;
-        const int n_it = xb - xa + 6;  // columns L = xa-3 .. xb+2
-
-        // Producer (lane 0): bring iteration j's columns into stage (it0+j) % S.
-        auto issue = [&](int j) {
-            const unsigned itj = it0 + (unsigned)j;
-            const int s = (int)(itj % (unsigned)S);
-            unsigned char *st = ring + (size_t)s * kStageBytes;
-            const int L = xa - 3 + j;
-            const bool pp = L >= xa, vv = L >= xa + 3;
-            mbar_expect_tx(&bars[s], (unsigned)kSlotBytes * (1u + (pp ? 4u : 0u) + (vv ? 2u : 0u)));
-            if (j == a.fault_iter) return;  // test knob: the stage's bytes never arrive
-            bulk_copy(st, src_vx + (ptrdiff_t)L * (ptrdiff_t)ld, kSlotBytes, &bars[s]);
-            if (pp) {
-                const ptrdiff_t cp = (ptrdiff_t)(L - 1) * (ptrdiff_t)ld;
-                bulk_copy(st + 1 * kSlotBytes, src_px + cp, kSlotBytes, &bars[s]);
-                bulk_copy(st + 2 * kSlotBytes, src_pz + cp, kSlotBytes, &bars[s]);
-                bulk_copy(st + 3 * kSlotBytes, src_k + cp, kSlotBytes, &bars[s]);
-                bulk_copy(st + 4 * kSlotBytes, src_vz + cp, kSlotBytes, &bars[s]);
-            }
-            if (vv) {
-                const ptrdiff_t cv = (ptrdiff_t)(L - 3) * (ptrdiff_t)ld;
-                bulk_copy(st + 5 * kSlotBytes, src_bx + cv, kSlotBytes, &bars[s]);
-                bulk_copy(st + 6 * kSlotBytes, src_bz + cv, kSlotBytes, &bars[s]);
-            }
-        };
-        if (lane == 0) {
-            const int pre = min(S, n_it);
-            for (int j = 0; j < pre; ++j) issue(j);
-        }
-
-        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 vq0 = zero, vq1 = zero, vq2 = zero, vq3 = zero;
-        float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
-        float4 zq0 = zero, zq1 = zero, zq2 = zero;
-        for (int j = 0; j < n_it; ++j) {
-            const unsigned itj = it0 + (unsigned)j;
-            const int s = (int)(itj % (unsigned)S);
-            if (!wait_stage(&bars[s], (itj / (unsigned)S) & 1u, a.spin_limit)) {
-                // Give up: record the error, let the copies already issued
-                // land (bounded), and leave without touching global state.
-                if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_WAIT);
-                const int last = min(n_it, j + S);
-                for (int k = j; k < last; ++k) {
-                    const unsigned itk = it0 + (unsigned)k;
-                    if (!wait_stage(&bars[itk % (unsigned)S], (itk / (unsigned)S) & 1u, drain_limit)) {
-                        if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_DRAIN);
-                    }
-                }
-                return;
-            }
-            const float4 *st = reinterpret_cast<const float4 *>(ring + (size_t)s * kStageBytes) + lane;
-            const int L = xa - 3 + j;
-            vq0 = vq1; vq1 = vq2; vq2 = vq3;
-            vq3 = st[0 * 32];
-            if (L >= xa) {
-                const int P = L - 1;
-                const float4 vz = st[4 * 32];
-                float4 pxn, pzn, dxv, dzv;
-                const float4 pn = p_update(ln, Sh, P, vq0, vq1, vq2, vq3, st[1 * 32], st[2 * 32], st[3 * 32], vz,
-                                           pxn, pzn, dxv, dzv);
-                const bool in_seg = P >= xa && P < xb;
-                const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
-                if (in_seg && ln.owner) {
-                    st4(pxo + colP, pxn);
-                    st4(pzo + colP, pzn);
-                }
-                if (rec && in_seg) record(ln, Sh, P, pn, slot);
-                pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
-                zq0 = zq1; zq1 = zq2; zq2 = vz;
-                if (L >= xa + 3) {
-                    const int V = L - 3;
-                    const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-                    float4 vxn, vzn, dxp, dzp;
-                    v_update(ln, Sh, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn, dxp, dzp);
-                    if (ln.owner) {
-                        st4(vxo + colV, vxn);
-                        st4(vzo + colV, vzn);
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0 && j + S < n_it) {
-                fence_proxy_async();
-                issue(j + S);
-            }
-        }
-        it0 += (unsigned)n_it;
+        const bool ok = rows_fast(Sh, c, c + S2D_STRIP_ROWS - 1)
+                            ? bulk_task<true>(a, Sh, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring, bars,
+                                              S, drain_limit, it0)
+                            : bulk_task<false>(a, Sh, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring, bars,
+                                               S, drain_limit, it0);
+        if (!ok) return;
     }
 }
 
@@ -428,9 +494,11 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
     else if (variant == kVariantBulk128)
         step_kernel_bulk<4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantLdgProducts)
-        step_kernel_ldg<true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        step_kernel_ldg<true, 3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdg128)
+        step_kernel_ldg<false, 4><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
-        step_kernel_ldg<false><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
@@ -452,13 +520,14 @@ namespace {
 const void *kernel_of(int variant) {
     if (variant == kVariantBulk) return (const void *)step_kernel_bulk<1>;
     if (variant == kVariantBulk128) return (const void *)step_kernel_bulk<4>;
-    if (variant == kVariantLdgProducts) return (const void *)step_kernel_ldg<true>;
-    return (const void *)step_kernel_ldg<false>;
+    if (variant == kVariantLdgProducts) return (const void *)step_kernel_ldg<true, 3>;
+    if (variant == kVariantLdg128) return (const void *)step_kernel_ldg<false, 4>;
+    return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace
 
 int step_kernel_prepare(int variant, size_t smem) {
-    if (variant == kVariantLdg || variant == kVariantLdgProducts) return 0;
+    if (variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128) return 0;
     const void *k = kernel_of(variant);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -466,7 +535,7 @@ int step_kernel_prepare(int variant, size_t smem) {
 }
 
 int step_kernel_occupancy(int variant, int block, size_t smem, int *blocks_per_sm) {
-    const bool ldg = variant == kVariantLdg || variant == kVariantLdgProducts;
+    const bool ldg = variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128;
     return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block, ldg ? 0 : smem);
 }
 

@@ -256,6 +256,7 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     sd.rec_id = reinterpret_cast<const int *>(at(o_rid));
     sd.seis = host_seis ? reinterpret_cast<float *>(at(o_seis)) : seis_out;
     sd.real_nt = rs.real_nt;
+    sd.zfast_lo = sd.zfast_hi = 0;  // every strip takes the general row path
     int bps = 1;
     if (rc == S2D_OK && (step_kernel_occupancy(kVariantLdg, 128, 0, &bps) || bps < 1)) bps = 1;
     int sms = 1;

@@ -40,7 +40,7 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
-VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2}
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -53,7 +53,7 @@ def test_golden_parity(ctx, name, variant):
     try:
         seis = ctx.forward([Shot(m, tuple(z["src"]), z["rec"])], _wave(c))[0]
     finally:
-        ctx.set_option("variant", 1)
+        ctx.set_option("autotune", 1)
     ref = z["seis"]
     assert seis.shape == ref.shape
     err = O.rel_l2(seis, ref)
@@ -197,10 +197,11 @@ def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
         ctx.set_option("task_order", order)
         got = ctx.forward(shot, _wave(c))[0]
     finally:
-        ctx.set_option("stages", 5)
+        ctx.set_option("stages", 3)
         ctx.set_option("block", 128)
         ctx.set_option("seg_len", 0)
         ctx.set_option("task_order", 1)
+        ctx.set_option("autotune", 1)
     np.testing.assert_array_equal(got, base)
 
 
@@ -223,7 +224,7 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx):
     finally:
         ctx.set_option("inject_wait_fault", -1)
         ctx.set_option("spin_limit", 1 << 20)
-        ctx.set_option("variant", 1)
+        ctx.set_option("autotune", 1)
     good = ctx.forward(shot, _wave(c))[0]
     assert O.rel_l2(good, z["seis"]) <= TOL
 
@@ -236,6 +237,8 @@ def test_unknown_option_rejected(ctx):
         ctx.set_option("stages", 1)
     with pytest.raises(Seis2dError):
         ctx.set_option("block", 256)
+    with pytest.raises(Seis2dError):
+        ctx.set_option("autotune", 2)
 
 
 def test_graph_chunking_is_transparent(ctx):
@@ -252,3 +255,106 @@ def test_graph_chunking_is_transparent(ctx):
             np.testing.assert_array_equal(ctx.forward(shot, _wave(c))[0], plain)
     finally:
         ctx.set_option("graph_chunk", 64)
+
+
+def _tall_grid(ctx, nshots=1):
+    """A 70 x 420 model (nb 32) with vertical gradients and a step at row 250,
+    receivers down a column and along the top; 450 steps."""
+    from seis2d_b200 import Shot, Wave
+    nx, nz, nb = 70, 420, 32
+    z = np.arange(nz)[None, :] * 10.0
+    vp = np.broadcast_to(1800.0 + 0.8 * z, (nx, nz)).astype(np.float32)
+    vp[:, 250:] += 400.0
+    rho = np.broadcast_to(1200.0 + 0.3 * z, (nx, nz)).astype(np.float32)
+    rec = np.stack([np.full(40, 300.0), np.arange(40) * 100.0 + 50.0], 1)
+    rec = np.concatenate([rec, np.stack([np.arange(0, 700, 20.0), np.full(35, 20.0)], 1)]).astype(np.float32)
+    wave = Wave(0.45, 0.001, 0.002, 15.0)
+    m = ctx.model(vp, rho, 10.0, 10.0, nb)
+    shots = [Shot(m, (350.0 - 40.0 * k, 2000.0 + 30.0 * k), rec) for k in range(nshots)]
+    p = O.Params(nx, nz, nb, 10.0, 10.0, 0.45, 0.001, 0.002, 15.0)
+    return vp, rho, rec, wave, shots, p
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_tall_grid_fast_rows(ctx, variant):
+    """A grid tall enough for strips clear of the z-sponge (the literal-row
+    fast path): bit-identical with the fast path off, and within the bar of
+    the FP64 oracle."""
+    vp, rho, rec, wave, shot, p = _tall_grid(ctx)
+    ctx.set_option("variant", VARIANTS[variant])
+    try:
+        fast = ctx.forward(shot, wave)[0]
+        ctx.set_option("fast_rows", 0)
+        slow = ctx.forward(shot, wave)[0]
+    finally:
+        ctx.set_option("fast_rows", 1)
+        ctx.set_option("autotune", 1)
+    np.testing.assert_array_equal(fast, slow)
+    ref = O.forward(p, vp, rho, (350.0, 2000.0), rec[:, 0], rec[:, 1], O.F64)
+    assert O.rel_l2(fast, ref) <= TOL
+
+
+def test_variants_compute_the_same_bits(ctx):
+    """Every step-kernel variant gives the same traces bit for bit (they share
+    the update arithmetic), which is what lets the autotuner time candidates
+    on the steps of a live run."""
+    _, _, _, wave, shots, _ = _tall_grid(ctx, nshots=3)
+    out = {}
+    try:
+        for name, v in sorted(VARIANTS.items()):
+            ctx.set_option("variant", v)
+            out[name] = np.concatenate(ctx.forward(shots, wave))
+    finally:
+        ctx.set_option("autotune", 1)
+    for name in out:
+        np.testing.assert_array_equal(out[name], out["ldg"], err_msg=name)
+
+
+def test_autotuner_tunes_once_per_shape_and_keeps_the_bits():
+    """A fresh context tunes on the first run of a batch shape (28 of its
+    steps), reuses the result for the next run of that shape, and the traces
+    equal those of a fixed configuration."""
+    from seis2d_b200 import Context
+    c = Context(0)
+    try:
+        _, _, _, wave, shots, _ = _tall_grid(c, nshots=2)
+        first = c.forward(shots, wave)
+        s1 = c.last_stats
+        again = c.forward(shots, wave)
+        s2 = c.last_stats
+        c.set_option("variant", 1)
+        fixed = c.forward(shots, wave)
+        s3 = c.last_stats
+    finally:
+        c.close()
+    assert s1.autotuned == 1 and s2.autotuned == 0 and s3.autotuned == 0
+    assert (s1.variant, s1.block, s1.stages) == (s2.variant, s2.block, s2.stages)
+    assert s1.variant in (0, 1, 2, 4) and s3.variant == 1
+    for a, b, f in zip(first, again, fixed):
+        np.testing.assert_array_equal(a, f)
+        np.testing.assert_array_equal(b, f)
+
+
+def test_autotuner_skips_short_calls():
+    """A call with fewer steps than two rounds of trials runs untuned, and a
+    later continuation with room tunes without changing the traces."""
+    from seis2d_b200 import Context
+    import torch
+    from seis2d_b200 import derive_steps
+    c = Context(0)
+    try:
+        _, _, rec, wave, shots, _ = _tall_grid(c, nshots=2)
+        nt = derive_steps(wave)["real_nt"]
+        out = torch.zeros(len(shots) * rec.shape[0] * nt, dtype=torch.float32, device="cuda")
+        c.forward(shots, wave, kt_begin=0, kt_count=20, out=out)
+        assert c.last_stats.autotuned == 0
+        c.forward(shots, wave, kt_begin=20, kt_count=0, out=out)
+        assert c.last_stats.autotuned == 1
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().reshape(len(shots), rec.shape[0], nt)
+        c.set_option("variant", 1)
+        ref = c.forward(shots, wave)
+    finally:
+        c.close()
+    for g, r in zip(got, ref):
+        np.testing.assert_array_equal(g, r)
