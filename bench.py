@@ -224,6 +224,41 @@ def surface_shots(nx, d, nshots, nrec=None):
     return src, rec
 
 
+def gradient_leg(ctx, nshots=32, T=3.0):
+    """FWI gradient on the 1201 x 401 models of fwi_models (nb 50, 10 Hz,
+    dt 1 ms, T seconds): the forward of `nshots` shots, then one warm-up
+    gradient and one timed gradient of the same shots, timed with CUDA events."""
+    import torch
+    from seis2d_b200 import Shot, Wave, derive_steps
+    true, start, rho = fwi_models()
+    wave = Wave(T, 0.001, 0.001, 10.0)
+    st = derive_steps(wave)
+    src, rec = surface_shots(1201, 10.0, nshots)
+    mt = ctx.model(true, rho, 10.0, 10.0, 50)
+    dobs = torch.zeros(nshots * rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
+    ctx.forward([Shot(mt, s_, rec) for s_ in src], wave, out=dobs)
+    mt.release()
+    ms = ctx.model(start, rho, 10.0, 10.0, 50)
+    shots = [Shot(ms, s_, rec) for s_ in src]
+    fbuf = torch.zeros_like(dobs)
+    ctx.forward(shots, wave, kt_count=60, out=fbuf)
+    tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
+    gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
+    grho = torch.zeros_like(gvp)
+    # warm-up with the same shot count: an inversion calls the gradient of the
+    # same shapes every iteration, its device buffers then come from the pool
+    ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho)
+    tg, g = _timed(lambda: ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho))
+    res = {"workload": f"FWI gradient, 1201x401 (seeded gradient + two +-300 m/s anomalies; start = gradient), "
+                       f"rho 2000, nb 50, {nshots} shots x 1201 receivers, nt {st['fd_nt']}",
+           "gradient_s_per_shot": tg / nshots, "forward_s_per_shot": tf / nshots,
+           "gradient_over_forward": tg / tf, "misfit": g.misfit,
+           "checkpoint_interval": int(g.stats.grad_segment),
+           "forward_gcells_per_s": ms.padded_cells * nshots * st["fd_nt"] / tf / 1e9}
+    ms.release()
+    return res
+
+
 def extra_legs(device):
     """Rates of the other BASELINE configurations (each a bounded part of its job)."""
     import torch
@@ -289,31 +324,7 @@ def extra_legs(device):
         for mm in models:
             mm.release()
         # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
-        true, start, rho = fwi_models()
-        wave = Wave(3.0, 0.001, 0.001, 10.0)
-        st = derive_steps(wave)
-        src, rec = surface_shots(1201, 10.0, 32)
-        mt = ctx.model(true, rho, 10.0, 10.0, 50)
-        dobs = torch.zeros(32 * rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
-        ctx.forward([Shot(mt, s_, rec) for s_ in src], wave, out=dobs)
-        mt.release()
-        ms = ctx.model(start, rho, 10.0, 10.0, 50)
-        shots = [Shot(ms, s_, rec) for s_ in src]
-        fbuf = torch.zeros_like(dobs)
-        ctx.forward(shots, wave, kt_count=60, out=fbuf)
-        tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
-        gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
-        grho = torch.zeros_like(gvp)
-        ctx.gradient(shots[:2], wave, dobs[: 2 * rec.shape[0] * st["real_nt"]], misfit=True, grad_vp=gvp,
-                     grad_rho=grho)
-        tg, g = _timed(lambda: ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho))
-        out["c5_gradient"] = {"workload": "FWI gradient, 1201x401 (seeded gradient + two +-300 m/s anomalies; "
-                                          "start = gradient), rho 2000, nb 50, 32 shots x 1201 receivers, nt 3000",
-                              "gradient_s_per_shot": tg / 32, "forward_s_per_shot": tf / 32,
-                              "gradient_over_forward": tg / tf, "misfit": g.misfit,
-                              "checkpoint_interval": int(g.stats.grad_segment),
-                              "forward_gcells_per_s": ms.padded_cells * 32 * st["fd_nt"] / tf / 1e9}
-        ms.release()
+        out["c5_gradient"] = gradient_leg(ctx, 32, 3.0)
     return out
 
 
@@ -409,7 +420,18 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the c1/c3/c4/c5 legs")
+    ap.add_argument("--leg", default="main", choices=["main", "gradient"],
+                    help="gradient: only the FWI gradient leg (--shots shots, --grad-time seconds)")
+    ap.add_argument("--grad-time", type=float, default=3.0, help="record length of the gradient leg (s)")
+    ap.add_argument("--grad-segment", type=int, default=0, help="checkpoint interval of the gradient leg (0: auto)")
     args = ap.parse_args()
+    if args.leg == "gradient":
+        import torch
+        from seis2d_b200 import Context
+        with Context(0) as ctx:
+            ctx.set_option("grad_segment", args.grad_segment)
+            print(json.dumps({"leg": "c5_gradient", **gradient_leg(ctx, args.shots or 32, args.grad_time)}))
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -14,7 +14,8 @@
 //   mvx = Dbx mvx' + Gx^T (Kx kappa mPX),  mvz = Dbz mvz' + Gz^T (Kz kappa mPZ)
 // and accumulates the imaging terms
 //   dJ/dkappa += Kx a mPX + Kz c mPZ,  dJ/dbx += Lx g mvx',  dJ/dbz += Lz h mvz'
-// with a, c, g, h of step kt saved by the forward (S2D_STEP_PRODUCTS).
+// with a, c, g, h of step kt saved by the forward (S2D_STEP_PRODUCTS); the
+// last two go straight into dJ/db through the buoyancy averages.
 //
 // The transposes are the gather forms of the reference's operators, edge rows
 // included: with (c0(j), c1(j)) the coefficient pair of forward row j,
@@ -30,35 +31,6 @@ namespace s2d {
 
 namespace {
 
-// Coefficient pair of forward row i along z; interior strips use constants.
-template <bool EDGE>
-__device__ __forceinline__ float zc0m(int i, int n) {
-    if (!EDGE) return kA0;
-    float c0, c1;
-    dm_coef(i, n, c0, c1);
-    return c0;
-}
-template <bool EDGE>
-__device__ __forceinline__ float zc1m(int i, int n) {
-    if (!EDGE) return kA1;
-    float c0, c1;
-    dm_coef(i, n, c0, c1);
-    return c1;
-}
-template <bool EDGE>
-__device__ __forceinline__ float zc0p(int i, int n) {
-    if (!EDGE) return kA0;
-    float c0, c1;
-    dp_coef(i, n, c0, c1);
-    return c0;
-}
-template <bool EDGE>
-__device__ __forceinline__ float zc1p(int i, int n) {
-    if (!EDGE) return kA1;
-    float c0, c1;
-    dp_coef(i, n, c0, c1);
-    return c1;
-}
 __device__ __forceinline__ float xc0m(int i, int n) { float c0, c1; dm_coef(i, n, c0, c1); return c0; }
 __device__ __forceinline__ float xc1m(int i, int n) { float c0, c1; dm_coef(i, n, c0, c1); return c1; }
 __device__ __forceinline__ float xc0p(int i, int n) { float c0, c1; dp_coef(i, n, c0, c1); return c0; }
@@ -66,15 +38,69 @@ __device__ __forceinline__ float xc1p(int i, int n) { float c0, c1; dp_coef(i, n
 
 __device__ __forceinline__ float4 ldrw(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-template <bool EDGE>
+// (H^T m) at the lane's 4 rows from m at those rows and the neighbours' edge
+// values (up_z = m[z0-2], up_w = m[z0-1], dn_x = m[z0+4]); pairs of rows z0-2 .. z0+4.
+template <bool FAST>
+__device__ __forceinline__ float4 hzt(const Lane<FAST> &ln, const float4 &m, float up_z, float up_w, float dn_x) {
+    float a0, a1, b0, b1, c0, c1, d0, d1, e0, e1, f0, f1, g0, g1;
+    zdp(ln, -2, a0, a1);
+    zdp(ln, -1, b0, b1);
+    zdp(ln, 0, c0, c1);
+    zdp(ln, 1, d0, d1);
+    zdp(ln, 2, e0, e1);
+    zdp(ln, 3, f0, f1);
+    zdp(ln, 4, g0, g1);
+    float4 r;
+    r.x = b0 * up_w - c0 * m.x + a1 * up_z - d1 * m.y;
+    r.y = c0 * m.x - d0 * m.y + b1 * up_w - e1 * m.z;
+    r.z = d0 * m.y - e0 * m.z + c1 * m.x - f1 * m.w;
+    r.w = e0 * m.z - f0 * m.w + d1 * m.y - g1 * dn_x;
+    return r;
+}
+// (G^T m) at the lane's 4 rows (up_w = m[z0-1], dn_x = m[z0+4], dn_y = m[z0+5]);
+// pairs of rows z0-1 .. z0+5.
+template <bool FAST>
+__device__ __forceinline__ float4 gzt(const Lane<FAST> &ln, const float4 &m, float up_w, float dn_x, float dn_y) {
+    float a0, a1, b0, b1, c0, c1, d0, d1, e0, e1, f0, f1, g0, g1;
+    zdm(ln, -1, a0, a1);
+    zdm(ln, 0, b0, b1);
+    zdm(ln, 1, c0, c1);
+    zdm(ln, 2, d0, d1);
+    zdm(ln, 3, e0, e1);
+    zdm(ln, 4, f0, f1);
+    zdm(ln, 5, g0, g1);
+    float4 r;
+    r.x = b0 * m.x - c0 * m.y + a1 * up_w - d1 * m.z;
+    r.y = c0 * m.y - d0 * m.z + b1 * m.x - e1 * m.w;
+    r.z = d0 * m.z - e0 * m.w + c1 * m.y - f1 * dn_x;
+    r.w = e0 * m.w - f0 * dn_x + d1 * m.z - g1 * dn_y;
+    return r;
+}
+
+// One (shot, strip, segment) task of the adjoint step.  The warp streams
+// along x: at column L it loads mvx' (the x-gather of H^T needs it at
+// Q-2 .. Q+1); the pressure adjoint, the z-velocity adjoint and the imaging
+// terms are formed at Q = L-1, the x-velocity adjoint at W = L-3 (its G^T
+// x-gather needs Kx kappa mPX at W-1 .. W+2).
+//
+// Imaging per step: dJ/dkappa += Kx a mPX + Kz c mPZ at Q.  The buoyancy
+// terms tbx = Lx g mvx', tbz = Lz h mvz' enter dJ/db through the averages
+// bx = (b[x] + b[x+1]) / 2, bz = (b[z] + b[z+1]) / 2 (cpu_modelling_kernels.cpp:89-119):
+// dJ/db(Q, z) += (tbx(Q) + tbx(Q-1)) / 2 + (tbz(z) + tbz(z-1)) / 2.
+// tbx at the last column and tbz at the last row vanish (the forward D+
+// rows there are zero), so the reference's last-row / last-column
+// replication adds nothing.  tbx(Q-1) comes from the previous column
+// (computed at Q = xa-1 too), tbz(z-1) from the lane above.
+template <bool FAST>
 __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                              int kt, int lane) {
-    const int nnx = S.nnx, nnz = S.nnz;
+    const int nnx = S.nnx;
     const size_t ld = (size_t)S.ld;
     const int xb = min(nnx, xa + seg_len);
     const int c = strip * S2D_STRIP_OUT - 4;
-    const int z0 = c + S2D_ZPT * lane;
-    const bool owner = lane >= 1 && lane <= 30;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    const int z0 = ln.z0;
     const int pin = (kt + 1) & 1, pout = kt & 1;
     const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
@@ -93,22 +119,17 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const float *__restrict__ bzp = S.bz + off;
     const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
     float *__restrict__ gk = S.grad[0] + off;
-    float *__restrict__ gbx = S.grad[1] + off;
-    float *__restrict__ gbz = S.grad[2] + off;
-    float4 zc[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) zc[i] = __ldg(S.zcoef + (z0 + S2D_GZ + i));
+    float *__restrict__ gb = S.grad[1] + off;
     const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
                      (kt + 1) / a.dt_factor - 1 < S.real_nt;
     const int slot = (kt + 1) / a.dt_factor - 1;
-    const int sdz = S.src_z - z0;
+    const bool row0 = FAST || z0 >= 1;  // the lane's first row has a row above it in the grid
 
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 mv0 = zero, mv1 = zero, mv2 = zero, mv3 = zero;  // mvx' at L-3 .. L
     float4 mg0 = zero, mg1 = zero, mg2 = zero, mg3 = zero;  // Lx bx mvx' at L-3 .. L
     float4 ma0 = zero, ma1 = zero, ma2 = zero, ma3 = zero;  // Kx kappa mPX at L-4 .. L-1
-    float4 mc0 = zero, mc1 = zero, mc2 = zero;              // Kz kappa mPZ at L-3 .. L-1
-    float4 mz0 = zero, mz1 = zero, mz2 = zero;              // mvz' at L-3 .. L-1
+    float4 tbp = zero;                                      // tbx at Q-1
 
     for (int L = xa - 3; L <= xb + 2; ++L) {
         {
@@ -120,46 +141,38 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             mg3 = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z, (lx * b.w) * m.w);
         }
         if (L < xa) continue;
-        // ---- pressure adjoint at column Q = L - 1 ----
         const int Q = L - 1;
         const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
         const bool in_seg = Q >= xa && Q < xb;
-        const bool upd = in_seg && owner;  // this lane writes column Q
+        const bool upd = in_seg && ln.owner;       // this lane writes column Q
+        const bool img = Q >= 0 && Q < xb;         // buoyancy terms at Q (xa-1 feeds column xa)
         const float4 mpx = ld4(mpxi + colQ), mpz = ld4(mpzi + colQ), mvz = ld4(mvzi + colQ);
         const float4 bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
-        // products of the forward step and the accumulators, loaded up front
-        float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tbx = zero, tbz = zero;
+        float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tb = zero;
         if (upd) {
             pa = ld4(pr + colQ);
             pc = ld4(pr + F + colQ);
+            tk = ldrw(gk + colQ);
+            tb = ldrw(gb + colQ);
+        }
+        if (img) {
             pg = ld4(pr + 2 * F + colQ);
             ph = ld4(pr + 3 * F + colQ);
-            tk = ldrw(gk + colQ);
-            tbx = ldrw(gbx + colQ);
-            tbz = ldrw(gbz + colQ);
         }
         const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
-        const float4 h = make_float4((zc[0].w * bz.x) * mvz.x, (zc[1].w * bz.y) * mvz.y,
-                                     (zc[2].w * bz.z) * mvz.z, (zc[3].w * bz.w) * mvz.w);
-        const float h_up_z = __shfl_up_sync(kFull, h.z, 1);
-        const float h_up_w = __shfl_up_sync(kFull, h.w, 1);
-        const float h_dn_x = __shfl_down_sync(kFull, h.x, 1);
-        float4 q;
+        const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
+        // ---- pressure adjoint at Q ----
+        const float4 h = make_float4((r0.w * bz.x) * mvz.x, (r1.w * bz.y) * mvz.y, (r2.w * bz.z) * mvz.z,
+                                     (r3.w * bz.w) * mvz.w);
+        float4 q = hzt(ln, h, __shfl_up_sync(kFull, h.z, 1), __shfl_up_sync(kFull, h.w, 1),
+                       __shfl_down_sync(kFull, h.x, 1));
         {
             const float p0a = xc0p(Q - 1, nnx), p0b = xc0p(Q, nnx), p1a = xc1p(Q - 2, nnx), p1b = xc1p(Q + 1, nnx);
-            q.x = p0a * mg1.x - p0b * mg2.x + p1a * mg0.x - p1b * mg3.x;
-            q.y = p0a * mg1.y - p0b * mg2.y + p1a * mg0.y - p1b * mg3.y;
-            q.z = p0a * mg1.z - p0b * mg2.z + p1a * mg0.z - p1b * mg3.z;
-            q.w = p0a * mg1.w - p0b * mg2.w + p1a * mg0.w - p1b * mg3.w;
+            q.x += p0a * mg1.x - p0b * mg2.x + p1a * mg0.x - p1b * mg3.x;
+            q.y += p0a * mg1.y - p0b * mg2.y + p1a * mg0.y - p1b * mg3.y;
+            q.z += p0a * mg1.z - p0b * mg2.z + p1a * mg0.z - p1b * mg3.z;
+            q.w += p0a * mg1.w - p0b * mg2.w + p1a * mg0.w - p1b * mg3.w;
         }
-        q.x += zc0p<EDGE>(z0 - 1, nnz) * h_up_w - zc0p<EDGE>(z0, nnz) * h.x + zc1p<EDGE>(z0 - 2, nnz) * h_up_z -
-               zc1p<EDGE>(z0 + 1, nnz) * h.y;
-        q.y += zc0p<EDGE>(z0, nnz) * h.x - zc0p<EDGE>(z0 + 1, nnz) * h.y + zc1p<EDGE>(z0 - 1, nnz) * h_up_w -
-               zc1p<EDGE>(z0 + 2, nnz) * h.z;
-        q.z += zc0p<EDGE>(z0 + 1, nnz) * h.y - zc0p<EDGE>(z0 + 2, nnz) * h.z + zc1p<EDGE>(z0, nnz) * h.x -
-               zc1p<EDGE>(z0 + 3, nnz) * h.w;
-        q.w += zc0p<EDGE>(z0 + 2, nnz) * h.z - zc0p<EDGE>(z0 + 3, nnz) * h.w + zc1p<EDGE>(z0 + 1, nnz) * h.y -
-               zc1p<EDGE>(z0 + 4, nnz) * h_dn_x;
         // Transpose of the receiver sampling (cpumodelling.cpp:356-360).  Every
         // warp computing column Q adds it (halo columns included, they feed the
         // neighbours' velocity adjoint); the receiver table covers columns
@@ -181,33 +194,46 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const float4 mPZ = make_float4(mpz.x + q.x, mpz.y + q.y, mpz.z + q.z, mpz.w + q.w);
         if (upd) {
             st4(mpxo + colQ, make_float4(xq.x * mPX.x, xq.x * mPX.y, xq.x * mPX.z, xq.x * mPX.w));
-            st4(mpzo + colQ, make_float4(zc[0].x * mPZ.x, zc[1].x * mPZ.y, zc[2].x * mPZ.z, zc[3].x * mPZ.w));
-            tk.x += (xq.y * pa.x) * mPX.x + (zc[0].y * pc.x) * mPZ.x;
-            tk.y += (xq.y * pa.y) * mPX.y + (zc[1].y * pc.y) * mPZ.y;
-            tk.z += (xq.y * pa.z) * mPX.z + (zc[2].y * pc.z) * mPZ.z;
-            tk.w += (xq.y * pa.w) * mPX.w + (zc[3].y * pc.w) * mPZ.w;
+            st4(mpzo + colQ, make_float4(r0.x * mPZ.x, r1.x * mPZ.y, r2.x * mPZ.z, r3.x * mPZ.w));
+            tk.x += (xq.y * pa.x) * mPX.x + (r0.y * pc.x) * mPZ.x;
+            tk.y += (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
+            tk.z += (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
+            tk.w += (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
             st4(gk + colQ, tk);
-            tbx.x += (xq.w * pg.x) * mv2.x;
-            tbx.y += (xq.w * pg.y) * mv2.y;
-            tbx.z += (xq.w * pg.z) * mv2.z;
-            tbx.w += (xq.w * pg.w) * mv2.w;
-            st4(gbx + colQ, tbx);
-            tbz.x += (zc[0].w * ph.x) * mvz.x;
-            tbz.y += (zc[1].w * ph.y) * mvz.y;
-            tbz.z += (zc[2].w * ph.z) * mvz.z;
-            tbz.w += (zc[3].w * ph.w) * mvz.w;
-            st4(gbz + colQ, tbz);
-            if (Q == S.src_x && sdz >= 0 && sdz < 4) S.srcadj[kt] = comp(mPX, sdz);
+            if (Q == S.src_x && ln.sdz >= 0 && ln.sdz < 4) S.srcadj[kt] = comp(mPX, ln.sdz);
         }
         ma0 = ma1; ma1 = ma2; ma2 = ma3;
         ma3 = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
                           (xq.y * kk.w) * mPX.w);
-        mc0 = mc1; mc1 = mc2;
-        mc2 = make_float4((zc[0].y * kk.x) * mPZ.x, (zc[1].y * kk.y) * mPZ.y, (zc[2].y * kk.z) * mPZ.z,
-                          (zc[3].y * kk.w) * mPZ.w);
-        mz0 = mz1; mz1 = mz2; mz2 = mvz;
+        // ---- z-velocity adjoint at Q ----
+        {
+            const float4 mc = make_float4((r0.y * kk.x) * mPZ.x, (r1.y * kk.y) * mPZ.y, (r2.y * kk.z) * mPZ.z,
+                                          (r3.y * kk.w) * mPZ.w);
+            const float4 g = gzt(ln, mc, __shfl_up_sync(kFull, mc.w, 1), __shfl_down_sync(kFull, mc.x, 1),
+                                 __shfl_down_sync(kFull, mc.y, 1));
+            if (upd)
+                st4(mvzo + colQ, make_float4(r0.z * mvz.x + g.x, r1.z * mvz.y + g.y, r2.z * mvz.z + g.z,
+                                             r3.z * mvz.w + g.w));
+        }
+        // ---- buoyancy imaging at Q ----
+        if (img) {
+            const float4 tbx = make_float4((xq.w * pg.x) * mv2.x, (xq.w * pg.y) * mv2.y, (xq.w * pg.z) * mv2.z,
+                                           (xq.w * pg.w) * mv2.w);
+            const float4 tbz = make_float4((r0.w * ph.x) * mvz.x, (r1.w * ph.y) * mvz.y, (r2.w * ph.z) * mvz.z,
+                                           (r3.w * ph.w) * mvz.w);
+            const float up = __shfl_up_sync(kFull, tbz.w, 1);
+            if (upd) {
+                const float4 px = Q >= 1 ? tbp : zero;
+                tb.x += 0.5f * ((tbx.x + px.x) + (tbz.x + (row0 ? up : 0.0f)));
+                tb.y += 0.5f * ((tbx.y + px.y) + (tbz.y + tbz.x));
+                tb.z += 0.5f * ((tbx.z + px.z) + (tbz.z + tbz.y));
+                tb.w += 0.5f * ((tbx.w + px.w) + (tbz.w + tbz.z));
+                st4(gb + colQ, tb);
+            }
+            tbp = tbx;
+        }
         if (L < xa + 3) continue;
-        // ---- velocity adjoint at column W = L - 3 ----
+        // ---- x-velocity adjoint at W = L - 3 ----
         const int W = L - 3;
         const ptrdiff_t colW = (ptrdiff_t)W * (ptrdiff_t)ld;
         const float dbx = __ldg(S.xcoef + (W + S2D_GX)).z;
@@ -217,27 +243,14 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         ovx.y = dbx * mv0.y + (m0a * ma1.y - m0b * ma2.y + m1a * ma0.y - m1b * ma3.y);
         ovx.z = dbx * mv0.z + (m0a * ma1.z - m0b * ma2.z + m1a * ma0.z - m1b * ma3.z);
         ovx.w = dbx * mv0.w + (m0a * ma1.w - m0b * ma2.w + m1a * ma0.w - m1b * ma3.w);
-        const float4 cc = mc0;
-        const float c_up_w = __shfl_up_sync(kFull, cc.w, 1);
-        const float c_dn_x = __shfl_down_sync(kFull, cc.x, 1);
-        const float c_dn_y = __shfl_down_sync(kFull, cc.y, 1);
-        float4 ovz;
-        ovz.x = zc[0].z * mz0.x + (zc0m<EDGE>(z0, nnz) * cc.x - zc0m<EDGE>(z0 + 1, nnz) * cc.y +
-                                   zc1m<EDGE>(z0 - 1, nnz) * c_up_w - zc1m<EDGE>(z0 + 2, nnz) * cc.z);
-        ovz.y = zc[1].z * mz0.y + (zc0m<EDGE>(z0 + 1, nnz) * cc.y - zc0m<EDGE>(z0 + 2, nnz) * cc.z +
-                                   zc1m<EDGE>(z0, nnz) * cc.x - zc1m<EDGE>(z0 + 3, nnz) * cc.w);
-        ovz.z = zc[2].z * mz0.z + (zc0m<EDGE>(z0 + 2, nnz) * cc.z - zc0m<EDGE>(z0 + 3, nnz) * cc.w +
-                                   zc1m<EDGE>(z0 + 1, nnz) * cc.y - zc1m<EDGE>(z0 + 4, nnz) * c_dn_x);
-        ovz.w = zc[3].z * mz0.w + (zc0m<EDGE>(z0 + 3, nnz) * cc.w - zc0m<EDGE>(z0 + 4, nnz) * c_dn_x +
-                                   zc1m<EDGE>(z0 + 2, nnz) * cc.z - zc1m<EDGE>(z0 + 5, nnz) * c_dn_y);
-        if (owner) {
-            st4(mvxo + colW, ovx);
-            st4(mvzo + colW, ovz);
-        }
+        if (ln.owner) st4(mvxo + colW, ovx);
     }
 }
 
-__global__ void __launch_bounds__(128) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
+// MINB blocks of 4 warps per SM: 2 leaves the compiler its registers (no
+// spills), 3 caps them at 168 (some spills, 12 warps per SM).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -249,11 +262,11 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const StepArgs *__restrict
         const ShotDev &S = task_of(a, t, strip, xa, seg_len);
         if (!task_in_bounds(a, S, strip, xa, seg_len, kt, true, 2)) continue;
         const int c = strip * S2D_STRIP_OUT - 4;
-        // rows c-2 .. c+129 all carry the interior coefficient pairs
-        if (strip >= 1 && c + 132 <= S.nnz)
-            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane);
-        else
+        // the z-transposes read the coefficient pairs of rows c-2 .. c+129
+        if (rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1))
             adjoint_task<true>(a, S, strip, xa, seg_len, kt, lane);
+        else
+            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane);
     }
 }
 
@@ -270,40 +283,29 @@ __global__ void add_source_terms(float *const *gk, const int *cells, const doubl
     for (int s = 0; s < nshots; ++s) gk[s][cells[s]] = (float)((double)gk[s][cells[s]] + vals[s]);
 }
 
-__global__ void sum_shots(float *const *gk, float *const *gbx, float *const *gbz, int nshots, int nnx, int nnz,
-                          int ld, float *tk, float *tbx, float *tbz) {
+__global__ void sum_shots(float *const *gk, float *const *gb, int nshots, int nnx, int nnz, int ld, float *tk,
+                          float *tb) {
     const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
     if (z >= nnz || x >= nnx) return;
     const size_t id = pad_id(x, z, ld);
-    double a = 0, b = 0, c = 0;
+    double a = 0, b = 0;
     for (int s = 0; s < nshots; ++s) {
         a += gk[s][id];
-        b += gbx[s][id];
-        c += gbz[s][id];
+        b += gb[s][id];
     }
     tk[id] = (float)a;
-    tbx[id] = (float)b;
-    tbz[id] = (float)c;
+    tb[id] = (float)b;
 }
 
-// dJ/db from dJ/dbx, dJ/dbz (transpose of cpu_modelling_kernels.cpp:89-119),
-// then kappa = vp^2 rho and b = 1/rho.
-__global__ void chain_rule(const float *tk, const float *tbx, const float *tbz, const float *vp, const float *rho,
-                           int nx, int nz, int nb, int ld, float *gvp, float *grho) {
+// kappa = vp^2 rho and b = 1/rho (the buoyancy averages are folded into dJ/db
+// by the adjoint step).
+__global__ void chain_rule(const float *tk, const float *tb, const float *vp, const float *rho, int nx, int nz,
+                           int nb, int ld, float *gvp, float *grho) {
     const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
     const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
     if (z >= nnz || x >= nnx) return;
     const size_t id = pad_id(x, z, ld);
-    double gb = 0;
-    if (z < nnz - 1) gb += 0.5 * tbz[id];
-    if (z >= 1) gb += 0.5 * tbz[id - 1];
-    if (x < nnx - 1) gb += 0.5 * tbx[id];
-    if (x >= 1) gb += 0.5 * tbx[id - ld];
-    if (x == nnx - 2) {
-        const size_t last = id + ld;
-        if (z < nnz - 1) gb += 0.5 * tbx[last];
-        if (z >= 1) gb += 0.5 * tbx[last - 1];
-    }
+    const double gb = tb[id];
     const int mx = min(max(x - nb, 0), nx - 1), mz = min(max(z - nb, 0), nz - 1);
     const double v = vp[(size_t)mx * nz + mz], r = rho[(size_t)mx * nz + mz];
     gvp[id] = (float)(2.0 * v * r * (double)tk[id]);
@@ -352,26 +354,30 @@ __global__ void residual_kernel(const float *seis, const float *obs, float *res,
 
 }  // namespace
 
-int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream) {
-    adjoint_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream) {
+    if (minb >= 3)
+        adjoint_kernel<3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else
+        adjoint_kernel<2><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
-int adjoint_kernel_occupancy(int block, int *blocks_per_sm) {
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint_kernel, block, 0);
+int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        blocks_per_sm, minb >= 3 ? adjoint_kernel<3> : adjoint_kernel<2>, block, 0);
 }
 
-int launch_gradient_finalize(float *const *gk, float *const *gbx, float *const *gbz, int nshots,
-                             const int *src_cells, const double *src_vals, const float *vp, const float *rho,
-                             int nx, int nz, int nb, int ld, float *tmp3, float *gvp_pad, float *grho_pad,
-                             float *grad_vp, float *grad_rho, void *stream) {
+int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
+                             const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
+                             int ld, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
+                             void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
     add_source_terms<<<1, 1, 0, st>>>(gk, src_cells, src_vals, nshots);
     dim3 blk(256), grd((nnz + 255) / 256, nnx);
-    sum_shots<<<grd, blk, 0, st>>>(gk, gbx, gbz, nshots, nnx, nnz, ld, tmp3, tmp3 + F, tmp3 + 2 * F);
-    chain_rule<<<grd, blk, 0, st>>>(tmp3, tmp3 + F, tmp3 + 2 * F, vp, rho, nx, nz, nb, ld, gvp_pad, grho_pad);
+    sum_shots<<<grd, blk, 0, st>>>(gk, gb, nshots, nnx, nnz, ld, tmp2, tmp2 + F);
+    chain_rule<<<grd, blk, 0, st>>>(tmp2, tmp2 + F, vp, rho, nx, nz, nb, ld, gvp_pad, grho_pad);
     dim3 grd2((nz + 255) / 256, nx);
     fold_sponge<<<grd2, blk, 0, st>>>(gvp_pad, grho_pad, nx, nz, nb, ld, grad_vp, grad_rho);
     return (int)cudaGetLastError();

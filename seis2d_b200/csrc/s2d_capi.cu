@@ -143,6 +143,7 @@ struct Ctx {
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
+    int opt_adj_minb = 3;     // adjoint kernel compiled for 2 or 3 blocks per SM
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     // Launch-argument block read by every step launch, and the graphs of step
@@ -291,15 +292,10 @@ int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
 }
 
 // Segment lengths, segment counts and task ranges of the batch's groups for
-// the resident warps of launch configuration `lc`; uploaded when they change.
-int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
-    const std::vector<long> key = {lc.variant, lc.block, lc.stages, c->opt_seg_len};
+// `resident_warps` warps looping over the tasks of a launch; uploaded when
+// `key` differs from the layout in place.
+int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<long> &key) {
     if (b.layout == key) return S2D_OK;
-    // resident warps of the configuration (its grid when the work is smaller)
-    LaunchCfg full;
-    int e = launch_config(c, 1L << 40, &full, lc.variant, lc.block, lc.stages);
-    if (e) return e;
-    const long resident_warps = (long)full.grid * (full.block / 32);
     long per_seg_total = 0;
     for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
     long max_tasks = 0;
@@ -329,6 +325,17 @@ int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
     b.max_tasks = max_tasks;
     b.layout = key;
     return S2D_OK;
+}
+
+// The layout for the resident warps of launch configuration `lc`.
+int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
+    const std::vector<long> key = {lc.variant, lc.block, lc.stages, c->opt_seg_len};
+    if (b.layout == key) return S2D_OK;
+    // resident warps of the configuration (its grid when the work is smaller)
+    LaunchCfg full;
+    int e = launch_config(c, 1L << 40, &full, lc.variant, lc.block, lc.stages);
+    if (e) return e;
+    return layout_groups_for(c, b, (long)full.grid * (full.block / 32), key);
 }
 
 // Graph of `n` step launches (kt_off = 0..n-1) for one launch configuration,
@@ -752,6 +759,9 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "adjoint_blocks") {
+        if (value != 2 && value != 3) return fail(c, S2D_ERR_ARG, "adjoint_blocks must be 2 or 3");
+        c->opt_adj_minb = (int)value;
     } else if (k == "fast_rows") {
         c->opt_fast_rows = value ? 1 : 0;
     } else if (k == "graph_chunk") {
@@ -1039,19 +1049,19 @@ int run_adjoint(Ctx *c, Batch &b, GradRun &g, StepArgs args, int kt_top, int n, 
         *launches += 1 + m;
         if (!use_graph) {
             for (int k = 0; k < m; ++k) {
-                e = launch_adjoint(args_d, k, grid, 128, c->stream);
+                e = launch_adjoint(args_d, k, grid, 128, c->opt_adj_minb, c->stream);
                 if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
             }
             continue;
         }
         (void)g;
-        const std::vector<long> key = {m, grid};
+        const std::vector<long> key = {m, grid, c->opt_adj_minb};
         auto it = c->adj_graphs.find(key);
         if (it == c->adj_graphs.end()) {
             cudaGraph_t gr;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < m; ++k) {
-                e = launch_adjoint(args_d, k, grid, 128, c->stream);
+                e = launch_adjoint(args_d, k, grid, 128, c->opt_adj_minb, c->stream);
                 if (e) {
                     cudaStreamEndCapture(c->stream, &gr);
                     if (gr) cudaGraphDestroy(gr);
@@ -1108,7 +1118,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
 
     // per-shot adjoint state, accumulators and source-adjoint trace
     std::vector<ShotDev> adj = b.shot_dev;
-    std::vector<float *> gk(nshots), gbx(nshots), gbz(nshots), sadj(nshots);
+    std::vector<float *> gk(nshots), gb(nshots), sadj(nshots);
     for (int s = 0; s < nshots; ++s) {
         for (int par = 0; par < 2; ++par)
             for (int f = 0; f < 4; ++f) {
@@ -1119,15 +1129,14 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
                 adj[s].st[par][f] = static_cast<float *>(p);
             }
         void *p;
-        for (int f = 0; f < 3; ++f) {
+        for (int f = 0; f < 2; ++f) {
             int e = grad_alloc(c, g, fb, &p);
             if (e) return e;
             CK(cudaMemsetAsync(p, 0, fb, c->stream));
             adj[s].grad[f] = static_cast<float *>(p);
         }
         gk[s] = adj[s].grad[0];
-        gbx[s] = adj[s].grad[1];
-        gbz[s] = adj[s].grad[2];
+        gb[s] = adj[s].grad[1];
         int e = grad_alloc(c, g, sizeof(float) * rs.fd_nt, &p);
         if (e) return e;
         CK(cudaMemsetAsync(p, 0, sizeof(float) * rs.fd_nt, c->stream));
@@ -1217,17 +1226,36 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
                                    cudaMemcpyDeviceToDevice, c->stream));
         return S2D_OK;
     };
+    // The steps that keep their products (the last segment of the sweep, the
+    // recomputes) and the adjoint steps run with a task layout for the
+    // resident warps of the adjoint kernel: the two kernels of the backward
+    // phase then each take whole rounds of tasks.
+    int agrid = 1;
+    auto backward_layout = [&]() -> int {
+        int bps = 0;
+        if (adjoint_kernel_occupancy(128, c->opt_adj_minb, &bps) || bps < 1) bps = 1;
+        const long resident = (long)c->sm_count * bps;
+        int e = layout_groups_for(c, b, resident * 4, {-1, resident, c->opt_seg_len});
+        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts, 128, 0);
+        if (e) return e;
+        agrid = (int)std::max<long>(1, std::min<long>(resident, (b.max_tasks * 32 + 127) / 128));
+        fa.total_tasks = batch_tasks(b);
+        return S2D_OK;
+    };
     for (int j = 0; j < nseg; ++j) {
         const int k0 = j * C, n = std::min(C, rs.fd_nt - k0);
-        StepArgs a = fa;
         if (j < nseg - 1) {
+            StepArgs a = fa;
             int e = save_ckpt(j);
             if (!e) e = run_loop(c, b, lc_fwd, a, k0, n, use_graph, &launches, &graph_used);
             if (e) return e;
         } else {
+            int e = backward_layout();
+            if (e) return e;
+            StepArgs a = fa;
             a.flags = S2D_STEP_PRODUCTS;
             a.prod_kt0 = k0;
-            int e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
+            e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
             if (e) return e;
         }
     }
@@ -1248,12 +1276,6 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         CK(cudaMemcpyAsync(adj_src, data, nseis * sizeof(float), dk, c->stream));
     }
     // ---- backward over the segments ----
-    int agrid = 1;
-    {
-        int bps = 0;
-        if (adjoint_kernel_occupancy(128, &bps) || bps < 1) bps = 1;
-        agrid = (int)std::max<long>(1, std::min<long>((long)c->sm_count * bps, (b.max_tasks * 32 + 127) / 128));
-    }
     StepArgs aa = fa;
     aa.shots = adj_table.as<ShotDev>();
     aa.err = c->dev_err.as<int>();
@@ -1315,24 +1337,23 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     {
         int e = grad_alloc(c, g, sizeof(int) * nshots, &p_cells);
         if (!e) e = grad_alloc(c, g, sizeof(double) * nshots, &p_vals);
-        if (!e) e = grad_alloc(c, g, sizeof(float *) * 3 * nshots, &p_ptrs);
-        if (!e) e = grad_alloc(c, g, 3 * fb, &p_tmp);
+        if (!e) e = grad_alloc(c, g, sizeof(float *) * 2 * nshots, &p_ptrs);
+        if (!e) e = grad_alloc(c, g, 2 * fb, &p_tmp);
         if (!e) e = grad_alloc(c, g, 2 * fb, &p_pad);
         if (!e && !dev_grad) e = grad_alloc(c, g, 2 * sizeof(float) * m.nx * m.nz, &p_out);
         if (e) return e;
     }
     std::vector<float *> ptrs;
     ptrs.insert(ptrs.end(), gk.begin(), gk.end());
-    ptrs.insert(ptrs.end(), gbx.begin(), gbx.end());
-    ptrs.insert(ptrs.end(), gbz.begin(), gbz.end());
+    ptrs.insert(ptrs.end(), gb.begin(), gb.end());
     CK(cudaMemcpyAsync(p_cells, cells.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(p_vals, vals.data(), sizeof(double) * nshots, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(p_ptrs, ptrs.data(), sizeof(float *) * 3 * nshots, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(p_ptrs, ptrs.data(), sizeof(float *) * 2 * nshots, cudaMemcpyHostToDevice, c->stream));
     float **dptrs = static_cast<float **>(p_ptrs);
     float *out_vp = dev_grad ? grad_vp : static_cast<float *>(p_out);
     float *out_rho = dev_grad ? grad_rho : static_cast<float *>(p_out) + (size_t)m.nx * m.nz;
     {
-        int e = launch_gradient_finalize(dptrs, dptrs + nshots, dptrs + 2 * nshots, nshots,
+        int e = launch_gradient_finalize(dptrs, dptrs + nshots, nshots,
                                          static_cast<int *>(p_cells), static_cast<double *>(p_vals),
                                          m.vp.as<float>(), m.rho.as<float>(), m.nx, m.nz, m.nb, m.ld,
                                          static_cast<float *>(p_tmp), static_cast<float *>(p_pad),

@@ -47,7 +47,7 @@ struct ShotDev {
     int pad_;
     // gradient runs only
     float *prod;                   // [steps][4][field]: D-x vx, D-z vz, D+x p, D+z p of each step
-    float *grad[3];                // accumulators dJ/dkappa, dJ/dbx, dJ/dbz (padded layout)
+    float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout)
     float *srcadj;                 // [fd_nt] adjoint pressure at the source after each step
     // element counts of the buffers above (device self-checks, S2D_DEVICE_CHECKS)
     size_t nfield;                 // every per-cell field
@@ -120,14 +120,14 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
                 void *stream);
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
 // Adjoint FD step (step kt = args.kt_base - kt_off) and the gradient finalisation.
-int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, void *stream);
-int adjoint_kernel_occupancy(int block, int *blocks_per_sm);
-// Sum the shots' accumulators, apply the buoyancy averaging transpose and the
-// kappa = vp^2 rho, b = 1/rho chain rule, fold the sponge onto the model.
-int launch_gradient_finalize(float *const *gk, float *const *gbx, float *const *gbz, int nshots,
-                             const int *src_cells, const double *src_vals, const float *vp, const float *rho,
-                             int nx, int nz, int nb, int ld, float *tmp3, float *gvp_pad, float *grho_pad,
-                             float *grad_vp, float *grad_rho, void *stream);
+int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream);
+int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm);
+// Sum the shots' accumulators (dJ/dkappa, dJ/db), apply the kappa = vp^2 rho,
+// b = 1/rho chain rule and fold the sponge onto the model.
+int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
+                             const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
+                             int ld, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
+                             void *stream);
 // Residual d - d_obs in place of d_obs... : res[i] = seis[i] - obs[i]; partial sums of res^2.
 int launch_residual(const float *seis, const float *obs, float *res, size_t n, double *sumsq, void *stream);
 int launch_prepare_model(const float *vp, const float *rho, int nx, int nz, int nb, int ld,
