@@ -38,7 +38,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-B_ALG = 44.0  # algorithmic bytes per padded-cell update: 4 state fields r+w (32) + 3 materials (12)
+# Algorithmic bytes per padded-cell update (the library reports them per run
+# in stats.alg_bytes): 4 state fields read and written (32 B) + 3 materials
+# (12 B) = 44 B; 36 B where both pressure dampings are 1 and the cell carries
+# p = px + pz alone.
 
 WORKLOADS = {
     "c2": dict(nx=5000, nz=5000, d=5.0, nb=60, vp=(2000.0, 3500.0), rho=(1800.0, 2300.0), iface=2500,
@@ -278,7 +281,7 @@ def extra_legs(device):
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         cells = m.padded_cells * st["fd_nt"]
         out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
-                     "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": 44 * cells / t / 1e9 / peak,
+                     "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": ctx.last_stats.alg_bytes / t / 1e9 / peak,
                      "note": "whole job ~37 MB of state: L2-resident"}
         m.release()
         # c3: salt 3201x1201, d 7.62, nb 50, 20 Hz, dt 0.6 ms, nt 10000, 1 shot; 1000 of the 10000 steps
@@ -294,9 +297,10 @@ def extra_legs(device):
         t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=1000, out=buf, sync=False))
         cells = m.padded_cells * 1000
         rate = cells / t / 1e9
+        frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         out["c3"] = {"workload": "3201x1201 salt (seeded), d 7.62, nb 50, 1 shot, 1000 of 10000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (m.padded_cells * st["fd_nt"]),
-                     "roofline_frac": 44 * rate / peak}
+                     "roofline_frac": frac}
         m.release()
         # c4: 48 shots on three layered models of uneven size, one launch sequence; 300 of 3000 steps
         wave = Wave(2.3996, 0.0008, 0.0008, 15.0)
@@ -315,12 +319,13 @@ def extra_legs(device):
         ctx.forward(shots, wave, kt_count=60, out=buf)
         t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=60, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
+        frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
         prate = cells_step * 60 / tp / 1e9
         out["c4"] = {"workload": "48 shots on 601x301 / 1201x601 / 2401x801 layered models (16 each), nb 50, "
                                  "one launch per step for all; 300 of 3000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (cells_step / 48 * st["fd_nt"]),
-                     "plain_gcells_per_s": prate, "roofline_frac": 44 * rate / peak}
+                     "plain_gcells_per_s": prate, "roofline_frac": frac}
         for mm in models:
             mm.release()
         # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
@@ -515,12 +520,13 @@ def main():
         ctx.forward(shots, wave, kt_begin=kt_r, kt_count=n_r, out=seis_dev)
         st = ctx.last_stats
         per_launch_s = st.loop_ms * 1e-3 / n_r
+        bytes_launch = st.alg_bytes / n_r
         peak, peak_kind = measured_peak()
-        achieved = B_ALG * cells_step / per_launch_s / 1e9
+        achieved = bytes_launch / per_launch_s / 1e9
         tr = traffic_per_launch(args.workload)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": tr, "peak_source": peak_kind, "bytes_per_launch": B_ALG * cells_step,
-                "launch_ms": per_launch_s * 1e3}
+                "traffic": tr, "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
+                "bytes_per_cell_update": bytes_launch / cells_step, "launch_ms": per_launch_s * 1e3}
 
     # ---- plain: the same shots one after another ----
     plain = None

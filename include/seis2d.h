@@ -112,6 +112,9 @@ typedef struct {
     int variant, block, stages;  /* launch configuration of the time loop     */
     int seg_len;             /* columns per warp task (first model group)     */
     int autotuned;           /* 1 if this call ran the autotuner's trials     */
+    double alg_bytes;        /* s2d_forward: algorithmic DRAM bytes of the loop:
+                                44 B per cell-update, 36 B where both pressure
+                                dampings are 1 (the cell carries p alone)     */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */

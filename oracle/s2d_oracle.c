@@ -286,8 +286,17 @@ static void f32_step(f32_state *s, int isrc, float src_add, int inject) {
             float dvx = cx0 * (AT(s->vx, ix, iz) - AT(s->vx, ix - 1, iz)) + cx1 * (AT(s->vx, ix + 1, iz) - AT(s->vx, ix - 2, iz));
             float dvz = cz0 * (AT(s->vz, ix, iz) - AT(s->vz, ix, iz - 1)) + cz1 * (AT(s->vz, ix, iz + 1) - AT(s->vz, ix, iz - 2));
             float k = s->kappa[id];
-            s->px[id] = s->damp2a[ix] * s->px[id] + (s->kxa[ix] * k) * dvx;
-            s->pz[id] = s->damp1a[iz] * s->pz[id] + (s->kza[iz] * k) * dvz;
+            if (s->damp2a[ix] == 1.0f && s->damp1a[iz] == 1.0f) {
+                /* Both split fields undamped: they only enter through
+                 * p = px + pz, so the cell carries p alone (px = p, pz = 0),
+                 * as the CUDA kernels do.  Same scheme in exact arithmetic. */
+                float t = s->kxa[ix] * dvx + s->kza[iz] * dvz;
+                s->px[id] = s->px[id] + k * t;
+                s->pz[id] = 0.0f;
+            } else {
+                s->px[id] = s->damp2a[ix] * s->px[id] + (s->kxa[ix] * k) * dvx;
+                s->pz[id] = s->damp1a[iz] * s->pz[id] + (s->kza[iz] * k) * dvz;
+            }
         }
     }
     if (inject) s->px[isrc] = s->px[isrc] + src_add;

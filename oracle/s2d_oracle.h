@@ -12,7 +12,9 @@
  *                                    src/src_cpu/cpu_modelling_kernels.cpp);
  *   orc_forward(..., ORC_F32, ...)  the same steps with FP32 wavefields and
  *                                   FP32 per-cell coefficients, the arithmetic
- *                                   the CUDA kernels use.
+ *                                   the CUDA kernels use (cells where both
+ *                                   pressure dampings are 1 carry p = px + pz
+ *                                   in px alone).
  */
 #ifndef S2D_ORACLE_H
 #define S2D_ORACLE_H

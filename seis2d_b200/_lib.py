@@ -67,7 +67,7 @@ class Stats(C.Structure):
     _fields_ = [("loop_ms", C.c_double), ("cell_updates", C.c_double), ("gcells_per_s", C.c_double),
                 ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int),
                 ("variant", C.c_int), ("block", C.c_int), ("stages", C.c_int), ("seg_len", C.c_int),
-                ("autotuned", C.c_int)]
+                ("autotuned", C.c_int), ("alg_bytes", C.c_double)]
 
 
 # Every symbol include/seis2d.h declares, with its ctypes signature.

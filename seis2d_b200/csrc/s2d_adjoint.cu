@@ -83,6 +83,11 @@ __device__ __forceinline__ float4 gzt(const Lane<FAST> &ln, const float4 &m, flo
 // terms are formed at Q = L-1, the x-velocity adjoint at W = L-3 (its G^T
 // x-gather needs Kx kappa mPX at W-1 .. W+2).
 //
+// Cells where both pressure dampings are 1 run the forward with p alone
+// (p' = p + kappa (Kx a + Kz c)); their adjoint carries one pressure field
+// (mpx, mpz unused) and the forward saved Kx a + Kz c in the first product
+// slot.
+//
 // Imaging per step: dJ/dkappa += Kx a mPX + Kz c mPZ at Q.  The buoyancy
 // terms tbx = Lx g mvx', tbz = Lz h mvz' enter dJ/db through the averages
 // bx = (b[x] + b[x+1]) / 2, bz = (b[z] + b[z+1]) / 2 (cpu_modelling_kernels.cpp:89-119):
@@ -146,12 +151,16 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const bool in_seg = Q >= xa && Q < xb;
         const bool upd = in_seg && ln.owner;       // this lane writes column Q
         const bool img = Q >= 0 && Q < xb;         // buoyancy terms at Q (xa-1 feeds column xa)
-        const float4 mpx = ld4(mpxi + colQ), mpz = ld4(mpzi + colQ), mvz = ld4(mvzi + colQ);
+        const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
+        const bool colm = xq.x == 1.0f;
+        const bool pz_live = !(FAST && colm);  // some cell of the column keeps mpz
+        const float4 mpx = ld4(mpxi + colQ), mvz = ld4(mvzi + colQ);
+        const float4 mpz = pz_live ? ld4(mpzi + colQ) : zero;
         const float4 bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
         float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tb = zero;
         if (upd) {
             pa = ld4(pr + colQ);
-            pc = ld4(pr + F + colQ);
+            if (pz_live) pc = ld4(pr + F + colQ);
             tk = ldrw(gk + colQ);
             tb = ldrw(gb + colQ);
         }
@@ -159,8 +168,10 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             pg = ld4(pr + 2 * F + colQ);
             ph = ld4(pr + 3 * F + colQ);
         }
-        const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
         const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
+        // merged cells (both pressure dampings 1) carry one pressure adjoint
+        const bool m0 = colm && (FAST || r0.x == 1.0f), m1 = colm && (FAST || r1.x == 1.0f);
+        const bool m2 = colm && (FAST || r2.x == 1.0f), m3 = colm && (FAST || r3.x == 1.0f);
         // ---- pressure adjoint at Q ----
         const float4 h = make_float4((r0.w * bz.x) * mvz.x, (r1.w * bz.y) * mvz.y, (r2.w * bz.z) * mvz.z,
                                      (r3.w * bz.w) * mvz.w);
@@ -191,14 +202,18 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             }
         }
         const float4 mPX = make_float4(mpx.x + q.x, mpx.y + q.y, mpx.z + q.z, mpx.w + q.w);
-        const float4 mPZ = make_float4(mpz.x + q.x, mpz.y + q.y, mpz.z + q.z, mpz.w + q.w);
+        const float4 mPZ = make_float4(m0 ? mPX.x : mpz.x + q.x, m1 ? mPX.y : mpz.y + q.y,
+                                       m2 ? mPX.z : mpz.z + q.z, m3 ? mPX.w : mpz.w + q.w);
         if (upd) {
             st4(mpxo + colQ, make_float4(xq.x * mPX.x, xq.x * mPX.y, xq.x * mPX.z, xq.x * mPX.w));
-            st4(mpzo + colQ, make_float4(r0.x * mPZ.x, r1.x * mPZ.y, r2.x * mPZ.z, r3.x * mPZ.w));
-            tk.x += (xq.y * pa.x) * mPX.x + (r0.y * pc.x) * mPZ.x;
-            tk.y += (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
-            tk.z += (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
-            tk.w += (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
+            if (pz_live)
+                st4(mpzo + colQ, make_float4(m0 ? 0.0f : r0.x * mPZ.x, m1 ? 0.0f : r1.x * mPZ.y,
+                                             m2 ? 0.0f : r2.x * mPZ.z, m3 ? 0.0f : r3.x * mPZ.w));
+            // merged cells saved Kx a + Kz c in the first product slot
+            tk.x += m0 ? pa.x * mPX.x : (xq.y * pa.x) * mPX.x + (r0.y * pc.x) * mPZ.x;
+            tk.y += m1 ? pa.y * mPX.y : (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
+            tk.z += m2 ? pa.z * mPX.z : (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
+            tk.w += m3 ? pa.w * mPX.w : (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
             st4(gk + colQ, tk);
             if (Q == S.src_x && ln.sdz >= 0 && ln.sdz < 4) S.srcadj[kt] = comp(mPX, ln.sdz);
         }

@@ -55,6 +55,15 @@ struct Model {
     DevBuf vp, rho;          // raw [nx][nz] copies (source amplitude needs vp, rho at the source)
     DevBuf kappa, bx, bz;    // padded layout
     std::vector<float> damp2a, damp2a1, damp2b, damp2b1, damp1a, damp1a1, damp1b, damp1b1;
+    // Algorithmic DRAM bytes of one FD step of one shot: 44 B per cell, 36 B
+    // where both pressure dampings are 1 (the cell carries p alone).
+    double step_bytes() const {
+        long cx = 0, cz = 0;
+        for (int x = 0; x < nnx; ++x) cx += damp2a[x] == 1.0f;
+        for (int z = 0; z < nnz; ++z) cz += damp1a[z] == 1.0f;
+        const double merged = (double)cx * (double)cz, all = (double)nnx * (double)nnz;
+        return 36.0 * merged + 44.0 * (all - merged);
+    }
     // coefficient tables for one fd_dt, rebuilt when fd_dt changes
     float coef_dt = -1.0f;
     DevBuf xcoef, zcoef;
@@ -995,13 +1004,15 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         CK(cudaEventSynchronize(c->ev1));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-        double cells = 0;
+        double cells = 0, bytes = 0;
         for (int s = 0; s < nshots; ++s) {
             const Model &m = *c->models[b.shots[s].model_id];
             cells += (double)m.nnx * m.nnz;
+            bytes += m.step_bytes();
         }
         stats->loop_ms = ms;
         stats->cell_updates = cells * nsteps;
+        stats->alg_bytes = bytes * nsteps;
         stats->gcells_per_s = ms > 0 ? stats->cell_updates / (ms * 1e6) : 0.0;
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;

@@ -28,7 +28,9 @@
 //
 // Traffic per cell-update: px, pz, vx, vz read once and written once
 // (32 B) and kappa, bx, bz read once (12 B, shared through L2 by the shots
-// of a batch that use the same model).
+// of a batch that use the same model).  Where both pressure dampings are 1
+// (the model's interior) the cell carries p = px + pz alone and pz is neither
+// read nor written: 36 B.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -50,15 +52,38 @@ __device__ __forceinline__ float upd(float a, float x, float b, float k, float d
     return __fmaf_rn(a, x, __fmul_rn(__fmul_rn(b, k), d));
 }
 
+// One cell of the pressure update.  Split (the reference's form): px and pz
+// damped separately.  Merged (both pressure dampings exactly 1): px and pz
+// only enter through p = px + pz, so the cell carries p in px (pz stays 0):
+//   p' = p + kappa (Kx Dx vx + Kz Dz vz).
+// The product saved for the gradient is Dx vx (split) or Kx Dx vx + Kz Dz vz
+// (merged) in the first slot, Dz vz (split) or 0 in the second.
+__device__ __forceinline__ void p_cell(bool merged, float dax, float kx, float daz, float kz, float px, float pz,
+                                       float k, float dx, float dz, float &pxn, float &pzn, float &t0, float &t1) {
+    if (merged) {
+        const float t = dif(kx, dx, kz, dz);
+        pxn = __fmaf_rn(k, t, px);
+        pzn = 0.0f;
+        t0 = t;
+        t1 = 0.0f;
+    } else {
+        pxn = upd(dax, px, kx, k, dx);
+        pzn = upd(daz, pz, kz, k, dz);
+        t0 = dx;
+        t1 = dz;
+    }
+}
+
 // Pressure at column P from vx at P-2..P+1 (q0..q3), old px, pz, kappa and vz
 // at P (cpu_modelling_kernels.cpp:201-258 and 335-351, cpumodelling.cpp:136-142).
-// Returns new p; new px, pz in pxn, pzn; D-x vx and D-z vz in dxv, dzv.
+// xc = (Dax, Kx, Dbx, Lx) of column P; colm: Dax == 1 (FAST tasks then have
+// every cell merged and pz is not read).  Returns new p; new px, pz in pxn,
+// pzn; the step's products in dxv, dzv.
 template <bool FAST>
-__device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &q0,
-                                           const float4 &q1, const float4 &q2, const float4 &q3, const float4 &px,
-                                           const float4 &pz, const float4 &kk, const float4 &vz, float4 &pxn,
-                                           float4 &pzn, float4 &dxv, float4 &dzv) {
-    const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
+__device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &xc,
+                                           bool colm, const float4 &q0, const float4 &q1, const float4 &q2,
+                                           const float4 &q3, const float4 &px, const float4 &pz, const float4 &kk,
+                                           const float4 &vz, float4 &pxn, float4 &pzn, float4 &dxv, float4 &dzv) {
     float cx0, cx1;
     dm_coef(P, S.nnx, cx0, cx1);
     const float up_z = __shfl_up_sync(kFull, vz.z, 1);
@@ -77,26 +102,23 @@ __device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &
     const float dx1 = dif(cx0, q2.y - q1.y, cx1, q3.y - q0.y);
     const float dx2 = dif(cx0, q2.z - q1.z, cx1, q3.z - q0.z);
     const float dx3 = dif(cx0, q2.w - q1.w, cx1, q3.w - q0.w);
-    dxv = make_float4(dx0, dx1, dx2, dx3);
-    dzv = make_float4(dz0, dz1, dz2, dz3);
-    pxn.x = upd(xc.x, px.x, xc.y, kk.x, dx0);
-    pxn.y = upd(xc.x, px.y, xc.y, kk.y, dx1);
-    pxn.z = upd(xc.x, px.z, xc.y, kk.z, dx2);
-    pxn.w = upd(xc.x, px.w, xc.y, kk.w, dx3);
-    float4 r = zrow(ln, 0);
-    pzn.x = upd(r.x, pz.x, r.y, kk.x, dz0);
-    r = zrow(ln, 1);
-    pzn.y = upd(r.x, pz.y, r.y, kk.y, dz1);
-    r = zrow(ln, 2);
-    pzn.z = upd(r.x, pz.z, r.y, kk.z, dz2);
-    r = zrow(ln, 3);
-    pzn.w = upd(r.x, pz.w, r.y, kk.w, dz3);
+    // z-damping of the lane's rows (FAST: 1, the cell is merged iff colm)
+    const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
+    p_cell(colm && (FAST || r0.x == 1.0f), xc.x, xc.y, r0.x, r0.y, px.x, pz.x, kk.x, dx0, dz0, pxn.x, pzn.x, dxv.x,
+           dzv.x);
+    p_cell(colm && (FAST || r1.x == 1.0f), xc.x, xc.y, r1.x, r1.y, px.y, pz.y, kk.y, dx1, dz1, pxn.y, pzn.y, dxv.y,
+           dzv.y);
+    p_cell(colm && (FAST || r2.x == 1.0f), xc.x, xc.y, r2.x, r2.y, px.z, pz.z, kk.z, dx2, dz2, pxn.z, pzn.z, dxv.z,
+           dzv.z);
+    p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, dxv.w,
+           dzv.w);
     if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
         if (ln.sdz == 0) pxn.x += ln.amp;
         else if (ln.sdz == 1) pxn.y += ln.amp;
         else if (ln.sdz == 2) pxn.z += ln.amp;
         else pxn.w += ln.amp;
     }
+    // merged cells: pzn = 0 and p = px exactly
     return make_float4(pxn.x + pzn.x, pxn.y + pzn.y, pxn.z + pzn.z, pxn.w + pzn.w);
 }
 
@@ -194,16 +216,19 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
         vq0 = vq1; vq1 = vq2; vq2 = vq3;
         vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
         const float4 vz = ld4(vzi + colP);
+        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = xc.x == 1.0f;
+        const bool pz_live = !(FAST && colm);  // some cell of the column keeps pz
         float4 pxn, pzn, dxv, dzv;
-        const float4 pn = p_update(ln, S, P, vq0, vq1, vq2, vq3, ld4(pxi + colP), ld4(pzi + colP),
-                                   ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
+        const float4 pn = p_update(ln, S, P, xc, colm, vq0, vq1, vq2, vq3, ld4(pxi + colP),
+                                   pz_live ? ld4(pzi + colP) : zero, ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
         const bool in_seg = P >= xa && P < xb;
         if (in_seg && ln.owner) {
             st4(pxo + colP, pxn);
-            st4(pzo + colP, pzn);
+            if (pz_live) st4(pzo + colP, pzn);
             if (PROD) {
                 st4(pr + colP, dxv);
-                st4(pr + F + colP, dzv);
+                if (pz_live) st4(pr + F + colP, dzv);
             }
         }
         if (rec && in_seg) record(ln, S, P, pn, slot);
@@ -322,13 +347,15 @@ __device__ __forceinline__ bool bulk_task(const StepArgs &a, const ShotDev &Sh, 
         unsigned char *st = ring + (size_t)s * kStageBytes;
         const int L = xa - 3 + j;
         const bool pp = L >= xa, vv = L >= xa + 3;
-        mbar_expect_tx(&bars[s], (unsigned)kSlotBytes * (1u + (pp ? 4u : 0u) + (vv ? 2u : 0u)));
+        // pz of column L-1 is not needed where every cell is merged
+        const bool pz = pp && !(FAST && __ldg(Sh.xcoef + (L - 1 + S2D_GX)).x == 1.0f);
+        mbar_expect_tx(&bars[s], (unsigned)kSlotBytes * (1u + (pp ? 3u : 0u) + (pz ? 1u : 0u) + (vv ? 2u : 0u)));
         if (j == a.fault_iter) return;  // test knob: the stage's bytes never arrive
         bulk_copy(st, src_vx + (ptrdiff_t)L * (ptrdiff_t)ld, kSlotBytes, &bars[s]);
         if (pp) {
             const ptrdiff_t cp = (ptrdiff_t)(L - 1) * (ptrdiff_t)ld;
             bulk_copy(st + 1 * kSlotBytes, src_px + cp, kSlotBytes, &bars[s]);
-            bulk_copy(st + 2 * kSlotBytes, src_pz + cp, kSlotBytes, &bars[s]);
+            if (pz) bulk_copy(st + 2 * kSlotBytes, src_pz + cp, kSlotBytes, &bars[s]);
             bulk_copy(st + 3 * kSlotBytes, src_k + cp, kSlotBytes, &bars[s]);
             bulk_copy(st + 4 * kSlotBytes, src_vz + cp, kSlotBytes, &bars[s]);
         }
@@ -370,14 +397,17 @@ __device__ __forceinline__ bool bulk_task(const StepArgs &a, const ShotDev &Sh, 
         if (L >= xa) {
             const int P = L - 1;
             const float4 vz = st[4 * 32];
+            const float4 xc = __ldg(Sh.xcoef + (P + S2D_GX));
+            const bool colm = xc.x == 1.0f;
+            const bool pz_live = !(FAST && colm);
             float4 pxn, pzn, dxv, dzv;
-            const float4 pn = p_update(ln, Sh, P, vq0, vq1, vq2, vq3, st[1 * 32], st[2 * 32], st[3 * 32], vz, pxn,
-                                       pzn, dxv, dzv);
+            const float4 pn = p_update(ln, Sh, P, xc, colm, vq0, vq1, vq2, vq3, st[1 * 32],
+                                       pz_live ? st[2 * 32] : zero, st[3 * 32], vz, pxn, pzn, dxv, dzv);
             const bool in_seg = P >= xa && P < xb;
             const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
             if (in_seg && ln.owner) {
                 st4(pxo + colP, pxn);
-                st4(pzo + colP, pzn);
+                if (pz_live) st4(pzo + colP, pzn);
             }
             if (rec && in_seg) record(ln, Sh, P, pn, slot);
             pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
