@@ -307,6 +307,29 @@ S2D_API int s2d_check_stability(const s2d_jobcard *job, float vmin, float vmax, 
 S2D_API int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming,
                             int check_stability, int verbose, char *errbuf, size_t errlen);
 
+/*
+ * Shots of rank `rank` of `nranks`: the contiguous block [*start, *start +
+ * *count) of nsrc, the first nsrc % nranks ranks one shot longer, as
+ * calculate_workload assigns them (workload.cpp:12-62).  S2D_ERR_ARG when
+ * nsrc < nranks (the reference aborts with -8) or the rank is out of range.
+ * Host only.
+ */
+S2D_API int s2d_workload(int nsrc, int nranks, int rank, int *start, int *count);
+
+/*
+ * s2d_run_jobcard for one rank of a multi-process job (one process per GPU,
+ * replacing the MPI master/worker split of modelling_master.cpp /
+ * modelling_worker.cpp and the per-device OpenMP team of
+ * gpumodelling_multi.cu:292-420): models the rank's block of shots
+ * (s2d_workload) and keeps the restart index of the block, counted from its
+ * first shot, in <outdir>/<jobname>checkpoint_rank<rank>.txt as the reference
+ * does (cpumodelling.cpp:294-321).  Output files are named by the shot's
+ * place in the whole geometry.  s2d_run_jobcard is rank 0 of 1.
+ */
+S2D_API int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, int naming,
+                                 int check_stability, int verbose, int rank, int nranks,
+                                 char *errbuf, size_t errlen);
+
 /* ---- forward modelling without device allocation ----------------------------- */
 
 /* Size of the device scratch s2d_forward_static works in (32 MiB). */

@@ -92,6 +92,9 @@ SIGNATURES = {
     "s2d_check_stability": ([C.POINTER(JobCard), C.c_float, C.c_float, C.c_char_p, C.c_size_t], C.c_int),
     "s2d_run_jobcard": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t],
                         C.c_int),
+    "s2d_workload": ([C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "s2d_run_jobcard_rank": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                              C.c_char_p, C.c_size_t], C.c_int),
     "s2d_forward_static": ([C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p,
                             C.POINTER(Wave), C.POINTER(Shot), C.c_void_p, C.c_uint, C.c_void_p, C.c_char_p,
                             C.c_size_t], C.c_int),

@@ -440,8 +440,24 @@ int s2d_check_stability(const s2d_jobcard *J, float vmin, float vmax, char *eb, 
     return S2D_OK;
 }
 
+int s2d_workload(int nsrc, int nranks, int rank, int *start, int *count) {
+    if (!start || !count || nranks < 1 || rank < 0 || rank >= nranks || nsrc < 0) return S2D_ERR_ARG;
+    // workload.cpp:21-31: fewer sources than ranks is an error (abort -8 there)
+    if (nsrc < nranks) return S2D_ERR_ARG;
+    // workload.cpp:34-48: contiguous blocks, the first nsrc % nranks one longer
+    const int div = nsrc / nranks, mod = nsrc % nranks;
+    *start = rank * div + std::min(rank, mod);
+    *count = div + (rank < mod ? 1 : 0);
+    return S2D_OK;
+}
+
 int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, int check_stability, int verbose,
                     char *eb, size_t el) {
+    return s2d_run_jobcard_rank(jobcard_path, device, nb, naming, check_stability, verbose, 0, 1, eb, el);
+}
+
+int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, int naming, int check_stability, int verbose,
+                         int rank, int nranks, char *eb, size_t el) {
     s2d_jobcard J;
     int e = s2d_jobcard_read(jobcard_path, &J, eb, el);
     if (e) return e;
@@ -471,9 +487,20 @@ int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, in
             return e;
         }
     }
-    // restart index (cpumodelling.cpp:294-321); this driver also writes it
-    // after every completed shot, which the reference never does
-    const std::string ckpt = std::string(J.tmppath) + J.jobname + "checkpoint_rank0.txt";
+    // this rank's block of shots (workload.cpp:12-62)
+    int first = 0, nmine = 0;
+    if (s2d_workload(G.nsrc, nranks, rank, &first, &nmine) != S2D_OK) {
+        s2d_geometry_free(&G);
+        if (nranks >= 1 && rank >= 0 && rank < nranks && G.nsrc < nranks)
+            return say(eb, el, S2D_ERR_ARG,
+                       "number of sources (%d) should be greater than or equal to the number of ranks (%d) "
+                       "(reference code -8)", G.nsrc, nranks);
+        return say(eb, el, S2D_ERR_ARG, "bad rank %d of %d", rank, nranks);
+    }
+    // restart index (cpumodelling.cpp:294-321): per rank, an index into the
+    // rank's own shots; this driver also writes it after every completed
+    // shot, which the reference never does
+    const std::string ckpt = std::string(J.tmppath) + J.jobname + "checkpoint_rank" + std::to_string(rank) + ".txt";
     int istart = 0;
     if (std::strcmp(J.jbtype, "Restart") == 0) {
         FILE *f = std::fopen(ckpt.c_str(), "r");
@@ -483,7 +510,7 @@ int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, in
         }
         if (std::fscanf(f, "%d", &istart) != 1) istart = 0;
         std::fclose(f);
-        istart = std::max(0, std::min(istart, G.nsrc));
+        istart = std::max(0, std::min(istart, nmine));
     }
     void *ctx = nullptr;
     e = s2d_create(&ctx, device);
@@ -501,16 +528,17 @@ int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, in
     const int nnx = J.nx + 2 * nb, nnz = J.nz + 2 * nb;
     const double per_shot = 8.0 * (nnx + 16.0) * (nnz + 136.0) * 4.0 * 1.05;
     int batch = (int)std::max(1.0, std::floor(0.85 * (double)free_b / per_shot));
-    for (int s0 = istart; !e && s0 < G.nsrc; s0 += batch) {
-        const int n = std::min(batch, G.nsrc - s0);
+    for (int s0 = istart; !e && s0 < nmine; s0 += batch) {
+        const int n = std::min(batch, nmine - s0);
         std::vector<s2d_shot> shots(n);
         size_t total = 0;
         for (int k = 0; k < n; ++k) {
+            const int g = first + s0 + k;
             shots[k].model_id = mid;
-            shots[k].src = G.src[s0 + k];
-            shots[k].nrec = G.nrec[s0 + k];
-            shots[k].rec = G.rec[s0 + k];
-            total += (size_t)G.nrec[s0 + k] * st.real_nt;
+            shots[k].src = G.src[g];
+            shots[k].nrec = G.nrec[g];
+            shots[k].rec = G.rec[g];
+            total += (size_t)G.nrec[g] * st.real_nt;
         }
         std::vector<float> seis(total);
         e = s2d_forward(ctx, shots.data(), n, &J.wave, nullptr, 0, 0, 0, seis.data(), 0, nullptr);
@@ -520,7 +548,7 @@ int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, in
         }
         size_t off = 0;
         for (int k = 0; k < n && !e; ++k) {
-            const int s = s0 + k;
+            const int s = first + s0 + k;  // index in the whole geometry
             std::string name = std::string(J.tmppath) + J.jobname;
             if (naming == 1) {
                 // gpumodelling.cu:471-477: "sx%.2f" of the source's grid x in metres
@@ -542,10 +570,10 @@ int s2d_run_jobcard(const char *jobcard_path, int device, int nb, int naming, in
             off += cnt;
             FILE *c = std::fopen(ckpt.c_str(), "w");
             if (c) {
-                std::fprintf(c, "%d\n", s + 1);
+                std::fprintf(c, "%d\n", s0 + k + 1);
                 std::fclose(c);
             }
-            if (verbose) std::printf(" Shot remaining: %d\n", G.nsrc - (s + 1));
+            if (verbose) std::printf(" Rank: %d   Shot remaining: %d\n", rank, nmine - (s0 + k + 1));
         }
     }
     s2d_destroy(ctx);

@@ -56,9 +56,12 @@ def check_stability(card: L.JobCard, vmin: float, vmax: float) -> None:
 
 
 def run_jobcard(path: str, device: int = 0, nb: int = 32, naming: str = "cpu", check_stability: bool = True,
-                verbose: bool = False) -> None:
+                verbose: bool = False, rank: int = 0, nranks: int = 1) -> None:
+    """The whole job (rank 0 of 1), or rank ``rank``'s block of shots of an
+    ``nranks``-process job (see seis2d_b200.sharding.run_jobcard_distributed)."""
     eb = _err()
-    rc = L.lib().s2d_run_jobcard(path.encode(), int(device), int(nb), 1 if naming == "gpu" else 0,
-                                 1 if check_stability else 0, 1 if verbose else 0, eb, 1024)
+    rc = L.lib().s2d_run_jobcard_rank(path.encode(), int(device), int(nb), 1 if naming == "gpu" else 0,
+                                      1 if check_stability else 0, 1 if verbose else 0, int(rank), int(nranks),
+                                      eb, 1024)
     if rc:
         raise L.Seis2dError(rc, eb.value.decode())

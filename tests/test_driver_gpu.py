@@ -74,3 +74,33 @@ def test_command_line_driver(tmp_path):
     (tmp_path / "case.json").write_text(str(z["jobcard"]).replace('"0.001"', '"0.004"', 1))
     r = subprocess.run([exe, "--quiet", "case.json"], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "reference code -" in r.stderr
+
+
+def test_ranks_of_a_job_write_the_whole_jobs_files(tmp_path, monkeypatch):
+    """The ranks of a 2-rank job (run one after the other on one GPU; they
+    never wait on each other) together write the files of the 1-rank job,
+    each rank keeping its own restart index of its block."""
+    monkeypatch.chdir(tmp_path)
+    z, c = _stage(tmp_path, "twolayer_split_nb32")
+    shots = [(200.0 + 150.0 * k, 20.0, 31, 0, 10.0, 1) for k in range(5)]
+    F.write_shotfile("geom.txt", shots)
+    D.run_jobcard("case.json", nb=c["nb"], naming="gpu")
+    whole = {n: open("out/" + n, "rb").read() for n in os.listdir("out") if n.endswith(".bin")}
+    assert len(whole) == 5
+    for n in os.listdir("out"):
+        os.remove("out/" + n)
+    for rank in (0, 1):
+        D.run_jobcard("case.json", nb=c["nb"], naming="gpu", rank=rank, nranks=2)
+    got = {n: open("out/" + n, "rb").read() for n in os.listdir("out") if n.endswith(".bin")}
+    assert got == whole
+    assert open("out/case_checkpoint_rank0.txt").read().strip() == "3"
+    assert open("out/case_checkpoint_rank1.txt").read().strip() == "2"
+    # restart of rank 1 after its first shot: only the last shot runs again
+    os.remove("out/case_sx800.00_seismogram.bin")
+    os.remove("out/case_sx500.00_seismogram.bin")
+    open("out/case_checkpoint_rank1.txt", "w").write("1\n")
+    (tmp_path / "case.json").write_text(str(z["jobcard"]).replace('"New"', '"Restart"'))
+    D.run_jobcard("case.json", nb=c["nb"], naming="gpu", rank=1, nranks=2)
+    assert os.path.exists("out/case_sx800.00_seismogram.bin")
+    assert not os.path.exists("out/case_sx500.00_seismogram.bin")
+    assert open("out/case_sx800.00_seismogram.bin", "rb").read() == whole["case_sx800.00_seismogram.bin"]

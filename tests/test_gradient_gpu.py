@@ -191,3 +191,33 @@ def test_torch_autograd(ctx):
     g = ctx.gradient([Shot(m, src, rec)], wave, dobs.detach().cpu().numpy(), misfit=True)
     assert O.rel_l2(vp_t.grad.cpu().numpy(), g.grad_vp) <= 1e-6
     assert O.rel_l2(rho_t.grad.cpu().numpy(), g.grad_rho) <= 1e-6
+
+
+def test_gradient_allreduce_through_nccl(ctx):
+    """seis2d_b200.sharding.gradient_allreduce on a one-rank NCCL group: the
+    device images and the misfit go through the all-reduce unchanged."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    from seis2d_b200 import Shot
+    from seis2d_b200.sharding import gradient_allreduce
+    vp, rho = _model(31)
+    m = ctx.model(vp, rho, D, D, NB)
+    shots = [Shot(m, *_geom(sx)) for sx in (200.0, 330.0, 460.0)]
+    d = torch.cat([torch.from_numpy(ctx.forward([s], _wave())[0].ravel()) for s in shots]).cuda() * 0.7
+    ref = ctx.gradient(shots, _wave(), d, misfit=True)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        gv, gr, mis = gradient_allreduce(ctx, shots, _wave(), d)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    np.testing.assert_allclose(gv.cpu().numpy(), ref.grad_vp, rtol=0, atol=0)
+    np.testing.assert_allclose(gr.cpu().numpy(), ref.grad_rho, rtol=0, atol=0)
+    assert abs(mis - ref.misfit) <= 1e-9 * ref.misfit
