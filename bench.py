@@ -425,6 +425,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the c1/c3/c4/c5 legs")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="force a step-kernel variant (s2d_set_option 'variant'); default: autotuned")
     ap.add_argument("--leg", default="main", choices=["main", "gradient"],
                     help="gradient: only the FWI gradient leg (--shots shots, --grad-time seconds)")
     ap.add_argument("--grad-time", type=float, default=3.0, help="record length of the gradient leg (s)")
@@ -473,6 +475,8 @@ def main():
     cells_step = cells_shot * nshots  # per FD step, this rank
 
     ctx = Context(local)
+    if args.variant >= 0:
+        ctx.set_option("variant", args.variant)
     m = ctx.model(vp, rho, w["d"], w["d"], w["nb"])
     shots = [Shot(m, s, rec) for s in src]
     nrec_tot = nshots * rec.shape[0]
@@ -519,14 +523,19 @@ def main():
     if n_r > 0:
         ctx.forward(shots, wave, kt_begin=kt_r, kt_count=n_r, out=seis_dev)
         st = ctx.last_stats
-        per_launch_s = st.loop_ms * 1e-3 / n_r
-        bytes_launch = st.alg_bytes / n_r
+        # one launch per FD step (two for the two-step variant, whose
+        # algorithmic bytes the library counts per pass)
+        spl = 2 if st.variant == 5 else 1
+        n_launch = max(1, n_r // spl)
+        per_launch_s = st.loop_ms * 1e-3 / n_launch
+        bytes_launch = st.alg_bytes / n_launch
         peak, peak_kind = measured_peak()
-        achieved = bytes_launch / per_launch_s / 1e9
+        achieved = st.alg_bytes / (st.loop_ms * 1e-3) / 1e9
         tr = traffic_per_launch(args.workload)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": tr, "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
-                "bytes_per_cell_update": bytes_launch / cells_step, "launch_ms": per_launch_s * 1e3}
+                "bytes_per_cell_update": st.alg_bytes / st.cell_updates, "launch_ms": per_launch_s * 1e3,
+                "fd_steps_per_launch": spl}
 
     # ---- plain: the same shots one after another ----
     plain = None

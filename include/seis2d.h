@@ -113,8 +113,10 @@ typedef struct {
     int seg_len;             /* columns per warp task (first model group)     */
     int autotuned;           /* 1 if this call ran the autotuner's trials     */
     double alg_bytes;        /* s2d_forward: algorithmic DRAM bytes of the loop:
-                                44 B per cell-update, 36 B where both pressure
-                                dampings are 1 (the cell carries p alone)     */
+                                44 B per cell and pass over the state, 36 B
+                                where both pressure dampings are 1 (the cell
+                                carries p alone); a pass is one FD step, or
+                                two with the two-step variant                 */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */
@@ -144,7 +146,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 Setting any of those three turns autotuning off.
  *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline
  *                 compiled for 128 registers (default), 4 plain loads compiled
- *                 for 128 registers
+ *                 for 128 registers, 5 two FD steps per launch (the state
+ *                 crosses HBM once per two steps; odd step counts end with one
+ *                 one-step launch); s2d_gradient always runs one step per launch
  *   "block"       threads per block: 32, 64, 96 or 128 (default 128)
  *   "task_order"  0: consecutive warps take the shots of one tile;
  *                 1: consecutive warps take adjacent strips of one shot (default)

@@ -85,6 +85,8 @@ struct Batch {
     std::vector<ShotDev> shot_dev;   // host mirror
     std::vector<GroupDev> groups;    // batched mode
     std::vector<int> group_nnx;      // padded columns of each group's model
+    std::vector<int> group_nnz;      // padded rows of each group's model
+    int cur = 0;                     // state buffer (parity) holding step kt_next
     std::vector<long> layout;        // launch configuration the groups are laid out for
     std::vector<std::unique_ptr<DevBuf>> state;   // 8 per shot
     std::vector<std::unique_ptr<DevBuf>> aux;     // amp tables, receiver tables
@@ -200,20 +202,20 @@ int fail(Ctx *c, int code, const char *fmt, ...) {
                         "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
     } while (0)
 
-// Columns per x-segment for a group.  Each task streams L + 6 columns (3 of
-// warm-up, 3 of halo); warps loop over tasks, so a launch takes about
+// Columns per x-segment for a group.  Each task streams L + halo columns (6
+// for one step per launch, 12 for two); warps loop over tasks, so a launch takes about
 // ceil(tasks / resident warps) rounds of the longest task.  Pick the L with
 // the fewest round-columns (longer segments on ties).
-int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps) {
-    static const int cand[] = {1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16};
-    int best = 16;
+int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps, int halo) {
+    static const int cand[] = {1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16, 12, 8};
+    int best = 8;
     double best_cost = 1e300;
     for (int L : cand) {
         const int Lc = std::min(L, nnx);
         const long nsegs = (nnx + Lc - 1) / Lc;
         const long tasks = tasks_per_seg * nsegs;
         const long rounds = (tasks + resident_warps - 1) / std::max(1L, resident_warps);
-        const double cost = (double)rounds * (Lc + 6);
+        const double cost = (double)rounds * (Lc + halo);
         if (cost < best_cost * 0.999) {
             best_cost = cost;
             best = Lc;
@@ -253,11 +255,12 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
     lc.block = std::max(32, std::min(128, block / 32 * 32));
     lc.stages = std::max(2, std::min(16, stages));
     const bool ldg = lc.variant == kVariantLdg || lc.variant == kVariantLdgProducts || lc.variant == kVariantLdg128;
-    if (ldg) {
+    const bool ts = ts_layout(lc.variant);
+    if (ldg || ts) {
         lc.block = 128;
         lc.stages = 0;
     }
-    lc.smem = ldg ? 0 : bulk_smem_bytes(lc.block / 32, lc.stages);
+    lc.smem = ldg ? 0 : ts ? (size_t)(lc.block / 32) * kTsWarpBytes : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
     if (e) return fail(c, S2D_ERR_ARG, "step kernel does not accept %zu B of shared memory: %s", lc.smem,
                        cudaGetErrorString((cudaError_t)e));
@@ -279,7 +282,7 @@ std::vector<long> tune_key(const Ctx *c, const Batch &b) {
     std::vector<long> k = {b.plain ? 1L : 0L, (long)c->sm_count};
     for (size_t g = 0; g < b.groups.size(); ++g) {
         k.push_back(b.group_nnx[g]);
-        k.push_back(b.groups[g].nstrips);
+        k.push_back(b.group_nnz[g]);
         k.push_back(b.groups[g].nshots);
     }
     return k;
@@ -303,8 +306,10 @@ int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
 // Segment lengths, segment counts and task ranges of the batch's groups for
 // `resident_warps` warps looping over the tasks of a launch; uploaded when
 // `key` differs from the layout in place.
-int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<long> &key) {
+int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<long> &key, bool ts = false) {
     if (b.layout == key) return S2D_OK;
+    for (size_t gi = 0; gi < b.groups.size(); ++gi)
+        b.groups[gi].nstrips = ts ? num_strips_ts(b.group_nnz[gi]) : num_strips(b.group_nnz[gi]);
     long per_seg_total = 0;
     for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
     long max_tasks = 0;
@@ -315,7 +320,7 @@ int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<l
         // plain mode: every shot is a group of its own and runs alone
         const long tasks_per_seg = b.plain ? (long)g.nstrips : per_seg_total;
         g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, nnx)
-                                       : choose_seg_len(nnx, tasks_per_seg, resident_warps);
+                                       : choose_seg_len(nnx, tasks_per_seg, resident_warps, ts ? 12 : 6);
         g.nsegs = (nnx + g.seg_len - 1) / g.seg_len;
         if (b.plain) {
             g.task_begin = 0;
@@ -338,13 +343,15 @@ int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<l
 
 // The layout for the resident warps of launch configuration `lc`.
 int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
-    const std::vector<long> key = {lc.variant, lc.block, lc.stages, c->opt_seg_len};
+    // the two-step kernel and its one-step companion share one layout
+    const int v = lc.variant == kVariantTs1 ? kVariantTs2 : lc.variant;
+    const std::vector<long> key = {v, lc.block, lc.stages, c->opt_seg_len};
     if (b.layout == key) return S2D_OK;
     // resident warps of the configuration (its grid when the work is smaller)
     LaunchCfg full;
-    int e = launch_config(c, 1L << 40, &full, lc.variant, lc.block, lc.stages);
+    int e = launch_config(c, 1L << 40, &full, v, lc.block, lc.stages);
     if (e) return e;
-    return layout_groups_for(c, b, (long)full.grid * (full.block / 32), key);
+    return layout_groups_for(c, b, (long)full.grid * (full.block / 32), key, ts_layout(v));
 }
 
 // Graph of `n` step launches (kt_off = 0..n-1) for one launch configuration,
@@ -396,7 +403,10 @@ void fast_rows(const Model &m, float fd_dt, int *lo, int *hi, float *kz) {
 
 // One pass over `nsteps` FD steps starting at kt_begin, for the launch
 // arguments `args` (a whole batch, or one shot of a plain run), as replays of
-// a graph of `graph_chunk` steps.
+// a graph of `graph_chunk` launches.  The state at kt_begin is in buffer
+// b.cur; each launch reads one buffer and writes the other, and b.cur follows.
+// A two-step configuration finishes an odd count with one launch of its
+// one-step companion (same strip layout).
 int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin, int nsteps, bool use_graph,
              int *launches, bool *graph_used) {
     if (nsteps <= 0) return S2D_OK;
@@ -406,13 +416,17 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
     args.fault_iter = c->opt_fault_iter;
     args.task_order = c->opt_order;
     StepArgs *args_d = c->args_d.as<StepArgs>();
-    const int chunk = use_graph ? std::max(1, c->opt_graph_chunk) : nsteps;
-    for (int done = 0; done < nsteps; done += chunk) {
-        const int n = std::min(chunk, nsteps - done);
-        args.kt_base = kt_begin + done;
+    const int spl = steps_per_launch(lc.variant);
+    const int nl = nsteps / spl, rem = nsteps - nl * spl;
+    const int chunk = use_graph ? std::max(1, c->opt_graph_chunk) : std::max(nl, 1);
+    for (int done = 0; done < nl; done += chunk) {
+        const int n = std::min(chunk, nl - done);
+        args.kt_base = kt_begin + done * spl;
+        args.par0 = b.cur;
         int e = launch_set_args(args, args_d, c->stream);
         if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
         *launches += 1 + n;
+        b.cur ^= n & 1;
         if (!use_graph) {
             for (int k = 0; k < n; ++k) {
                 e = launch_step(lc.variant, args_d, k, lc.grid, lc.block, lc.smem, c->stream);
@@ -425,6 +439,15 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
         if (e) return e;
         CK(cudaGraphLaunch(ge, c->stream));
         *graph_used = true;
+    }
+    if (rem) {
+        args.kt_base = kt_begin + nl * spl;
+        args.par0 = b.cur;
+        int e = launch_set_args(args, args_d, c->stream);
+        if (!e) e = launch_step(kVariantTs1, args_d, 0, lc.grid, lc.block, lc.smem, c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "step launch: %s", cudaGetErrorString((cudaError_t)e));
+        *launches += 2;
+        b.cur ^= 1;
     }
     return S2D_OK;
 }
@@ -591,6 +614,7 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             g.nstrips = num_strips(m.nnz);
             b.groups.push_back(g);
             b.group_nnx.push_back(m.nnx);
+            b.group_nnz.push_back(m.nnz);
         }
     } else {
         // shots of one model must be contiguous in the shot table for shot0
@@ -606,6 +630,7 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             g.nstrips = num_strips(m.nnz);
             b.groups.push_back(g);
             b.group_nnx.push_back(m.nnx);
+            b.group_nnz.push_back(m.nnz);
             for (int s : ss) reordered.push_back(b.shot_dev[s]);
         }
         CK(cudaMemcpy(b.shots_d.p, reordered.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
@@ -642,11 +667,18 @@ int check_device_error(Ctx *c) {
 // Candidate launch configurations of the autotuner: (variant, block, stages).
 constexpr int kTuneCandidates[][3] = {
     {kVariantBulk128, 128, 3}, {kVariantBulk128, 128, 2}, {kVariantBulk128, 64, 3}, {kVariantBulk128, 64, 4},
-    {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},
+    {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
-constexpr int kTuneWarm = 1, kTuneTimed = 3;
-constexpr int kTuneSteps = kNumTuneCandidates * (kTuneWarm + kTuneTimed);
+constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
+// FD steps the trials take (a two-step candidate advances two per launch).
+constexpr int tune_steps() {
+    int n = 0;
+    for (int i = 0; i < kNumTuneCandidates; ++i)
+        n += (kTuneWarm + kTuneTimed) * (kTuneCandidates[i][0] == kVariantTs2 ? 2 : 1);
+    return n;
+}
+constexpr int kTuneSteps = tune_steps();
 
 // Sum of the task counts of a batched launch sequence.
 int batch_tasks(const Batch &b) {
@@ -656,11 +688,12 @@ int batch_tasks(const Batch &b) {
 }
 
 // Autotuner: advance the batch by kTuneSteps real FD steps from kt_begin,
-// kTuneWarm + kTuneTimed under each candidate configuration (every candidate
-// computes the same bits: they share the update arithmetic and differ only in
-// how columns reach registers and how tasks map to warps), with each timed
-// step between two events.  The candidate with the lowest median step time
-// is cached for the batch's shape and returned, its segment layout in place.
+// kTuneWarm + kTuneTimed launches under each candidate configuration (every
+// candidate computes the same bits: they share the update arithmetic and
+// differ only in how columns reach registers, how many steps a pass makes and
+// how tasks map to warps), with each timed launch between two events.  The
+// candidate with the lowest median time per FD step is cached for the batch's
+// shape and returned, its segment layout in place.
 int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best) {
     std::vector<cudaEvent_t> ev(2 * kTuneTimed * kNumTuneCandidates, nullptr);
     for (auto &e : ev) {
@@ -700,10 +733,11 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
         }
         cfg[i] = lc;
         a.total_tasks = batch_tasks(b);
-        for (int s = 0; s < kTuneWarm + kTuneTimed; ++s, ++kt) {
+        const int spl = steps_per_launch(lc.variant);
+        for (int s = 0; s < kTuneWarm + kTuneTimed; ++s, kt += spl) {
             const int t = s - kTuneWarm;
             if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t)], c->stream));
-            e = run_loop(c, b, lc, a, kt, 1, false, launches, &graph_used);
+            e = run_loop(c, b, lc, a, kt, spl, false, launches, &graph_used);
             if (e) {
                 release();
                 return e;
@@ -719,7 +753,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
         for (int s = 0; s < kTuneTimed && ce == cudaSuccess; ++s)
             ce = cudaEventElapsedTime(&t[s], ev[2 * (i * kTuneTimed + s)], ev[2 * (i * kTuneTimed + s) + 1]);
         std::sort(t, t + kTuneTimed);
-        const float med = t[kTuneTimed / 2];
+        const float med = t[kTuneTimed / 2] / (float)steps_per_launch(cfg[i].variant);  // per FD step
         if (ok[i] && (i == 0 || med < pick_ms)) {
             pick = i;
             pick_ms = med;
@@ -746,7 +780,8 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     const std::string k(key);
     // an explicit launch configuration turns the autotuner off
     if (k == "variant") {
-        if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128)
+        if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
+            value != kVariantTs2)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;
@@ -964,10 +999,13 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         tuned_now = 1;
     }
     if (b.plain) {
+        // every shot advances from the same buffer through the same launches
+        const int cur0 = b.cur;
         for (int s = 0; s < nshots; ++s) {
             a.groups = b.groups_d.as<GroupDev>() + s;
             a.ngroups = 1;
             a.total_tasks = b.groups[s].nstrips * b.groups[s].nsegs;
+            b.cur = cur0;
             int e = run_loop(c, b, lc, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
             if (e) return e;
         }
@@ -1012,7 +1050,11 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         }
         stats->loop_ms = ms;
         stats->cell_updates = cells * nsteps;
-        stats->alg_bytes = bytes * nsteps;
+        // one pass over the state per launch (two steps per pass for the
+        // two-step kernel; the autotuner's trial steps are counted as one-step)
+        const int passes = steps_per_launch(lc.variant) == 2 ? (kt_end - kt_run + 1) / 2 + (kt_run - kt_begin)
+                                                             : nsteps;
+        stats->alg_bytes = bytes * passes;
         stats->gcells_per_s = ms > 0 ? stats->cell_updates / (ms * 1e6) : 0.0;
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;
@@ -1215,6 +1257,10 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     LaunchCfg lc_fwd, lc_prod;
     {
         int e = base_config(c, b, &lc_fwd);
+        // the gradient keeps every step's state (checkpoints at kt parity):
+        // one step per launch
+        if (!e && steps_per_launch(lc_fwd.variant) != 1)
+            e = launch_config(c, b.max_tasks, &lc_fwd, kVariantLdg128, 128, 0);
         if (!e) e = layout_groups(c, b, lc_fwd);
         if (!e) e = launch_config(c, b.max_tasks, &lc_fwd, lc_fwd.variant, lc_fwd.block, lc_fwd.stages);
         if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts, 128, 0);
@@ -1255,6 +1301,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     };
     for (int j = 0; j < nseg; ++j) {
         const int k0 = j * C, n = std::min(C, rs.fd_nt - k0);
+        b.cur = k0 & 1;  // one step per launch: the state of step kt is in buffer kt & 1
         if (j < nseg - 1) {
             StepArgs a = fa;
             int e = save_ckpt(j);
@@ -1301,6 +1348,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
             StepArgs a = fa;
             a.flags = S2D_STEP_PRODUCTS | S2D_STEP_NO_RECORD;
             a.prod_kt0 = k0;
+            b.cur = k0 & 1;
             int e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
             if (e) return e;
         }

@@ -12,11 +12,12 @@
 #include <cstddef>
 #include <cstdint>
 
-#define S2D_GX 4            // ghost columns on each side
-#define S2D_GZ 4            // ghost rows above z = 0
+#define S2D_GX 8            // ghost columns on each side
+#define S2D_GZ 8            // ghost rows above z = 0
 #define S2D_ZPT 4           // rows per lane (one float4)
 #define S2D_STRIP_ROWS 128  // rows a warp reads (32 lanes x 4)
-#define S2D_STRIP_OUT 120   // rows a warp writes; strip k writes [120k, 120k+120)
+#define S2D_STRIP_OUT 120   // rows a one-step warp writes; strip k writes [120k, 120k+120), reads from 120k-4
+#define S2D_TS_OUT 112      // rows a two-step warp writes; strip k writes [112k, 112k+112), reads from 112k-8
 
 namespace s2d {
 
@@ -25,9 +26,16 @@ constexpr float kA1 = -1.0f / 24.0f;       // cpu_modelling_kernels.cpp:10 (floa
 
 inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-// Strips a grid of nnz rows needs, and the leading dimension that holds them.
+// Strips a grid of nnz rows needs (one-step and two-step kernels), and the
+// leading dimension that holds the rows either kind reads.
 inline int num_strips(int nnz) { return (nnz + S2D_STRIP_OUT - 1) / S2D_STRIP_OUT; }
-inline int leading_dim(int nnz) { return round_up(S2D_GZ + S2D_STRIP_OUT * num_strips(nnz) + 8, 32); }
+inline int num_strips_ts(int nnz) { return (nnz + S2D_TS_OUT - 1) / S2D_TS_OUT; }
+inline int leading_dim(int nnz) {
+    const int rows = S2D_STRIP_OUT * num_strips(nnz) > S2D_TS_OUT * num_strips_ts(nnz)
+                         ? S2D_STRIP_OUT * num_strips(nnz)
+                         : S2D_TS_OUT * num_strips_ts(nnz);
+    return round_up(S2D_GZ + rows + 8, 32);
+}
 
 // One shot of a launch.  State pointers point at the allocation base
 // (ghost origin); st[parity][field] with fields px, pz, vx, vz.
@@ -84,6 +92,7 @@ struct StepArgs {
     int dt_factor;
     int fd_nt;
     int kt_base;          // FD step of the launch with kt_off = 0
+    int par0;             // state buffer holding step kt_base; launch kt_off reads par0 ^ (kt_off & 1)
     int stages;           // bulk-copy pipeline depth (shared-memory ring stages per warp)
     int *err;             // device error word (S2D_DEV_ERR_* bits), 0 when all waits completed
     int spin_limit;       // polls of an mbarrier before a wait counts as timed out
@@ -91,7 +100,6 @@ struct StepArgs {
     int task_order;       // 0: shot fastest, 1: strip fastest (see task_of)
     int flags;            // S2D_STEP_* bits
     int prod_kt0;         // FD step stored in plane 0 of ShotDev::prod
-    int pad2_;
 };
 
 #define S2D_STEP_NO_RECORD 1  // forward: do not sample receivers; adjoint: do not inject the adjoint source
@@ -104,7 +112,21 @@ struct StepArgs {
 // Step kernel variants.
 enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantLdgProducts = 3 /* plain loads + S2D_STEP_PRODUCTS, gradient runs */,
-                   kVariantLdg128 = 4 /* plain loads, compiled for 128 registers */ };
+                   kVariantLdg128 = 4 /* plain loads, compiled for 128 registers */,
+                   kVariantTs2 = 5 /* two FD steps per launch (112-row strips) */,
+                   kVariantTs1 = 6 /* one FD step in the two-step kernel's layout (odd remainders) */ };
+
+// FD steps one launch of a variant advances.
+inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
+// Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 halo columns).
+inline bool ts_layout(int variant) { return variant == kVariantTs2 || variant == kVariantTs1; }
+
+// Per-warp shared-memory delay lines of the two-step kernel (4 columns each):
+// the first step's px, pz and vz, and the kappa, bx, bz columns the first step
+// loaded, until the second step uses them.
+constexpr int kTsRing = 4;
+constexpr int kTsFields = 6;
+constexpr int kTsWarpBytes = kTsRing * kTsFields * S2D_STRIP_ROWS * 4;
 
 // Shared memory of one pipeline stage: 7 slots of one 128-row column each
 // (vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3).

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__r
     const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
     const int kt = a.kt_base + kt_off;
     if (kt >= a.fd_nt) return;
-    const int par = kt & 1;
+    const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
         fence_mbar_init();
     }
     __syncwarp();
-    const int par = kt & 1;
+    const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
     unsigned it0 = 0;  // pipeline iterations consumed by this warp so far
@@ -471,6 +471,177 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
                             : bulk_task<false>(a, Sh, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring, bars,
                                                S, drain_limit, it0);
         if (!ok) return;
+    }
+}
+
+// ------------------------------------------------------------ two-step variant
+//
+// One launch advances the batch by two FD steps (kt, kt+1): the state is read
+// from HBM once and written once per two steps.  The warp streams along x as
+// the one-step kernel does; step A (kt) runs at the front of the stream and
+// step B (kt+1) trails it:
+//   column L of vx (step-A input) is loaded at loop index L;
+//   step A: p at L-1, v at L-3 (as in the one-step kernel);
+//   step B: p at L-4 (needs step-A vx at L-6 .. L-3), v at L-6 (needs step-B p
+//           at L-7 .. L-4).
+// Step-A results never reach HBM: vx in a 4-column register window, px, pz
+// and vz in per-warp shared-memory delay lines of 4 columns (each lane reads
+// back only what it wrote); the kappa, bx, bz columns step A loads wait in
+// the same delay lines for step B, so the second step reads nothing from
+// memory.  Two steps of z-halo leave lanes 2..29 valid
+// (rows c+8 .. c+119 of a strip starting at c = 112k - 8), so strips write
+// 112 rows; the segment's stream starts 6 columns early and ends 5 late.
+// TWO = false is the same kernel doing step A alone (odd remainders), in the
+// same strip layout.
+
+__device__ __forceinline__ float4 &ring_at(float4 *ring, int field, int col, int lane) {
+    return ring[(field * kTsRing + ((col + 2 * S2D_GX) & (kTsRing - 1))) * 32 + lane];
+}
+
+template <bool FAST, bool TWO>
+__device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                        int kt, int par, int lane, float4 *ring) {
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t ld = (size_t)S.ld;
+    const int c = strip * S2D_TS_OUT - 8;
+    Lane<FAST> la;
+    lane_setup(la, S, c, lane, kt);
+    la.owner = lane >= 2 && lane <= 29;
+    Lane<FAST> lb = la;
+    if (TWO) lb.amp = __ldg(S.amp + kt + 1);
+    const bool rec = !(a.flags & S2D_STEP_NO_RECORD);
+    const bool rec_a = rec && ((kt + 1) % a.dt_factor) == 0 && (kt + 1) / a.dt_factor - 1 < S.real_nt;
+    const int slot_a = (kt + 1) / a.dt_factor - 1;
+    const bool rec_b = TWO && rec && ((kt + 2) % a.dt_factor) == 0 && (kt + 2) / a.dt_factor - 1 < S.real_nt;
+    const int slot_b = (kt + 2) / a.dt_factor - 1;
+    const size_t off = (size_t)(la.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const float *__restrict__ pxi = S.st[par][0] + off;
+    const float *__restrict__ pzi = S.st[par][1] + off;
+    const float *__restrict__ vxi = S.st[par][2] + off;
+    const float *__restrict__ vzi = S.st[par][3] + off;
+    float *__restrict__ pxo = S.st[par ^ 1][0] + off;
+    float *__restrict__ pzo = S.st[par ^ 1][1] + off;
+    float *__restrict__ vxo = S.st[par ^ 1][2] + off;
+    float *__restrict__ vzo = S.st[par ^ 1][3] + off;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = S.bx + off;
+    const float *__restrict__ bzp = S.bz + off;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    // step A windows: vx at L-3..L, new p at L-4..L-1, vz at L-3..L-1
+    float4 vq0 = zero, vq1, vq2, vq3;
+    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+    float4 zq0 = zero, zq1 = zero, zq2 = zero;
+    // step B windows: step-A vx at L-6..L-3, step-B p at L-7..L-4
+    float4 wq0 = zero, wq1 = zero, wq2 = zero, wq3 = zero;
+    float4 bq0 = zero, bq1 = zero, bq2 = zero, bq3 = zero;
+    const int h = TWO ? 3 : 0;  // step A runs over [xa - h, xb + h)
+    const int xaa = xa - h, xba = xb + h;
+    vq1 = ld4(vxi + (ptrdiff_t)(xaa - 3) * (ptrdiff_t)ld);
+    vq2 = ld4(vxi + (ptrdiff_t)(xaa - 2) * (ptrdiff_t)ld);
+    vq3 = ld4(vxi + (ptrdiff_t)(xaa - 1) * (ptrdiff_t)ld);
+    for (int L = xaa; L <= xba + 2; ++L) {
+        // ---- step A: p at PA = L-1 ----
+        const int PA = L - 1;
+        const ptrdiff_t colA = (ptrdiff_t)PA * (ptrdiff_t)ld;
+        const ptrdiff_t colV0 = (ptrdiff_t)(L - 3) * (ptrdiff_t)ld;
+        const float4 xa4 = __ldg(S.xcoef + (PA + S2D_GX));
+        const bool colm = xa4.x == 1.0f;
+        const bool pz_live = !(FAST && colm);
+        const float4 cvx = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
+        const float4 cvz = ld4(vzi + colA);
+        const float4 cpx = ld4(pxi + colA);
+        const float4 cpz = pz_live ? ld4(pzi + colA) : zero;
+        const float4 ckk = ld4(kap + colA);
+        const float4 cbx = ld4(bxp + colV0);
+        const float4 cbz = ld4(bzp + colV0);
+        vq0 = vq1; vq1 = vq2; vq2 = vq3;
+        vq3 = cvx;
+        const float4 vz = cvz;
+        float4 pxn, pzn, dxv, dzv;
+        const float4 kka = ckk;
+        const float4 pn = p_update(la, S, PA, xa4, colm, vq0, vq1, vq2, vq3, cpx, cpz, kka, vz, pxn, pzn, dxv, dzv);
+        const bool in_a = PA >= xa && PA < xb;
+        if (TWO) {
+            ring_at(ring, 0, PA, lane) = pxn;
+            ring_at(ring, 1, PA, lane) = pzn;
+            ring_at(ring, 3, PA, lane) = kka;
+        } else if (in_a && la.owner) {
+            st4(pxo + colA, pxn);
+            if (pz_live) st4(pzo + colA, pzn);
+        }
+        if (rec_a && in_a) record(la, S, PA, pn, slot_a);
+        pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+        zq0 = zq1; zq1 = zq2; zq2 = vz;
+        if (L < xaa + 3) continue;
+        // ---- step A: v at VA = L-3 ----
+        const int VA = L - 3;
+        const ptrdiff_t colVA = (ptrdiff_t)VA * (ptrdiff_t)ld;
+        float4 vxn, vzn, dxp, dzp;
+        const float4 bxa = cbx, bza = cbz;
+        v_update(la, S, VA, pq0, pq1, pq2, pq3, vq0, zq0, bxa, bza, vxn, vzn, dxp, dzp);
+        if (!TWO) {
+            if (la.owner) {
+                st4(vxo + colVA, vxn);
+                st4(vzo + colVA, vzn);
+            }
+            continue;
+        }
+        wq0 = wq1; wq1 = wq2; wq2 = wq3; wq3 = vxn;
+        ring_at(ring, 2, VA, lane) = vzn;
+        ring_at(ring, 4, VA, lane) = bxa;
+        ring_at(ring, 5, VA, lane) = bza;
+        if (L < xa + 3) continue;
+        // ---- step B: p at PB = L-4 ----
+        const int PB = L - 4;
+        const ptrdiff_t colB = (ptrdiff_t)PB * (ptrdiff_t)ld;
+        const float4 vzb = ring_at(ring, 2, PB, lane);
+        const float4 xb4 = __ldg(S.xcoef + (PB + S2D_GX));
+        const bool colmb = xb4.x == 1.0f;
+        const bool pz_liveb = !(FAST && colmb);
+        float4 pxm, pzm, dxw, dzw;
+        const float4 pm = p_update(lb, S, PB, xb4, colmb, wq0, wq1, wq2, wq3, ring_at(ring, 0, PB, lane),
+                                   pz_liveb ? ring_at(ring, 1, PB, lane) : zero, ring_at(ring, 3, PB, lane), vzb,
+                                   pxm, pzm, dxw, dzw);
+        const bool in_b = PB >= xa && PB < xb;
+        if (in_b && la.owner) {
+            st4(pxo + colB, pxm);
+            if (pz_liveb) st4(pzo + colB, pzm);
+        }
+        if (rec_b && in_b) record(lb, S, PB, pm, slot_b);
+        bq0 = bq1; bq1 = bq2; bq2 = bq3; bq3 = pm;
+        if (L < xa + 6) continue;
+        // ---- step B: v at VB = L-6 ----
+        const int VB = L - 6;
+        const ptrdiff_t colVB = (ptrdiff_t)VB * (ptrdiff_t)ld;
+        float4 vxm, vzm, dxq, dzq;
+        v_update(lb, S, VB, bq0, bq1, bq2, bq3, wq0, ring_at(ring, 2, VB, lane), ring_at(ring, 4, VB, lane),
+                 ring_at(ring, 5, VB, lane), vxm, vzm, dxq, dzq);
+        if (la.owner) {
+            st4(vxo + colVB, vxm);
+            st4(vzo + colVB, vzm);
+        }
+    }
+}
+
+template <bool TWO>
+__global__ void __launch_bounds__(128, 3) step_kernel_ts(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base + (TWO ? 2 : 1) * kt_off;
+    if (kt + (TWO ? 1 : 0) >= a.fd_nt) return;
+    const int par = a.par0 ^ (kt_off & 1);
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kTsWarpBytes);
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const int c = strip * S2D_TS_OUT - 8;
+        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1))
+            ts_task<true, TWO>(a, S, strip, xa, seg_len, kt, par, lane, ring);
+        else
+            ts_task<false, TWO>(a, S, strip, xa, seg_len, kt, par, lane, ring);
     }
 }
 
@@ -527,6 +698,10 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_ldg<true, 3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantLdg128)
         step_kernel_ldg<false, 4><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantTs2)
+        step_kernel_ts<true><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantTs1)
+        step_kernel_ts<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
         step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
@@ -552,6 +727,8 @@ const void *kernel_of(int variant) {
     if (variant == kVariantBulk128) return (const void *)step_kernel_bulk<4>;
     if (variant == kVariantLdgProducts) return (const void *)step_kernel_ldg<true, 3>;
     if (variant == kVariantLdg128) return (const void *)step_kernel_ldg<false, 4>;
+    if (variant == kVariantTs2) return (const void *)step_kernel_ts<true>;
+    if (variant == kVariantTs1) return (const void *)step_kernel_ts<false>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace

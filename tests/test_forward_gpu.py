@@ -40,7 +40,7 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
-VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4}
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -358,3 +358,25 @@ def test_autotuner_skips_short_calls():
         c.close()
     for g, r in zip(got, ref):
         np.testing.assert_array_equal(g, r)
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_odd_continuations_equal_one_run(ctx, variant):
+    """A run cut into calls of 7 steps (odd: the two-step variant ends every
+    call with a one-step launch and the next call starts from the other
+    buffer) records the same traces as one call."""
+    import torch
+    from seis2d_b200 import derive_steps
+    _, _, rec, wave, shots, _ = _tall_grid(ctx, nshots=2)
+    steps = derive_steps(wave)
+    nt, fd_nt = steps["real_nt"], steps["fd_nt"]
+    ctx.set_option("variant", VARIANTS[variant])
+    try:
+        whole = np.concatenate(ctx.forward(shots, wave))
+        out = torch.zeros(len(shots) * rec.shape[0] * nt, dtype=torch.float32, device="cuda")
+        for k0 in range(0, fd_nt, 7):
+            ctx.forward(shots, wave, kt_begin=k0, kt_count=7, out=out)
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_option("autotune", 1)
+    np.testing.assert_array_equal(out.cpu().numpy().reshape(whole.shape), whole)
