@@ -688,7 +688,8 @@ int batch_tasks(const Batch &b) {
 }
 
 // Autotuner: advance the batch by kTuneSteps real FD steps from kt_begin,
-// kTuneWarm + kTuneTimed launches under each candidate configuration (every
+// kTuneWarm + kTuneTimed launches under each candidate configuration, in
+// rounds that visit every candidate once (every
 // candidate computes the same bits: they share the update arithmetic and
 // differ only in how columns reach registers, how many steps a pass makes and
 // how tasks map to warps), with each timed launch between two events.  The
@@ -707,35 +708,39 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     auto release = [&]() {
         for (auto &x : ev) cudaEventDestroy(x);
     };
-    std::vector<LaunchCfg> cfg(kNumTuneCandidates);
+    std::vector<LaunchCfg> cfg(kNumTuneCandidates), full(kNumTuneCandidates);
     std::vector<bool> ok(kNumTuneCandidates, false);
-    int kt = kt_begin;
-    bool graph_used = false;
     for (int i = 0; i < kNumTuneCandidates; ++i) {
         const int *k = kTuneCandidates[i];
-        LaunchCfg lc;
-        if (launch_config(c, 1L << 40, &lc, k[0], k[1], k[2]) != S2D_OK) {
+        if (launch_config(c, 1L << 40, &full[i], k[0], k[1], k[2]) == S2D_OK) {
+            ok[i] = true;
+        } else {
             if (i == 0) {
                 release();
                 return S2D_ERR_ARG;
             }
-            // a configuration this device cannot run: its steps run under the
-            // first candidate instead and are not timed
-            lc = cfg[0];
-        } else {
-            ok[i] = true;
+            // a configuration this device cannot run: its trial steps run
+            // under the first candidate instead and are not counted
+            full[i] = full[0];
         }
-        int e = layout_groups(c, b, lc);
-        if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
-        if (e) {
-            release();
-            return e;
-        }
-        cfg[i] = lc;
-        a.total_tasks = batch_tasks(b);
-        const int spl = steps_per_launch(lc.variant);
-        for (int s = 0; s < kTuneWarm + kTuneTimed; ++s, kt += spl) {
-            const int t = s - kTuneWarm;
+    }
+    // Rounds: one untimed, then kTuneTimed timed, each visiting every
+    // candidate once, so clock ramps and drift reach all candidates alike.
+    int kt = kt_begin;
+    bool graph_used = false;
+    for (int r = 0; r < kTuneWarm + kTuneTimed; ++r) {
+        const int t = r - kTuneWarm;
+        for (int i = 0; i < kNumTuneCandidates; ++i) {
+            LaunchCfg lc = full[i];
+            int e = layout_groups(c, b, lc);
+            if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
+            if (e) {
+                release();
+                return e;
+            }
+            cfg[i] = lc;
+            a.total_tasks = batch_tasks(b);
+            const int spl = steps_per_launch(lc.variant);
             if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t)], c->stream));
             e = run_loop(c, b, lc, a, kt, spl, false, launches, &graph_used);
             if (e) {
@@ -743,6 +748,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
                 return e;
             }
             if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t) + 1], c->stream));
+            kt += spl;
         }
     }
     cudaError_t ce = cudaStreamSynchronize(c->stream);
