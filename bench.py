@@ -437,6 +437,8 @@ def main():
         from seis2d_b200 import Context
         with Context(0) as ctx:
             ctx.set_option("grad_segment", args.grad_segment)
+            if args.variant >= 0:
+                ctx.set_option("variant", args.variant)
             print(json.dumps({"leg": "c5_gradient", **gradient_leg(ctx, args.shots or 32, args.grad_time)}))
         return 0
 
