@@ -539,6 +539,45 @@ def main():
                 "bytes_per_cell_update": st.alg_bytes / st.cell_updates, "launch_ms": per_launch_s * 1e3,
                 "fd_steps_per_launch": spl}
 
+    # ---- end to end through the C ABI from pinned host memory ----
+    e2e = None
+    if not args.no_e2e:
+        vp_h = torch.from_numpy(vp).pin_memory()
+        rho_h = torch.from_numpy(rho).pin_memory()
+        out_h = torch.zeros(nrec_tot * steps["real_nt"], dtype=torch.float32).pin_memory()
+        short = Wave(chunk * w["dt"], w["dt"], w["dt"], w["f"])
+        real_short = derive_steps(short)["real_nt"]
+        out_h = out_h[: nrec_tot * real_short]
+        n_e2e = max(1, min(args.steps, 3))
+
+        loop_s = []
+
+        def one():
+            mm = ctx.model(vp_h.numpy(), rho_h.numpy(), w["d"], w["d"], w["nb"])
+            ctx.forward([Shot(mm, s, rec) for s in src], short, out=out_h.numpy())
+            loop_s.append(ctx.last_stats.loop_ms * 1e-3)
+            mm.release()
+
+        one()
+        barrier()
+        eclk = ClockSampler(torch.cuda.current_device())
+        eclk.start()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            one()
+        barrier()
+        et = torch.tensor([time.perf_counter() - t0], device="cuda")
+        eclocks = eclk.stop()
+        if dist is not None:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        ecells = cells_step * derive_steps(short)["fd_nt"] * n_e2e * world
+        e2e = {"value": ecells / float(et.item()) / 1e9, "unit": "Gcell/s",
+               "h2d_bytes_per_step": int(vp.nbytes + rho.nbytes),
+               "d2h_bytes_per_step": int(nrec_tot * real_short * 4),
+               "sample": f"{n_e2e} calls: model upload + {nshots} shots x {derive_steps(short)['fd_nt']} FD steps "
+                         f"+ seismogram download, pinned host buffers", "clocks": eclocks,
+               "wall_s_per_call": float(et.item()) / n_e2e, "loop_s_per_call": sum(loop_s[1:]) / n_e2e}
+
     # ---- plain: the same shots one after another ----
     plain = None
     if not args.no_plain and nshots > 1:
@@ -554,38 +593,6 @@ def main():
         prate = cells_step * pch / (pms * 1e-3) / 1e9
         plain = {"value": prate * world, "unit": "Gcell/s", "speedup_batched_vs_plain": value / (prate * world),
                  "sample": f"{nshots} shots x {pch} FD steps, shot after shot"}
-
-    # ---- end to end through the C ABI from pinned host memory ----
-    e2e = None
-    if not args.no_e2e:
-        vp_h = torch.from_numpy(vp).pin_memory()
-        rho_h = torch.from_numpy(rho).pin_memory()
-        out_h = torch.zeros(nrec_tot * steps["real_nt"], dtype=torch.float32).pin_memory()
-        short = Wave(chunk * w["dt"], w["dt"], w["dt"], w["f"])
-        real_short = derive_steps(short)["real_nt"]
-        out_h = out_h[: nrec_tot * real_short]
-        n_e2e = max(1, min(args.steps, 3))
-
-        def one():
-            mm = ctx.model(vp_h.numpy(), rho_h.numpy(), w["d"], w["d"], w["nb"])
-            ctx.forward([Shot(mm, s, rec) for s in src], short, out=out_h.numpy())
-            mm.release()
-
-        one()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(n_e2e):
-            one()
-        barrier()
-        et = torch.tensor([time.perf_counter() - t0], device="cuda")
-        if dist is not None:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        ecells = cells_step * derive_steps(short)["fd_nt"] * n_e2e * world
-        e2e = {"value": ecells / float(et.item()) / 1e9, "unit": "Gcell/s",
-               "h2d_bytes_per_step": int(vp.nbytes + rho.nbytes),
-               "d2h_bytes_per_step": int(nrec_tot * real_short * 4),
-               "sample": f"{n_e2e} calls: model upload + {nshots} shots x {derive_steps(short)['fd_nt']} FD steps "
-                         f"+ seismogram download, pinned host buffers"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
