@@ -53,7 +53,10 @@ struct Model {
     float dx = 0, dz = 0;
     size_t field_elems = 0;  // nxa * ld
     DevBuf vp, rho;          // raw [nx][nz] copies (source amplitude needs vp, rho at the source)
-    DevBuf kappa, bx, bz;    // padded layout
+    DevBuf mat;              // kappa, bx, bz in one allocation, field_elems apart (padded layout)
+    float *kappa() const { return mat.as<float>(); }
+    float *bx() const { return mat.as<float>() + field_elems; }
+    float *bz() const { return mat.as<float>() + 2 * field_elems; }
     std::vector<float> damp2a, damp2a1, damp2b, damp2b1, damp1a, damp1a1, damp1b, damp1b1;
     // Algorithmic DRAM bytes of one FD step of one shot: 44 B per cell, 36 B
     // where both pressure dampings are 1 (the cell carries p alone).
@@ -517,17 +520,20 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         ShotDev &d = b.shot_dev[s];
         std::memset(&d, 0, sizeof d);
         const size_t fb = m.field_elems * sizeof(float);
-        for (int par = 0; par < 2; ++par)
-            for (int f = 0; f < 4; ++f) {
-                cudaError_t ae;
-                b.state.push_back(c->pool.take(fb, &ae));
-                CK(ae);
-                CK(cudaMemsetAsync(b.state.back()->p, 0, fb, c->stream));
-                d.st[par][f] = b.state.back()->as<float>();
-            }
-        d.kappa = m.kappa.as<float>();
-        d.bx = m.bx.as<float>();
-        d.bz = m.bz.as<float>();
+        // the 8 state fields of the shot in one allocation (ShotDev::fstride)
+        {
+            cudaError_t ae;
+            b.state.push_back(c->pool.take(8 * fb, &ae));
+            CK(ae);
+            CK(cudaMemsetAsync(b.state.back()->p, 0, 8 * fb, c->stream));
+            for (int par = 0; par < 2; ++par)
+                for (int f = 0; f < 4; ++f)
+                    d.st[par][f] = b.state.back()->as<float>() + (size_t)(par * 4 + f) * m.field_elems;
+        }
+        d.fstride = (int)m.field_elems;
+        d.kappa = m.kappa();
+        d.bx = m.bx();
+        d.bz = m.bz();
         d.xcoef = m.xcoef.as<float4>();
         d.zcoef = m.zcoef.as<float4>();
         d.nnx = m.nnx;
@@ -904,6 +910,10 @@ int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, cons
     m->ld = leading_dim(m->nnz);
     m->nxa = m->nnx + 2 * S2D_GX;
     m->field_elems = (size_t)m->nxa * m->ld;
+    // kernels address the 8 state fields of a shot with 32-bit offsets
+    if (8 * m->field_elems >= (size_t)1 << 31)
+        return fail(c, S2D_ERR_ARG, "padded grid %d x %d is too large (8 fields of %zu cells exceed 2^31)", m->nnx,
+                    m->nnz, m->field_elems);
     const size_t raw = (size_t)nx * nz * sizeof(float);
     CK(m->vp.alloc(raw));
     CK(m->rho.alloc(raw));
@@ -911,17 +921,13 @@ int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, cons
     CK(cudaMemcpyAsync(m->vp.p, vp, raw, kind, c->stream));
     CK(cudaMemcpyAsync(m->rho.p, rho, raw, kind, c->stream));
     const size_t fb = m->field_elems * sizeof(float);
-    CK(m->kappa.alloc(fb));
-    CK(m->bx.alloc(fb));
-    CK(m->bz.alloc(fb));
+    CK(m->mat.alloc(3 * fb));
     DevBuf bue;
     CK(bue.alloc(fb));
-    CK(cudaMemsetAsync(m->kappa.p, 0, fb, c->stream));
-    CK(cudaMemsetAsync(m->bx.p, 0, fb, c->stream));
-    CK(cudaMemsetAsync(m->bz.p, 0, fb, c->stream));
+    CK(cudaMemsetAsync(m->mat.p, 0, 3 * fb, c->stream));
     CK(cudaMemsetAsync(bue.p, 0, fb, c->stream));
-    int e = launch_prepare_model(m->vp.as<float>(), m->rho.as<float>(), nx, nz, nb, m->ld, m->kappa.as<float>(),
-                                 bue.as<float>(), m->bx.as<float>(), m->bz.as<float>(), c->stream);
+    int e = launch_prepare_model(m->vp.as<float>(), m->rho.as<float>(), nx, nz, nb, m->ld, m->kappa(), bue.as<float>(),
+                                 m->bx(), m->bz(), c->stream);
     if (e) return fail(c, S2D_ERR_CUDA, "prepare_model: %s", cudaGetErrorString((cudaError_t)e));
     CK(cudaStreamSynchronize(c->stream));
     sponge_a(nb, nx, m->damp2a, m->damp2a1);
@@ -1179,20 +1185,22 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     std::vector<ShotDev> adj = b.shot_dev;
     std::vector<float *> gk(nshots), gb(nshots), sadj(nshots);
     for (int s = 0; s < nshots; ++s) {
-        for (int par = 0; par < 2; ++par)
-            for (int f = 0; f < 4; ++f) {
-                void *p;
-                int e = grad_alloc(c, g, fb, &p);
-                if (e) return e;
-                CK(cudaMemsetAsync(p, 0, fb, c->stream));
-                adj[s].st[par][f] = static_cast<float *>(p);
-            }
+        // adjoint state: 8 fields in one allocation, as the forward state
         void *p;
-        for (int f = 0; f < 2; ++f) {
-            int e = grad_alloc(c, g, fb, &p);
+        {
+            int e = grad_alloc(c, g, 8 * fb, &p);
             if (e) return e;
-            CK(cudaMemsetAsync(p, 0, fb, c->stream));
-            adj[s].grad[f] = static_cast<float *>(p);
+            CK(cudaMemsetAsync(p, 0, 8 * fb, c->stream));
+            for (int par = 0; par < 2; ++par)
+                for (int f = 0; f < 4; ++f) adj[s].st[par][f] = static_cast<float *>(p) + (size_t)(par * 4 + f) * F;
+        }
+        // accumulators dJ/dkappa, dJ/db, one allocation
+        {
+            int e = grad_alloc(c, g, 2 * fb, &p);
+            if (e) return e;
+            CK(cudaMemsetAsync(p, 0, 2 * fb, c->stream));
+            adj[s].grad[0] = static_cast<float *>(p);
+            adj[s].grad[1] = static_cast<float *>(p) + F;
         }
         gk[s] = adj[s].grad[0];
         gb[s] = adj[s].grad[1];

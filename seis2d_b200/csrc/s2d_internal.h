@@ -38,7 +38,10 @@ inline int leading_dim(int nnz) {
 }
 
 // One shot of a launch.  State pointers point at the allocation base
-// (ghost origin); st[parity][field] with fields px, pz, vx, vz.
+// (ghost origin); st[parity][field] with fields px, pz, vx, vz.  The eight
+// state fields are one allocation, field k (= parity*4 + field) at
+// st[0][0] + k*fstride, and kappa, bx, bz likewise (bx = kappa + fstride,
+// bz = kappa + 2*fstride): the kernels address every field from one base.
 struct ShotDev {
     float *st[2][4];
     const float *kappa, *bx, *bz;  // materials, same layout as the state
@@ -52,10 +55,10 @@ struct ShotDev {
     const int *rec_id;             // index of the entry's trace in seis
     float *seis;                   // [nrec][real_nt]; the adjoint reads its source here
     int real_nt;
-    int pad_;
+    int fstride;                   // elements between consecutive fields (8 * fstride < 2^31)
     // gradient runs only
     float *prod;                   // [steps][4][field]: D-x vx, D-z vz, D+x p, D+z p of each step
-    float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout)
+    float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout, grad[1] = grad[0] + fstride)
     float *srcadj;                 // [fd_nt] adjoint pressure at the source after each step
     // element counts of the buffers above (device self-checks, S2D_DEVICE_CHECKS)
     size_t nfield;                 // every per-cell field

@@ -192,17 +192,22 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
     float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
-    const float *__restrict__ pxi = S.st[par][0] + off;
-    const float *__restrict__ pzi = S.st[par][1] + off;
-    const float *__restrict__ vxi = S.st[par][2] + off;
-    const float *__restrict__ vzi = S.st[par][3] + off;
-    float *__restrict__ pxo = S.st[par ^ 1][0] + off;
-    float *__restrict__ pzo = S.st[par ^ 1][1] + off;
-    float *__restrict__ vxo = S.st[par ^ 1][2] + off;
-    float *__restrict__ vzo = S.st[par ^ 1][3] + off;
+    // every field from one base and a 32-bit stride (fewer live registers
+    // than eleven 64-bit pointers)
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    const float *__restrict__ pxi = sb + ib;
+    const float *__restrict__ pzi = sb + ib + fs;
+    const float *__restrict__ vxi = sb + ib + 2 * fs;
+    const float *__restrict__ vzi = sb + ib + 3 * fs;
+    float *__restrict__ pxo = sb + ob;
+    float *__restrict__ pzo = sb + ob + fs;
+    float *__restrict__ vxo = sb + ob + 2 * fs;
+    float *__restrict__ vzo = sb + ob + 3 * fs;
     const float *__restrict__ kap = S.kappa + off;
-    const float *__restrict__ bxp = S.bx + off;
-    const float *__restrict__ bzp = S.bz + off;
+    const float *__restrict__ bxp = kap + fs;
+    const float *__restrict__ bzp = kap + 2 * fs;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 vq0 = zero, vq1, vq2, vq3;
     float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
@@ -333,11 +338,12 @@ __device__ __forceinline__ bool bulk_task(const StepArgs &a, const ShotDev &Sh, 
     // column 0 of the warp's strip in each field (row c), and this lane's rows
     const size_t wofs = (size_t)(c + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t lofs = wofs + (size_t)(S2D_ZPT * lane);
-    const float *src_vx = Sh.st[par][2] + wofs, *src_px = Sh.st[par][0] + wofs;
-    const float *src_pz = Sh.st[par][1] + wofs, *src_vz = Sh.st[par][3] + wofs;
-    const float *src_k = Sh.kappa + wofs, *src_bx = Sh.bx + wofs, *src_bz = Sh.bz + wofs;
-    float *pxo = Sh.st[par ^ 1][0] + lofs, *pzo = Sh.st[par ^ 1][1] + lofs;
-    float *vxo = Sh.st[par ^ 1][2] + lofs, *vzo = Sh.st[par ^ 1][3] + lofs;
+    const int fs = Sh.fstride;
+    const float *src_px = Sh.st[0][0] + wofs + par * 4 * fs;
+    const float *src_pz = src_px + fs, *src_vx = src_px + 2 * fs, *src_vz = src_px + 3 * fs;
+    const float *src_k = Sh.kappa + wofs, *src_bx = src_k + fs, *src_bz = src_k + 2 * fs;
+    float *pxo = Sh.st[0][0] + lofs + (par ^ 1) * 4 * fs, *pzo = pxo + fs;
+    float *vxo = pxo + 2 * fs, *vzo = pxo + 3 * fs;
     const int n_it = xb - xa + 6;  // columns L = xa-3 .. xb+2
 
     // Producer (lane 0): bring iteration j's columns into stage (it0+j) % S.
@@ -515,17 +521,20 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
     const bool rec_b = TWO && rec && ((kt + 2) % a.dt_factor) == 0 && (kt + 2) / a.dt_factor - 1 < S.real_nt;
     const int slot_b = (kt + 2) / a.dt_factor - 1;
     const size_t off = (size_t)(la.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
-    const float *__restrict__ pxi = S.st[par][0] + off;
-    const float *__restrict__ pzi = S.st[par][1] + off;
-    const float *__restrict__ vxi = S.st[par][2] + off;
-    const float *__restrict__ vzi = S.st[par][3] + off;
-    float *__restrict__ pxo = S.st[par ^ 1][0] + off;
-    float *__restrict__ pzo = S.st[par ^ 1][1] + off;
-    float *__restrict__ vxo = S.st[par ^ 1][2] + off;
-    float *__restrict__ vzo = S.st[par ^ 1][3] + off;
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    const float *__restrict__ pxi = sb + ib;
+    const float *__restrict__ pzi = sb + ib + fs;
+    const float *__restrict__ vxi = sb + ib + 2 * fs;
+    const float *__restrict__ vzi = sb + ib + 3 * fs;
+    float *__restrict__ pxo = sb + ob;
+    float *__restrict__ pzo = sb + ob + fs;
+    float *__restrict__ vxo = sb + ob + 2 * fs;
+    float *__restrict__ vzo = sb + ob + 3 * fs;
     const float *__restrict__ kap = S.kappa + off;
-    const float *__restrict__ bxp = S.bx + off;
-    const float *__restrict__ bzp = S.bz + off;
+    const float *__restrict__ bxp = kap + fs;
+    const float *__restrict__ bzp = kap + 2 * fs;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     // step A windows: vx at L-3..L, new p at L-4..L-1, vz at L-3..L-1
     float4 vq0 = zero, vq1, vq2, vq3;

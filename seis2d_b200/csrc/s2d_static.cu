@@ -149,10 +149,13 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
                  o_rid = cv.take<int>(std::max(nrec, 1));
     const size_t o_vp = host_model ? cv.take<float>((size_t)nx * nz) : 0;
     const size_t o_rho = host_model ? cv.take<float>((size_t)nx * nz) : 0;
-    const size_t o_kap = cv.take<float>(F), o_bx = cv.take<float>(F), o_bz = cv.take<float>(F),
-                 o_bue = cv.take<float>(F);
+    // kappa, bx, bz and the 8 state fields each one block, fields F apart
+    // (the kernels address them from one base, ShotDev::fstride)
+    const size_t o_kap = cv.take<float>(3 * F), o_bx = o_kap + F * sizeof(float), o_bz = o_kap + 2 * F * sizeof(float);
+    const size_t o_bue = cv.take<float>(F);
     size_t o_st[8];
-    for (int f = 0; f < 8; ++f) o_st[f] = cv.take<float>(F);
+    o_st[0] = cv.take<float>(8 * F);
+    for (int f = 1; f < 8; ++f) o_st[f] = o_st[0] + (size_t)f * F * sizeof(float);
     const size_t seis_n = (size_t)nrec * rs.real_nt;
     const size_t o_seis = host_seis ? cv.take<float>(std::max<size_t>(seis_n, 1)) : 0;
     if (cv.used > kScratchBytes)
@@ -209,7 +212,7 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
 
     // device contents: clear what must start at zero, copy tables and model
     SCK(cudaMemsetAsync(at(o_err), 0, sizeof(int), st));
-    SCK(cudaMemsetAsync(at(o_kap), 0, (o_st[0] - o_kap), st));            // materials incl. ghosts
+    SCK(cudaMemsetAsync(at(o_kap), 0, (o_st[0] - o_kap), st));            // materials (and bue) incl. ghosts
     SCK(cudaMemsetAsync(at(o_st[0]), 0, (o_st[7] + F * sizeof(float)) - o_st[0], st));  // 8 state fields
     if (host_seis) SCK(cudaMemsetAsync(at(o_seis), 0, std::max<size_t>(seis_n, 1) * sizeof(float), st));
     else SCK(cudaMemsetAsync(seis_out, 0, seis_n * sizeof(float), st));
@@ -240,6 +243,7 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     std::memset(&sd, 0, sizeof sd);
     for (int par = 0; par < 2; ++par)
         for (int f = 0; f < 4; ++f) sd.st[par][f] = reinterpret_cast<float *>(at(o_st[par * 4 + f]));
+    sd.fstride = (int)F;
     sd.kappa = reinterpret_cast<const float *>(at(o_kap));
     sd.bx = reinterpret_cast<const float *>(at(o_bx));
     sd.bz = reinterpret_cast<const float *>(at(o_bz));
