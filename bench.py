@@ -251,13 +251,17 @@ def gradient_leg(ctx, nshots=32, T=3.0):
     # warm-up with the same shot count: an inversion calls the gradient of the
     # same shapes every iteration, its device buffers then come from the pool
     ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho)
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.start()
     tg, g = _timed(lambda: ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho))
+    clocks = clk.stop()
     res = {"workload": f"FWI gradient, 1201x401 (seeded gradient + two +-300 m/s anomalies; start = gradient), "
                        f"rho 2000, nb 50, {nshots} shots x 1201 receivers, nt {st['fd_nt']}",
            "gradient_s_per_shot": tg / nshots, "forward_s_per_shot": tf / nshots,
            "gradient_over_forward": tg / tf, "misfit": g.misfit,
            "checkpoint_interval": int(g.stats.grad_segment),
-           "forward_gcells_per_s": ms.padded_cells * nshots * st["fd_nt"] / tf / 1e9}
+           "forward_gcells_per_s": ms.padded_cells * nshots * st["fd_nt"] / tf / 1e9,
+           "clocks_during_gradient": clocks}
     ms.release()
     return res
 

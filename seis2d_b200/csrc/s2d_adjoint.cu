@@ -110,25 +110,23 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
     // Every buffer below is distinct: restrict lets the compiler issue the
-    // accumulator and product loads ahead of the state stores.  All fields
-    // of a kind come from one base and a 32-bit stride.
-    const int fs = S.fstride;
-    float *const sb = S.st[0][0] + off;
-    const int ib = pin * 4 * fs, ob = pout * 4 * fs;
-    const float *__restrict__ mpxi = sb + ib;
-    const float *__restrict__ mpzi = sb + ib + fs;
-    const float *__restrict__ mvxi = sb + ib + 2 * fs;
-    const float *__restrict__ mvzi = sb + ib + 3 * fs;
-    float *__restrict__ mpxo = sb + ob;
-    float *__restrict__ mpzo = sb + ob + fs;
-    float *__restrict__ mvxo = sb + ob + 2 * fs;
-    float *__restrict__ mvzo = sb + ob + 3 * fs;
+    // accumulator and product loads ahead of the state stores.  (Per-field
+    // pointers here: the base-and-stride form the forward kernels use costs
+    // this kernel more address arithmetic than it saves in spills.)
+    const float *__restrict__ mpxi = S.st[pin][0] + off;
+    const float *__restrict__ mpzi = S.st[pin][1] + off;
+    const float *__restrict__ mvxi = S.st[pin][2] + off;
+    const float *__restrict__ mvzi = S.st[pin][3] + off;
+    float *__restrict__ mpxo = S.st[pout][0] + off;
+    float *__restrict__ mpzo = S.st[pout][1] + off;
+    float *__restrict__ mvxo = S.st[pout][2] + off;
+    float *__restrict__ mvzo = S.st[pout][3] + off;
     const float *__restrict__ kap = S.kappa + off;
-    const float *__restrict__ bxp = kap + fs;
-    const float *__restrict__ bzp = kap + 2 * fs;
+    const float *__restrict__ bxp = S.bx + off;
+    const float *__restrict__ bzp = S.bz + off;
     const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
     float *__restrict__ gk = S.grad[0] + off;
-    float *__restrict__ gb = gk + fs;
+    float *__restrict__ gb = S.grad[1] + off;
     const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
                      (kt + 1) / a.dt_factor - 1 < S.real_nt;
     const int slot = (kt + 1) / a.dt_factor - 1;
