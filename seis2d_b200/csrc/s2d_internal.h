@@ -125,10 +125,9 @@ inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1
 inline bool ts_layout(int variant) { return variant == kVariantTs2 || variant == kVariantTs1; }
 
 // Per-warp shared-memory delay lines of the two-step kernel (4 columns each):
-// the first step's px, pz and vz, and the kappa, bx, bz columns the first step
-// loaded, until the second step uses them.
+// the first step's px, pz, vz and vx and the second step's p.
 constexpr int kTsRing = 4;
-constexpr int kTsFields = 6;
+constexpr int kTsFields = 5;
 constexpr int kTsWarpBytes = kTsRing * kTsFields * S2D_STRIP_ROWS * 4;
 
 // Shared memory of one pipeline stage: 7 slots of one 128-row column each

@@ -490,11 +490,11 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_bulk(const StepArgs *__
 //   step A: p at L-1, v at L-3 (as in the one-step kernel);
 //   step B: p at L-4 (needs step-A vx at L-6 .. L-3), v at L-6 (needs step-B p
 //           at L-7 .. L-4).
-// Step-A results never reach HBM: vx in a 4-column register window, px, pz
-// and vz in per-warp shared-memory delay lines of 4 columns (each lane reads
-// back only what it wrote); the kappa, bx, bz columns step A loads wait in
-// the same delay lines for step B, so the second step reads nothing from
-// memory.  Two steps of z-halo leave lanes 2..29 valid
+// Step-A results never reach HBM: px, pz, vz and vx of step A and the
+// step-B pressure wait in per-warp shared-memory delay lines of 4 columns
+// (each lane reads back only what it wrote), which also serve as step B's
+// x-stencil windows, so the kernel fits 128 registers (4 blocks per SM);
+// kappa, bx, bz are read again for step B (L1/L2 hits: DRAM reads them once).  Two steps of z-halo leave lanes 2..29 valid
 // (rows c+8 .. c+119 of a strip starting at c = 112k - 8), so strips write
 // 112 rows; the segment's stream starts 6 columns early and ends 5 late.
 // TWO = false is the same kernel doing step A alone (odd remainders), in the
@@ -541,8 +541,6 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
     float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
     float4 zq0 = zero, zq1 = zero, zq2 = zero;
     // step B windows: step-A vx at L-6..L-3, step-B p at L-7..L-4
-    float4 wq0 = zero, wq1 = zero, wq2 = zero, wq3 = zero;
-    float4 bq0 = zero, bq1 = zero, bq2 = zero, bq3 = zero;
     const int h = TWO ? 3 : 0;  // step A runs over [xa - h, xb + h)
     const int xaa = xa - h, xba = xb + h;
     vq1 = ld4(vxi + (ptrdiff_t)(xaa - 3) * (ptrdiff_t)ld);
@@ -573,7 +571,6 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         if (TWO) {
             ring_at(ring, 0, PA, lane) = pxn;
             ring_at(ring, 1, PA, lane) = pzn;
-            ring_at(ring, 3, PA, lane) = kka;
         } else if (in_a && la.owner) {
             st4(pxo + colA, pxn);
             if (pz_live) st4(pzo + colA, pzn);
@@ -595,10 +592,8 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
             }
             continue;
         }
-        wq0 = wq1; wq1 = wq2; wq2 = wq3; wq3 = vxn;
         ring_at(ring, 2, VA, lane) = vzn;
-        ring_at(ring, 4, VA, lane) = bxa;
-        ring_at(ring, 5, VA, lane) = bza;
+        ring_at(ring, 3, VA, lane) = vxn;
         if (L < xa + 3) continue;
         // ---- step B: p at PB = L-4 ----
         const int PB = L - 4;
@@ -608,8 +603,9 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const bool colmb = xb4.x == 1.0f;
         const bool pz_liveb = !(FAST && colmb);
         float4 pxm, pzm, dxw, dzw;
-        const float4 pm = p_update(lb, S, PB, xb4, colmb, wq0, wq1, wq2, wq3, ring_at(ring, 0, PB, lane),
-                                   pz_liveb ? ring_at(ring, 1, PB, lane) : zero, ring_at(ring, 3, PB, lane), vzb,
+        const float4 pm = p_update(lb, S, PB, xb4, colmb, ring_at(ring, 3, PB - 2, lane), ring_at(ring, 3, PB - 1, lane),
+                                   ring_at(ring, 3, PB, lane), ring_at(ring, 3, PB + 1, lane), ring_at(ring, 0, PB, lane),
+                                   pz_liveb ? ring_at(ring, 1, PB, lane) : zero, ld4(kap + colB), vzb,
                                    pxm, pzm, dxw, dzw);
         const bool in_b = PB >= xa && PB < xb;
         if (in_b && la.owner) {
@@ -617,14 +613,15 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
             if (pz_liveb) st4(pzo + colB, pzm);
         }
         if (rec_b && in_b) record(lb, S, PB, pm, slot_b);
-        bq0 = bq1; bq1 = bq2; bq2 = bq3; bq3 = pm;
+        ring_at(ring, 4, PB, lane) = pm;
         if (L < xa + 6) continue;
         // ---- step B: v at VB = L-6 ----
         const int VB = L - 6;
         const ptrdiff_t colVB = (ptrdiff_t)VB * (ptrdiff_t)ld;
         float4 vxm, vzm, dxq, dzq;
-        v_update(lb, S, VB, bq0, bq1, bq2, bq3, wq0, ring_at(ring, 2, VB, lane), ring_at(ring, 4, VB, lane),
-                 ring_at(ring, 5, VB, lane), vxm, vzm, dxq, dzq);
+        v_update(lb, S, VB, ring_at(ring, 4, VB - 1, lane), ring_at(ring, 4, VB, lane), ring_at(ring, 4, VB + 1, lane),
+                 ring_at(ring, 4, VB + 2, lane), ring_at(ring, 3, VB, lane), ring_at(ring, 2, VB, lane),
+                 ld4(bxp + colVB), ld4(bzp + colVB), vxm, vzm, dxq, dzq);
         if (la.owner) {
             st4(vxo + colVB, vxm);
             st4(vzo + colVB, vzm);
@@ -633,7 +630,7 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
 }
 
 template <bool TWO>
-__global__ void __launch_bounds__(128, 3) step_kernel_ts(const StepArgs *__restrict__ A, int kt_off) {
+__global__ void __launch_bounds__(128, 4) step_kernel_ts(const StepArgs *__restrict__ A, int kt_off) {
     extern __shared__ __align__(128) unsigned char smem[];
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
