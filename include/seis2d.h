@@ -161,7 +161,7 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 (same results, a check of the fast path)
  *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
  *                 run needs (default 64)
- *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2 or 3 (default)
+ *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 (default) or 4
  *                 blocks of 128 threads per SM
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
  *                 longest that fits in free device memory (default)

@@ -96,9 +96,17 @@ __device__ __forceinline__ float4 gzt(const Lane<FAST> &ln, const float4 &m, flo
 // rows there are zero), so the reference's last-row / last-column
 // replication adds nothing.  tbx(Q-1) comes from the previous column
 // (computed at Q = xa-1 too), tbz(z-1) from the lane above.
+// Per-warp shared-memory delay lines of the adjoint step (4 columns each):
+// mvx', Lx bx mvx' and Kx kappa mPX, the inputs of its x-gathers.
+constexpr int kAdjRing = 4, kAdjFields = 3;
+constexpr int kAdjWarpBytes = kAdjRing * kAdjFields * S2D_STRIP_ROWS * 4;
+__device__ __forceinline__ float4 &adj_ring(float4 *ring, int field, int col, int lane) {
+    return ring[(field * kAdjRing + ((col + 2 * S2D_GX) & (kAdjRing - 1))) * 32 + lane];
+}
+
 template <bool FAST>
 __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
-                                             int kt, int lane) {
+                                             int kt, int lane, float4 *ring) {
     const int nnx = S.nnx;
     const size_t ld = (size_t)S.ld;
     const int xb = min(nnx, xa + seg_len);
@@ -133,9 +141,6 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const bool row0 = FAST || z0 >= 1;  // the lane's first row has a row above it in the grid
 
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 mv0 = zero, mv1 = zero, mv2 = zero, mv3 = zero;  // mvx' at L-3 .. L
-    float4 mg0 = zero, mg1 = zero, mg2 = zero, mg3 = zero;  // Lx bx mvx' at L-3 .. L
-    float4 ma0 = zero, ma1 = zero, ma2 = zero, ma3 = zero;  // Kx kappa mPX at L-4 .. L-1
     float4 tbp = zero;                                      // tbx at Q-1
 
     for (int L = xa - 3; L <= xb + 2; ++L) {
@@ -143,9 +148,9 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
             const float4 m = ld4(mvxi + colL), b = ld4(bxp + colL);
             const float lx = __ldg(S.xcoef + (L + S2D_GX)).w;
-            mv0 = mv1; mv1 = mv2; mv2 = mv3; mv3 = m;
-            mg0 = mg1; mg1 = mg2; mg2 = mg3;
-            mg3 = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z, (lx * b.w) * m.w);
+            adj_ring(ring, 0, L, lane) = m;
+            adj_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
+                                                     (lx * b.w) * m.w);
         }
         if (L < xa) continue;
         const int Q = L - 1;
@@ -181,6 +186,8 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
                        __shfl_down_sync(kFull, h.x, 1));
         {
             const float p0a = xc0p(Q - 1, nnx), p0b = xc0p(Q, nnx), p1a = xc1p(Q - 2, nnx), p1b = xc1p(Q + 1, nnx);
+            const float4 mg0 = adj_ring(ring, 1, L - 3, lane), mg1 = adj_ring(ring, 1, L - 2, lane);
+            const float4 mg2 = adj_ring(ring, 1, L - 1, lane), mg3 = adj_ring(ring, 1, L, lane);
             q.x += p0a * mg1.x - p0b * mg2.x + p1a * mg0.x - p1b * mg3.x;
             q.y += p0a * mg1.y - p0b * mg2.y + p1a * mg0.y - p1b * mg3.y;
             q.z += p0a * mg1.z - p0b * mg2.z + p1a * mg0.z - p1b * mg3.z;
@@ -219,8 +226,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             st4(gk + colQ, tk);
             if (Q == S.src_x && ln.sdz >= 0 && ln.sdz < 4) S.srcadj[kt] = comp(mPX, ln.sdz);
         }
-        ma0 = ma1; ma1 = ma2; ma2 = ma3;
-        ma3 = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
+        adj_ring(ring, 2, Q, lane) = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
                           (xq.y * kk.w) * mPX.w);
         // ---- z-velocity adjoint at Q ----
         {
@@ -234,6 +240,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         }
         // ---- buoyancy imaging at Q ----
         if (img) {
+            const float4 mv2 = adj_ring(ring, 0, Q, lane);
             const float4 tbx = make_float4((xq.w * pg.x) * mv2.x, (xq.w * pg.y) * mv2.y, (xq.w * pg.z) * mv2.z,
                                            (xq.w * pg.w) * mv2.w);
             const float4 tbz = make_float4((r0.w * ph.x) * mvz.x, (r1.w * ph.y) * mvz.y, (r2.w * ph.z) * mvz.z,
@@ -255,6 +262,9 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const ptrdiff_t colW = (ptrdiff_t)W * (ptrdiff_t)ld;
         const float dbx = __ldg(S.xcoef + (W + S2D_GX)).z;
         const float m0a = xc0m(W, nnx), m0b = xc0m(W + 1, nnx), m1a = xc1m(W - 1, nnx), m1b = xc1m(W + 2, nnx);
+        const float4 mv0 = adj_ring(ring, 0, W, lane);
+        const float4 ma0 = adj_ring(ring, 2, W - 1, lane), ma1 = adj_ring(ring, 2, W, lane);
+        const float4 ma2 = adj_ring(ring, 2, W + 1, lane), ma3 = adj_ring(ring, 2, W + 2, lane);
         float4 ovx;
         ovx.x = dbx * mv0.x + (m0a * ma1.x - m0b * ma2.x + m1a * ma0.x - m1b * ma3.x);
         ovx.y = dbx * mv0.y + (m0a * ma1.y - m0b * ma2.y + m1a * ma0.y - m1b * ma3.y);
@@ -264,10 +274,12 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     }
 }
 
-// MINB blocks of 4 warps per SM: 2 leaves the compiler its registers (no
-// spills), 3 caps them at 168 (some spills, 12 warps per SM).
+// MINB blocks of 4 warps per SM: 2 leaves the compiler its registers, 3 caps
+// them at 168 (12 warps per SM), 4 at 128 (16 warps per SM, some spills).
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kAdjWarpBytes);
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -281,9 +293,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__re
         const int c = strip * S2D_STRIP_OUT - 4;
         // the z-transposes read the coefficient pairs of rows c-2 .. c+129
         if (rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1))
-            adjoint_task<true>(a, S, strip, xa, seg_len, kt, lane);
+            adjoint_task<true>(a, S, strip, xa, seg_len, kt, lane, ring);
         else
-            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane);
+            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane, ring);
     }
 }
 
@@ -372,16 +384,21 @@ __global__ void residual_kernel(const float *seis, const float *obs, float *res,
 }  // namespace
 
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream) {
-    if (minb >= 3)
-        adjoint_kernel<3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
+    if (minb >= 4)
+        adjoint_kernel<4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (minb == 3)
+        adjoint_kernel<3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
-        adjoint_kernel<2><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        adjoint_kernel<2><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
+    const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
     return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        blocks_per_sm, minb >= 3 ? adjoint_kernel<3> : adjoint_kernel<2>, block, 0);
+        blocks_per_sm, minb >= 4 ? adjoint_kernel<4> : minb == 3 ? adjoint_kernel<3> : adjoint_kernel<2>, block,
+        smem);
 }
 
 int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,

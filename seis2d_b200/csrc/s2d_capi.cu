@@ -157,7 +157,7 @@ struct Ctx {
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
-    int opt_adj_minb = 3;     // adjoint kernel compiled for 2 or 3 blocks per SM
+    int opt_adj_minb = 3;     // adjoint kernel compiled for 2, 3 or 4 blocks per SM
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     // Launch-argument block read by every step launch, and the graphs of step
@@ -816,7 +816,7 @@ int s2d_set_option(void *ctx, const char *key, long value) {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
     } else if (k == "adjoint_blocks") {
-        if (value != 2 && value != 3) return fail(c, S2D_ERR_ARG, "adjoint_blocks must be 2 or 3");
+        if (value < 2 || value > 4) return fail(c, S2D_ERR_ARG, "adjoint_blocks must be 2, 3 or 4");
         c->opt_adj_minb = (int)value;
     } else if (k == "fast_rows") {
         c->opt_fast_rows = value ? 1 : 0;
