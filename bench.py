@@ -281,7 +281,7 @@ def extra_legs(device):
         st = derive_steps(wave)
         buf = torch.zeros(rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
         shots = [Shot(m, src[0], rec)]
-        ctx.forward(shots, wave, kt_count=60, out=buf)  # warm-up; autotunes this shape
+        ctx.forward(shots, wave, kt_count=80, out=buf)  # warm-up; autotunes this shape (>= 72 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         cells = m.padded_cells * st["fd_nt"]
         out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
@@ -320,8 +320,8 @@ def extra_legs(device):
             cells_step += 16 * mm.padded_cells
             total_rec += 16 * rec.shape[0]
         buf = torch.zeros(total_rec * st["real_nt"], dtype=torch.float32, device="cuda")
-        ctx.forward(shots, wave, kt_count=60, out=buf)
-        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=60, kt_count=300, out=buf, sync=False))
+        ctx.forward(shots, wave, kt_count=80, out=buf)  # warm-up; autotunes this shape (>= 72 steps)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=80, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
