@@ -603,6 +603,13 @@ def main():
         cpu, err = ref_cpu_rate(w)
         if cpu is None:
             cpu = {"unavailable": err}
+        else:
+            # the 1000 x 1000 case on one thread and on all host threads
+            # (bounded samples: 4 and 204 FD steps of one shot)
+            c1 = WORKLOADS["c1"]
+            one, _ = ref_cpu_rate(c1, (4, 204), threads=1)
+            allc, _ = ref_cpu_rate(c1, (4, 204))
+            cpu["c1_reference"] = {"one_thread": one, "all_threads": allc}
 
     ctx.close()
     extras = None
