@@ -333,7 +333,10 @@ def extra_legs(device):
         for mm in models:
             mm.release()
         # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
+        # checkpoint every 100 steps, as the configuration states
+        ctx.set_option("grad_segment", 100)
         out["c5_gradient"] = gradient_leg(ctx, 32, 3.0)
+        ctx.set_option("grad_segment", 0)
     return out
 
 
@@ -628,6 +631,7 @@ def main():
                        "parallelism": f"shots sharded over {world} GPU(s), no collective",
                        "launch": tune},
             "shots_per_s": value * 1e9 / (cells_shot * fd_nt),
+            "physical_gcells_per_s": value * (w["nx"] * w["nz"]) / cells_shot,
             "plain": plain, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": launches, "other_configs": extras,
         }
