@@ -283,10 +283,12 @@ def extra_legs(device):
         shots = [Shot(m, src[0], rec)]
         ctx.forward(shots, wave, kt_count=80, out=buf)  # warm-up; autotunes this shape (>= 72 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
+        l1 = ctx.last_stats
         cells = m.padded_cells * st["fd_nt"]
         out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
                      "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": ctx.last_stats.alg_bytes / t / 1e9 / peak,
-                     "note": "whole job ~37 MB of state: L2-resident"}
+                     "note": "whole job ~37 MB of state: L2-resident",
+                     "launch": {"variant": l1.variant, "seg_len": l1.seg_len}}
         m.release()
         # c3: salt 3201x1201, d 7.62, nb 50, 20 Hz, dt 0.6 ms, nt 10000, 1 shot; 1000 of the 10000 steps
         vp, rho = salt_model()
@@ -302,9 +304,10 @@ def extra_legs(device):
         cells = m.padded_cells * 1000
         rate = cells / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
+        l3 = ctx.last_stats
         out["c3"] = {"workload": "3201x1201 salt (seeded), d 7.62, nb 50, 1 shot, 1000 of 10000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (m.padded_cells * st["fd_nt"]),
-                     "roofline_frac": frac}
+                     "roofline_frac": frac, "launch": {"variant": l3.variant, "seg_len": l3.seg_len}}
         m.release()
         # c4: 48 shots on three layered models of uneven size, one launch sequence; 300 of 3000 steps
         wave = Wave(2.3996, 0.0008, 0.0008, 15.0)
@@ -324,12 +327,14 @@ def extra_legs(device):
         t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=80, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
+        l4 = ctx.last_stats
         tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
         prate = cells_step * 60 / tp / 1e9
         out["c4"] = {"workload": "48 shots on 601x301 / 1201x601 / 2401x801 layered models (16 each), nb 50, "
                                  "one launch per step for all; 300 of 3000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (cells_step / 48 * st["fd_nt"]),
-                     "plain_gcells_per_s": prate, "roofline_frac": frac}
+                     "plain_gcells_per_s": prate, "roofline_frac": frac,
+                     "launch": {"variant": l4.variant, "seg_len": l4.seg_len}}
         for mm in models:
             mm.release()
         # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
