@@ -137,16 +137,17 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 56 steps
- *                 spends 28 of them, 4 under each candidate configuration
- *                 (the results do not change: every candidate computes the same
- *                 bits), times them with events and keeps the fastest for that
- *                 shape in the context; untuned runs use variant 2, block 128,
- *                 stages 3.  0: use "variant", "block" and "stages".
+ *                 shape (models, grids, shot counts) with at least 72 steps
+ *                 spends 36 of them on 8 candidate configurations, one untimed
+ *                 and three timed launches each, in rounds (the results do not
+ *                 change: every candidate computes the same bits), times them
+ *                 with events and keeps the fastest per FD step for that shape
+ *                 in the context; runs that do not tune (shorter calls, S2D_PLAIN)
+ *                 use variant 4.  0: use "variant", "block" and "stages".
  *                 Setting any of those three turns autotuning off.
  *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline
- *                 compiled for 128 registers (default), 4 plain loads compiled
- *                 for 128 registers, 5 two FD steps per launch (the state
+ *                 compiled for 128 registers, 4 plain loads compiled for 128
+ *                 registers (default), 5 two FD steps per launch (the state
  *                 crosses HBM once per two steps; odd step counts end with one
  *                 one-step launch); s2d_gradient always runs one step per launch
  *   "block"       threads per block: 32, 64, 96 or 128 (default 128)

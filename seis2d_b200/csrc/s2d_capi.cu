@@ -134,9 +134,9 @@ struct Pool {
 
 // Launch configuration of the step kernel.
 struct LaunchCfg {
-    int variant = kVariantBulk128;
+    int variant = kVariantLdg128;  // the fastest single configuration on the c2 and c5 workloads
     int block = 128;      // threads per block (whole warps)
-    int stages = 3;       // bulk-copy ring depth per warp
+    int stages = 3;       // bulk-copy ring depth per warp (bulk-copy variants)
     size_t smem = 0;
     int grid = 0;
 };
@@ -146,7 +146,7 @@ struct Ctx {
     int sm_count = 0;
     // tuning options (s2d_set_option)
     // explicit launch configuration, used when autotuning is off
-    int opt_variant = kVariantBulk128;
+    int opt_variant = kVariantLdg128;
     int opt_block = 128;
     int opt_stages = 3;
     int opt_autotune = 1;     // time candidate configurations on a new batch shape

@@ -191,6 +191,7 @@ def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
     shot = [Shot(m, tuple(z["src"]), z["rec"])]
     base = ctx.forward(shot, _wave(c))[0]
     try:
+        ctx.set_option("variant", 2)  # the bulk-copy pipeline: ring depth and block size matter
         ctx.set_option("stages", stages)
         ctx.set_option("block", block)
         ctx.set_option("seg_len", seg_len)
