@@ -267,7 +267,7 @@ def gradient_leg(ctx, nshots=32, T=3.0):
 
 
 def extra_legs(device):
-    """Rates of the other BASELINE configurations (each a bounded part of its job)."""
+    """Rates of the other workload configurations (each a bounded part of its job)."""
     import torch
     from seis2d_b200 import Context, Shot, Wave, derive_steps
     peak, _ = measured_peak()
