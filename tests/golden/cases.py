@@ -31,6 +31,16 @@ CASES = {
     "corner_source_nb40": dict(
         nb=40, nx=120, nz=90, dx=10.0, dz=10.0, T=0.3, dt=0.001, ddt=0.001, f=12.0,
         model="gradient_anomaly", geom=("explicit", "corner")),
+    # the 7.62 m grid spacing and 0.6 ms step of the salt configuration, its
+    # 50-cell sponge, a split spread at a non-integer receiver spacing, dt_factor 2
+    "salt_grid_nb50": dict(
+        nb=50, nx=200, nz=120, dx=7.62, dz=7.62, T=0.24, dt=0.0006, ddt=0.0012, f=15.0,
+        model="gradient_anomaly", geom=("shot", [(762.0, 15.24, 81, 0, 15.24, 1)])),
+    # the 5 m spacing, 0.5 ms step, 20 Hz and 60-cell sponge of the large
+    # two-layer configuration
+    "twolayer_5m_nb60": dict(
+        nb=60, nx=180, nz=140, dx=5.0, dz=5.0, T=0.2, dt=0.0005, ddt=0.0005, f=20.0,
+        model="twolayer", geom=("shot", [(450.0, 10.0, 161, 0, 5.0, 1)])),
 }
 
 

@@ -18,7 +18,8 @@ TOL = 1e-5
 
 
 @pytest.mark.parametrize("name", ["twolayer_split_nb32", "gradient_endonleft_nb40", "edges_explicit_nb32",
-                                  "layers_endonright_near_nb32", "corner_source_nb40"])
+                                  "layers_endonright_near_nb32", "corner_source_nb40", "salt_grid_nb50",
+                                  "twolayer_5m_nb60"])
 def test_dropin_writes_the_reference_file(tmp_path, name):
     if not os.path.exists(DROPIN):
         pytest.skip("oracle/_ref/seis_dropin not built")
