@@ -69,6 +69,9 @@ extern "C" {
 
 /* flags for s2d_model_create */
 #define S2D_MODEL_DEVICE 0x1u  /* vp and rho are device pointers               */
+#define S2D_MODEL_FREE_SURFACE 0x2u /* pressure-release surface at the first model
+                                   row (job card "Free surface" : "1"), see
+                                   s2d_model_create                             */
 
 /* Source/receiver position in metres; layout of crd2d_t
  * (src/src_cpu/modelling.h:35-38). */
@@ -186,6 +189,16 @@ S2D_API int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out);
  * sponge by edge replication (cpumodelling.cpp:39-60) and forms
  * kappa = vp^2 rho and the staggered buoyancies (cpu_modelling_kernels.cpp:
  * 64-121) on the device.  Returns a model id in *model_id.
+ *
+ * S2D_MODEL_FREE_SURFACE: the first model row (padded row nb) becomes a
+ * pressure-release surface in its vacuum form: kappa is held at 0 on padded
+ * rows 0..nb, so p = 0 on the surface row and above it, a source on those rows
+ * injects nothing (its amplitude scales with kappa at the source), receivers
+ * there record 0, and s2d_gradient treats kappa on those rows as fixed.  The
+ * step kernels are unchanged.  The reference parses the job card's
+ * "Free surface" key and ignores it (src/src_cpu/json_parser.cpp:236-244; its
+ * Instructions file: "Free surface yet not implemented"), so without this
+ * flag the results are the reference's.
  */
 S2D_API int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb,
                      const float *vp, const float *rho, unsigned flags, int *model_id);
@@ -264,7 +277,8 @@ typedef struct {
     float dx, dz;
     s2d_wave wave;
     int geomflag;          /* 0: explicit geometry file, 1: shot file */
-    int frsf;              /* free-surface flag (parsed, not implemented, as in the reference) */
+    int frsf;              /* "Free surface": 1 models with S2D_MODEL_FREE_SURFACE (the
+                              reference parses the key and ignores it) */
     int fdop;              /* FD order (only 4 exists) */
     char jbtype[8];        /* "New" or "Restart" */
     char shotfile[224], geomfile[224];

@@ -103,6 +103,17 @@ static void stagger(const float *vpe, const float *rhoe, float *bue, float *bx, 
     for (int i1 = 0; i1 < nnz; i1++) bx[(size_t)(nnx - 1) * nnz + i1] = bz[(size_t)(nnx - 2) * nnz + i1];
 }
 
+/* Pressure-release (free) surface at the first model row, the vacuum form:
+ * kappa = 0 on padded rows 0..nb keeps px = pz = p = 0 there, so the
+ * surface row carries p = 0 and the rows above it are vacuum.  A source on
+ * those rows injects nothing (its amplitude scales with kappa at the source).
+ * No counterpart in the reference, which parses "Free surface" and ignores it
+ * (json_parser.cpp:236-244; Instructions: "Free surface yet not implemented"). */
+static void free_surface_rows(double *kappa, int nb, int nnz, int nnx) {
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz <= nb && iz < nnz; iz++) kappa[(size_t)iz + (size_t)ix * nnz] = 0.0;
+}
+
 /* CK:123-153: sponge at integer nodes.  spg uses the float overload of exp
  * (its argument is float), spg1 the double one. */
 static void sponge_a(float fac, float *damp, float *damp1, int nb, int n) {
@@ -343,6 +354,7 @@ int orc_forward(const orc_params *prm, int precision,
     expand(vel, vp, nb, nnz, nnx, prm->nz, prm->nx);
     expand(den, rho, nb, nnz, nnx, prm->nz, prm->nx);
     stagger(vel, den, bue, bx, bz, kappa, nnz, nnx);
+    if (prm->free_surface) free_surface_rows(kappa, nb, nnz, nnx);
 
     /* CM:233-234 (plus the one-past-the-end sample read at kt == nts, CM:136,
      * taken as 0 here) */
@@ -623,6 +635,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
     expand(vel, vp, nb, nnz, nnx, prm->nz, prm->nx);
     expand(den, rho, nb, nnz, nnx, prm->nz, prm->nx);
     stagger(vel, den, bue, bx, bz, kappa, nnz, nnx);
+    if (prm->free_surface) free_surface_rows(kappa, nb, nnz, nnx);
     int nw = wavelet ? nwav : d.nts;
     double *w = calloc((size_t)(nw > 0 ? nw : 0) + 1, sizeof(double));
     if (wavelet) memcpy(w, wavelet, (size_t)nw * sizeof(double));
@@ -730,6 +743,11 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
         memcpy(mvz, nvz, N * 8);
     }
     gk[isrc] += gk_src;
+    /* with a free surface kappa is held at 0 on rows 0..nb: not a function of
+     * vp or rho there */
+    if (prm->free_surface)
+        for (int ix = 0; ix < nnx; ix++)
+            for (int iz = 0; iz <= nb && iz < nnz; iz++) gk[(size_t)iz + (size_t)ix * nnz] = 0.0;
     if (grad_kappa) memcpy(grad_kappa, gk, N * 8);
     if (grad_bx) memcpy(grad_bx, gbx, N * 8);
     if (grad_bz) memcpy(grad_bz, gbz, N * 8);

@@ -33,6 +33,11 @@ typedef struct {
     float fd_dt;       /* "FD DT"     seconds */
     float real_dt;     /* "DATA DT"   seconds */
     float fm;          /* "Frequency" Hz */
+    int free_surface;  /* "Free surface" 1: pressure-release surface at the
+                          first model row (kappa = 0 on padded rows 0..nb).
+                          The reference parses this key and ignores it
+                          (src/src_cpu/json_parser.cpp:236-244); 0 keeps
+                          the reference's behaviour. */
 } orc_params;
 
 typedef struct {

@@ -103,16 +103,21 @@ class Context:
         """Step-kernel tuning knob (see s2d_set_option in include/seis2d.h)."""
         self._check(L.lib().s2d_set_option(self._h, key.encode(), int(value)))
 
-    def model(self, vp, rho, dx: float, dz: float, nb: int = 32) -> Model:
-        """Upload a ``[nx][nz]`` model (numpy or CUDA tensor, float32)."""
-        flags = 0
+    def model(self, vp, rho, dx: float, dz: float, nb: int = 32, free_surface: bool = False) -> Model:
+        """Upload a ``[nx][nz]`` model (numpy or CUDA tensor, float32).
+
+        ``free_surface``: the first model row is a pressure-release surface
+        (kappa held at 0 on it and on the sponge rows above it), what the job
+        card's ``"Free surface" : "1"`` asks for; the reference parses that key
+        and ignores it, so the default keeps its results."""
+        flags = L.S2D_MODEL_FREE_SURFACE if free_surface else 0
         if _is_torch(vp):
             import torch
             assert vp.is_cuda and rho.is_cuda and vp.dtype == torch.float32 and rho.dtype == torch.float32
             vp, rho = vp.contiguous(), rho.contiguous()
             nx, nz = vp.shape
             pv, pr = C.c_void_p(vp.data_ptr()), C.c_void_p(rho.data_ptr())
-            flags = L.S2D_MODEL_DEVICE
+            flags |= L.S2D_MODEL_DEVICE
             keep = (vp, rho)
         else:
             vp = np.ascontiguousarray(vp, np.float32)
@@ -265,12 +270,12 @@ Context.gradient = _gradient
 
 def modelling_module(vp: np.ndarray, rho: np.ndarray, dx: float, dz: float, wave: Wave,
                      geometry: Sequence[Tuple[Tuple[float, float], np.ndarray]], nb: int = 32,
-                     device: int = 0, plain: bool = False) -> List[np.ndarray]:
+                     device: int = 0, plain: bool = False, free_surface: bool = False) -> List[np.ndarray]:
     """The reference seam with explicit arguments: every shot of
     ``geometry`` = ``[((sx, sz), rec_xz), ...]`` on one model, returning the
     per-shot ``[nrec][real_nt]`` seismograms the reference writes to disk
     (src/src_cpu/cpumodelling.cpp:158-383)."""
     with Context(device) as ctx:
-        m = ctx.model(vp, rho, dx, dz, nb)
+        m = ctx.model(vp, rho, dx, dz, nb, free_surface=free_surface)
         shots = [Shot(m, src, np.asarray(rec, np.float32)) for src, rec in geometry]
         return [s.copy() for s in ctx.forward(shots, wave, plain=plain)]

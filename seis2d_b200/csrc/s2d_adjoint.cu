@@ -327,18 +327,20 @@ __global__ void sum_shots(float *const *gk, float *const *gb, int nshots, int nn
 }
 
 // kappa = vp^2 rho and b = 1/rho (the buoyancy averages are folded into dJ/db
-// by the adjoint step).
+// by the adjoint step).  Rows z < kfix hold kappa at 0 (free surface): their
+// dJ/dkappa does not depend on vp or rho.
 __global__ void chain_rule(const float *tk, const float *tb, const float *vp, const float *rho, int nx, int nz,
-                           int nb, int ld, float *gvp, float *grho) {
+                           int nb, int ld, int kfix, float *gvp, float *grho) {
     const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
     const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
     if (z >= nnz || x >= nnx) return;
     const size_t id = pad_id(x, z, ld);
     const double gb = tb[id];
+    const double gk = z < kfix ? 0.0 : (double)tk[id];
     const int mx = min(max(x - nb, 0), nx - 1), mz = min(max(z - nb, 0), nz - 1);
     const double v = vp[(size_t)mx * nz + mz], r = rho[(size_t)mx * nz + mz];
-    gvp[id] = (float)(2.0 * v * r * (double)tk[id]);
-    grho[id] = (float)(v * v * (double)tk[id] + (r > 0 ? -gb / (r * r) : 0.0));
+    gvp[id] = (float)(2.0 * v * r * gk);
+    grho[id] = (float)(v * v * gk + (r > 0 ? -gb / (r * r) : 0.0));
 }
 
 // Fold the sponge onto the model cells it replicates (transpose of
@@ -403,15 +405,15 @@ int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
 
 int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
                              const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
-                             int ld, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
-                             void *stream) {
+                             int ld, int kappa_fixed_rows, float *tmp2, float *gvp_pad, float *grho_pad,
+                             float *grad_vp, float *grad_rho, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const int nnx = nx + 2 * nb, nnz = nz + 2 * nb;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
     add_source_terms<<<1, 1, 0, st>>>(gk, src_cells, src_vals, nshots);
     dim3 blk(256), grd((nnz + 255) / 256, nnx);
     sum_shots<<<grd, blk, 0, st>>>(gk, gb, nshots, nnx, nnz, ld, tmp2, tmp2 + F);
-    chain_rule<<<grd, blk, 0, st>>>(tmp2, tmp2 + F, vp, rho, nx, nz, nb, ld, gvp_pad, grho_pad);
+    chain_rule<<<grd, blk, 0, st>>>(tmp2, tmp2 + F, vp, rho, nx, nz, nb, ld, kappa_fixed_rows, gvp_pad, grho_pad);
     dim3 grd2((nz + 255) / 256, nx);
     fold_sponge<<<grd2, blk, 0, st>>>(gvp_pad, grho_pad, nx, nz, nb, ld, grad_vp, grad_rho);
     return (int)cudaGetLastError();

@@ -51,6 +51,7 @@ struct DevBuf {
 struct Model {
     int nx = 0, nz = 0, nb = 0, nnx = 0, nnz = 0, ld = 0, nxa = 0;
     float dx = 0, dz = 0;
+    bool free_surface = false;  // kappa held at 0 on padded rows 0..nb (S2D_MODEL_FREE_SURFACE)
     size_t field_elems = 0;  // nxa * ld
     DevBuf vp, rho;          // raw [nx][nz] copies (source amplitude needs vp, rho at the source)
     DevBuf mat;              // kappa, bx, bz in one allocation, field_elems apart (padded layout)
@@ -555,7 +556,8 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         float vr[2];
         CK(cudaMemcpy(&vr[0], m.vp.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(&vr[1], m.rho.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
-        const double ksrc = ((double)vr[0] * (double)vr[0]) * (double)vr[1];
+        // a source on the free surface or above it (kappa held at 0) injects nothing
+        const double ksrc = m.free_surface && h.src_z <= m.nb ? 0.0 : ((double)vr[0] * (double)vr[0]) * (double)vr[1];
         const float dxdz = m.dx * m.dz;
         std::vector<float> amp(rs.fd_nt, 0.0f);
         for (int kt = 0; kt < rs.fd_nt && kt <= inject_last; ++kt) {
@@ -929,6 +931,13 @@ int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, cons
     int e = launch_prepare_model(m->vp.as<float>(), m->rho.as<float>(), nx, nz, nb, m->ld, m->kappa(), bue.as<float>(),
                                  m->bx(), m->bz(), c->stream);
     if (e) return fail(c, S2D_ERR_CUDA, "prepare_model: %s", cudaGetErrorString((cudaError_t)e));
+    if (flags & S2D_MODEL_FREE_SURFACE) {
+        // vacuum form of a pressure-release surface: kappa = 0 on padded rows
+        // 0..nb of every column, so p stays 0 on the surface row and above it
+        m->free_surface = true;
+        CK(cudaMemset2DAsync(m->kappa() + (size_t)S2D_GX * m->ld + S2D_GZ, sizeof(float) * m->ld, 0,
+                             sizeof(float) * (nb + 1), m->nnx, c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
     sponge_a(nb, nx, m->damp2a, m->damp2a1);
     sponge_b(nb, nx, m->damp2b, m->damp2b1);
@@ -1394,7 +1403,9 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         float vr[2];
         CK(cudaMemcpy(&vr[0], m.vp.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(&vr[1], m.rho.as<float>() + (size_t)mx * m.nz + mz, sizeof(float), cudaMemcpyDeviceToHost));
-        const double ksrc = ((double)vr[0] * (double)vr[0]) * (double)vr[1];
+        const double ksrc = m.free_surface && b.shots[s].src_z <= m.nb
+                                ? 0.0
+                                : ((double)vr[0] * (double)vr[0]) * (double)vr[1];
         double v = 0;
         for (int kt = 0; kt < rs.fd_nt; ++kt) {
             const bool injected = kt <= inject_last;
@@ -1429,6 +1440,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         int e = launch_gradient_finalize(dptrs, dptrs + nshots, nshots,
                                          static_cast<int *>(p_cells), static_cast<double *>(p_vals),
                                          m.vp.as<float>(), m.rho.as<float>(), m.nx, m.nz, m.nb, m.ld,
+                                         m.free_surface ? m.nb + 1 : 0,
                                          static_cast<float *>(p_tmp), static_cast<float *>(p_pad),
                                          static_cast<float *>(p_pad) + F, out_vp, out_rho, c->stream);
         if (e) return fail(c, S2D_ERR_CUDA, "gradient finalize: %s", cudaGetErrorString((cudaError_t)e));

@@ -519,7 +519,10 @@ int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, int namin
         return say(eb, el, e, "no usable CUDA device %d", device);
     }
     int mid = 0;
-    e = s2d_model_create(ctx, J.nx, J.nz, J.dx, J.dz, nb, vp.data(), rho.data(), 0, &mid);
+    // "Free surface" : "1" (parsed and ignored by the reference) turns the
+    // first model row into a pressure-release surface
+    e = s2d_model_create(ctx, J.nx, J.nz, J.dx, J.dz, nb, vp.data(), rho.data(),
+                         J.frsf ? S2D_MODEL_FREE_SURFACE : 0u, &mid);
     s2d_steps st;
     if (!e) e = s2d_derive_steps(&J.wave, &st);
     // shots per batch: what fits in free device memory (8 wavefield buffers per shot)

@@ -147,10 +147,12 @@ int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream);
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm);
 // Sum the shots' accumulators (dJ/dkappa, dJ/db), apply the kappa = vp^2 rho,
-// b = 1/rho chain rule and fold the sponge onto the model.
+// b = 1/rho chain rule and fold the sponge onto the model.  kappa_fixed_rows:
+// padded rows [0, kappa_fixed_rows) whose kappa is held at 0 (free surface),
+// so their dJ/dkappa does not reach vp or rho.
 int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
                              const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
-                             int ld, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
+                             int ld, int kappa_fixed_rows, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
                              void *stream);
 // Residual d - d_obs in place of d_obs... : res[i] = seis[i] - obs[i]; partial sums of res^2.
 int launch_residual(const float *seis, const float *obs, float *res, size_t n, double *sumsq, void *stream);

@@ -58,7 +58,11 @@ void modelling_module(int my_nsrc, geo2d_t *g) {
         std::memcpy(&rho[(size_t)ix * nz], mod_sp->rho2d[ix], sizeof(float) * nz);
     }
     int model = 0;
-    if (s2d_model_create(ctx, nx, nz, mod_sp->dx, mod_sp->dz, nb, vp.data(), rho.data(), 0, &model) != S2D_OK)
+    // job_sp->frsf ("Free surface", json_parser.cpp:236-244) is parsed and
+    // ignored by the reference's modelling; here 1 gives a pressure-release
+    // surface at the first model row
+    const unsigned mflags = job_sp->frsf ? S2D_MODEL_FREE_SURFACE : 0u;
+    if (s2d_model_create(ctx, nx, nz, mod_sp->dx, mod_sp->dz, nb, vp.data(), rho.data(), mflags, &model) != S2D_OK)
         die(ctx, "model");
 
     s2d_wave w;  // the fields of wave_t (modelling.h:27-31)
