@@ -337,6 +337,25 @@ def extra_legs(device):
                      "launch": {"variant": l4.variant, "seg_len": l4.seg_len}}
         for mm in models:
             mm.release()
+        # the 8th-order operator ("Order of FD Operator" : "8") on the 5000x5000
+        # two-layer model: 16 of its 64 shots, 200 steps after a warm-up that
+        # autotunes the shape (same algorithmic bytes per cell as order 4)
+        w2 = WORKLOADS["c2"]
+        vp, rho, src2, rec2 = build_workload(w2)
+        m = ctx.model(vp, rho, w2["d"], w2["d"], w2["nb"], fd_order=8)
+        wave = Wave(w2["T"], w2["dt"], w2["dt"], w2["f"])
+        st = derive_steps(wave)
+        shots = [Shot(m, s_, rec2) for s_ in src2[:16]]
+        buf = torch.zeros(16 * rec2.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
+        ctx.forward(shots, wave, kt_count=40, out=buf)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=40, kt_count=200, out=buf, sync=False))
+        l8 = ctx.last_stats
+        rate = 16 * m.padded_cells * 200 / t / 1e9
+        out["c2_order8"] = {"workload": "5000x5000 two-layer, nb 60, 8th-order operator, 16 shots x 5000 receivers; "
+                                        "200 of 4000 steps",
+                            "gcells_per_s": rate, "roofline_frac": l8.alg_bytes / t / 1e9 / peak,
+                            "launch": {"variant": l8.variant, "seg_len": l8.seg_len}}
+        m.release()
         # c5: FWI gradient, 32 shots, 1201x401, nb 50, 10 Hz, dt 1 ms, nt 3000
         # checkpoint every 100 steps, as the configuration states
         ctx.set_option("grad_segment", 100)

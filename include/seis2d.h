@@ -72,6 +72,8 @@ extern "C" {
 #define S2D_MODEL_FREE_SURFACE 0x2u /* pressure-release surface at the first model
                                    row (job card "Free surface" : "1"), see
                                    s2d_model_create                             */
+#define S2D_MODEL_ORDER8 0x4u  /* 8th-order FD operator (job card "Order of FD
+                                  Operator" : "8"), see s2d_model_create       */
 
 /* Source/receiver position in metres; layout of crd2d_t
  * (src/src_cpu/modelling.h:35-38). */
@@ -199,6 +201,16 @@ S2D_API int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out);
  * "Free surface" key and ignores it (src/src_cpu/json_parser.cpp:236-244; its
  * Instructions file: "Free surface yet not implemented"), so without this
  * flag the results are the reference's.
+ *
+ * S2D_MODEL_ORDER8: shots on this model run the staggered 8th-order operator
+ * D- f[i] = sum_k c_k (f[i+k-1] - f[i-k]), D+ f[i] = sum_k c_k (f[i+k] - f[i-k+1]),
+ * c = (1225/1024, -245/3072, 49/5120, -5/7168) in float, with the reference's
+ * 4th-order pair, plain difference and zero row where the 8 taps would leave
+ * the grid; sponge, source and receivers as for order 4.  The reference
+ * parses "Order of FD Operator" and steps only for 4 (cpumodelling.cpp:121).
+ * All shots of one s2d_forward call must share the order; s2d_gradient
+ * rejects order-8 models.  Stable for vmax dt / min(dx, dz) <= 0.549 (0.606
+ * for order 4).
  */
 S2D_API int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb,
                      const float *vp, const float *rho, unsigned flags, int *model_id);
@@ -305,7 +317,9 @@ S2D_API int s2d_geometry_read(const s2d_jobcard *job, s2d_geometry *out, char *e
 S2D_API void s2d_geometry_free(s2d_geometry *geometry);
 
 /* Stability (dt <= 0.606 h_min / v_max) and dispersion (2 f <= v_min / (5 h_max))
- * criteria of check_stability.cpp:8-72.  Host only. */
+ * criteria of check_stability.cpp:8-72.  Host only.  For job->fdop == 8 the
+ * stability bound is 0.549 h_min / v_max (the 8th-order operator; no
+ * counterpart in the reference). */
 S2D_API int s2d_check_stability(const s2d_jobcard *job, float vmin, float vmax, char *errbuf, size_t errlen);
 
 /*

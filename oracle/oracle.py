@@ -26,7 +26,7 @@ class _Params(C.Structure):
     _fields_ = [("nx", C.c_int), ("nz", C.c_int), ("nb", C.c_int),
                 ("dx", C.c_float), ("dz", C.c_float), ("rec_len", C.c_float),
                 ("fd_dt", C.c_float), ("real_dt", C.c_float), ("fm", C.c_float),
-                ("free_surface", C.c_int)]
+                ("free_surface", C.c_int), ("fd_order", C.c_int)]
 
 
 class _Derived(C.Structure):
@@ -82,10 +82,11 @@ class Params:
     real_dt: float
     fm: float
     free_surface: int = 0  # 1: pressure-release surface at the first model row
+    fd_order: int = 4      # 4: the reference's operator; 8: the 8th-order operator
 
     def c(self) -> _Params:
         return _Params(self.nx, self.nz, self.nb, self.dx, self.dz, self.rec_len,
-                       self.fd_dt, self.real_dt, self.fm, int(self.free_surface))
+                       self.fd_dt, self.real_dt, self.fm, int(self.free_surface), int(self.fd_order))
 
 
 def derive(p: Params) -> dict:

@@ -328,6 +328,129 @@ static void f32_step(f32_state *s, int isrc, float src_add, int inject) {
 }
 #undef AT
 
+/* ------------- 8th-order operator (no counterpart in the reference) -------
+ *
+ * "Order of FD Operator" = 8.  The reference parses the key and runs its step
+ * only for 4 (cpumodelling.cpp:121, `if (NJ == 4)`), so this is new
+ * capability with no reference output.  Staggered-grid 8th-order Taylor
+ * coefficients (c1..c4 = 1225/1024, -245/3072, 49/5120, -5/7168, rounded to
+ * float), in the forms
+ *   D- f[i] = sum_k c_k (f[i+k-1] - f[i-k])     (taps i-4 .. i+3)
+ *   D+ f[i] = sum_k c_k (f[i+k] - f[i-k+1])     (taps i-3 .. i+4)
+ * Rows whose taps would leave the grid fall back to the reference's operator:
+ * its 4th-order pair (a0, a1), its plain difference, its zero row. */
+static const float ORC_C81 = 1225.0f / 1024.0f;
+static const float ORC_C82 = -245.0f / 3072.0f;
+static const float ORC_C83 = 49.0f / 5120.0f;
+static const float ORC_C84 = -5.0f / 7168.0f;
+
+static inline void dm8_coef(int i, int n, float c[4]) { /* D-: 8th on [4, n-4], then the reference's rows */
+    if (i >= 4 && i <= n - 4) { c[0] = ORC_C81; c[1] = ORC_C82; c[2] = ORC_C83; c[3] = ORC_C84; return; }
+    c[2] = c[3] = 0.0f;
+    dm_coef(i, n, &c[0], &c[1]);
+}
+static inline void dp8_coef(int i, int n, float c[4]) { /* D+: 8th on [3, n-5], then the reference's rows */
+    if (i >= 3 && i <= n - 5) { c[0] = ORC_C81; c[1] = ORC_C82; c[2] = ORC_C83; c[3] = ORC_C84; return; }
+    c[2] = c[3] = 0.0f;
+    dp_coef(i, n, &c[0], &c[1]);
+}
+
+/* FP64 step, split fields everywhere as the reference's FP64 path (CM:115-156
+ * with the 8th-order operators). */
+static void f64_step8(f64_state *s, int isrc, double src_add, int inject) {
+    const int nnz = s->nnz, nnx = s->nnx;
+#define AT64(a, ix, iz) ((ix) < 0 || (ix) >= nnx || (iz) < 0 || (iz) >= nnz ? 0.0 : (a)[(size_t)(ix) * nnz + (iz)])
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx[4];
+        dm8_coef(ix, nnx, cx);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz[4];
+            dm8_coef(iz, nnz, cz);
+            double dvx = 0.0, dvz = 0.0;
+            for (int k = 0; k < 4; k++) {
+                dvx += (double)cx[k] * (AT64(s->vx, ix + k, iz) - AT64(s->vx, ix - 1 - k, iz));
+                dvz += (double)cz[k] * (AT64(s->vz, ix, iz + k) - AT64(s->vz, ix, iz - 1 - k));
+            }
+            size_t id = (size_t)ix * nnz + iz;
+            s->px[id] = s->damp2a[ix] * s->px[id] + s->kw2[id] * dvx;
+            s->pz[id] = s->damp1a[iz] * s->pz[id] + s->kw1[id] * dvz;
+        }
+    }
+    if (inject) s->px[isrc] = s->px[isrc] + src_add;
+    for (size_t id = 0; id < s->N; id++) s->p[id] = s->px[id] + s->pz[id];
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx[4];
+        dp8_coef(ix, nnx, cx);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz[4];
+            dp8_coef(iz, nnz, cz);
+            double dpx = 0.0, dpz = 0.0;
+            for (int k = 0; k < 4; k++) {
+                dpx += (double)cx[k] * (AT64(s->p, ix + 1 + k, iz) - AT64(s->p, ix - k, iz));
+                dpz += (double)cz[k] * (AT64(s->p, ix, iz + 1 + k) - AT64(s->p, ix, iz - k));
+            }
+            size_t id = (size_t)ix * nnz + iz;
+            s->vx[id] = s->damp2b[ix] * s->vx[id] + s->bw2[id] * dpx;
+            s->vz[id] = s->damp1b[iz] * s->vz[id] + s->bw1[id] * dpz;
+        }
+    }
+#undef AT64
+}
+
+/* FP32 step with the CUDA kernel's rounding: every derivative
+ * fma(c1, d1, fma(c2, d2, fma(c3, d3, c4*d4))), every update
+ * fma(damping, field, (coefficient * material) * derivative), merged cells
+ * (both pressure dampings 1) carrying p alone as in f32_step. */
+#define AT(a, ix, iz) ((ix) < 0 || (ix) >= nnx || (iz) < 0 || (iz) >= nnz ? 0.0f : (a)[(size_t)(ix) * nnz + (iz)])
+static inline float dif8(const float c[4], float d1, float d2, float d3, float d4) {
+    return fmaf(c[0], d1, fmaf(c[1], d2, fmaf(c[2], d3, c[3] * d4)));
+}
+static void f32_step8(f32_state *s, int isrc, float src_add, int inject) {
+    const int nnz = s->nnz, nnx = s->nnx;
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx[4];
+        dm8_coef(ix, nnx, cx);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz[4];
+            dm8_coef(iz, nnz, cz);
+            size_t id = (size_t)ix * nnz + iz;
+            const float *vx = s->vx, *vz = s->vz;
+            float dvx = dif8(cx, AT(vx, ix, iz) - AT(vx, ix - 1, iz), AT(vx, ix + 1, iz) - AT(vx, ix - 2, iz),
+                             AT(vx, ix + 2, iz) - AT(vx, ix - 3, iz), AT(vx, ix + 3, iz) - AT(vx, ix - 4, iz));
+            float dvz = dif8(cz, AT(vz, ix, iz) - AT(vz, ix, iz - 1), AT(vz, ix, iz + 1) - AT(vz, ix, iz - 2),
+                             AT(vz, ix, iz + 2) - AT(vz, ix, iz - 3), AT(vz, ix, iz + 3) - AT(vz, ix, iz - 4));
+            float k = s->kappa[id];
+            if (s->damp2a[ix] == 1.0f && s->damp1a[iz] == 1.0f) {
+                float t = fmaf(s->kxa[ix], dvx, s->kza[iz] * dvz);
+                s->px[id] = fmaf(k, t, s->px[id]);
+                s->pz[id] = 0.0f;
+            } else {
+                s->px[id] = fmaf(s->damp2a[ix], s->px[id], (s->kxa[ix] * k) * dvx);
+                s->pz[id] = fmaf(s->damp1a[iz], s->pz[id], (s->kza[iz] * k) * dvz);
+            }
+        }
+    }
+    if (inject) s->px[isrc] = s->px[isrc] + src_add;
+    for (size_t id = 0; id < s->N; id++) s->p[id] = s->px[id] + s->pz[id];
+    for (int ix = 0; ix < nnx; ix++) {
+        float cx[4];
+        dp8_coef(ix, nnx, cx);
+        for (int iz = 0; iz < nnz; iz++) {
+            float cz[4];
+            dp8_coef(iz, nnz, cz);
+            size_t id = (size_t)ix * nnz + iz;
+            const float *p = s->p;
+            float dpx = dif8(cx, AT(p, ix + 1, iz) - AT(p, ix, iz), AT(p, ix + 2, iz) - AT(p, ix - 1, iz),
+                             AT(p, ix + 3, iz) - AT(p, ix - 2, iz), AT(p, ix + 4, iz) - AT(p, ix - 3, iz));
+            float dpz = dif8(cz, AT(p, ix, iz + 1) - AT(p, ix, iz), AT(p, ix, iz + 2) - AT(p, ix, iz - 1),
+                             AT(p, ix, iz + 3) - AT(p, ix, iz - 2), AT(p, ix, iz + 4) - AT(p, ix, iz - 3));
+            s->vx[id] = fmaf(s->damp2b[ix], s->vx[id], (s->kxb[ix] * s->bx[id]) * dpx);
+            s->vz[id] = fmaf(s->damp1b[iz], s->vz[id], (s->kzb[iz] * s->bz[id]) * dpz);
+        }
+    }
+}
+#undef AT
+
 /* ------------------------------ driver ---------------------------------- */
 
 int orc_forward(const orc_params *prm, int precision,
@@ -338,6 +461,8 @@ int orc_forward(const orc_params *prm, int precision,
     if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz || !seis))) return -1;
     if (prm->nx < 1 || prm->nz < 1 || prm->nb < 2) return -1;
     if (precision != ORC_F64 && precision != ORC_F32) return -1;
+    if (prm->fd_order != 0 && prm->fd_order != 4 && prm->fd_order != 8) return -1;
+    const int o8 = prm->fd_order == 8;
     orc_derived d;
     orc_derive(prm, &d);
     if (d.dt_factor < 1 || d.fd_nt < 1) return -2;
@@ -406,7 +531,8 @@ int orc_forward(const orc_params *prm, int precision,
             /* CM:136-140 */
             double wk = kt < nw ? w[kt] : 0.0;
             double add = prm->fd_dt * wk * kappa[isrc] / (dxdz);
-            f64_step(&s, isrc, add, kt <= d.nts);
+            if (o8) f64_step8(&s, isrc, add, kt <= d.nts);
+            else f64_step(&s, isrc, add, kt <= d.nts);
             /* CM:356-360 */
             if ((kt + 1) % d.dt_factor == 0) {
                 int it = (kt + 1) / d.dt_factor - 1;
@@ -437,7 +563,8 @@ int orc_forward(const orc_params *prm, int precision,
         for (int kt = 0; kt < nsteps; kt++) {
             double wk = kt < nw ? w[kt] : 0.0;
             float add = (float)(prm->fd_dt * wk * kappa[isrc] / (dxdz));
-            f32_step(&s, isrc, add, kt <= d.nts);
+            if (o8) f32_step8(&s, isrc, add, kt <= d.nts);
+            else f32_step(&s, isrc, add, kt <= d.nts);
             if ((kt + 1) % d.dt_factor == 0) {
                 int it = (kt + 1) / d.dt_factor - 1;
                 if (it < d.real_nt)
@@ -624,6 +751,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                  double *grad_kappa, double *grad_bx, double *grad_bz,
                  double *src_adj, double *seis64) {
     if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz))) return -1;
+    if (prm->fd_order != 0 && prm->fd_order != 4) return -4; /* the adjoint of the 4th-order scheme only */
     orc_derived d;
     orc_derive(prm, &d);
     if (d.dt_factor < 1 || d.fd_nt < 1) return -2;

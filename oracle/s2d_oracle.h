@@ -38,6 +38,11 @@ typedef struct {
                           The reference parses this key and ignores it
                           (src/src_cpu/json_parser.cpp:236-244); 0 keeps
                           the reference's behaviour. */
+    int fd_order;      /* "Order of FD Operator": 0 or 4 the reference's
+                          4th-order operator (cpumodelling.cpp:121, NJ == 4);
+                          8 the 8th-order staggered operator of this project
+                          (the reference runs no step for NJ != 4).  The
+                          gradient supports order 4 only. */
 } orc_params;
 
 typedef struct {

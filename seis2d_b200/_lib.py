@@ -31,6 +31,7 @@ S2D_NO_GRAPH = 0x4
 S2D_SYNC = 0x8
 S2D_MODEL_DEVICE = 0x1
 S2D_MODEL_FREE_SURFACE = 0x2
+S2D_MODEL_ORDER8 = 0x4
 S2D_GRAD_MISFIT = 0x10
 S2D_GRAD_DEVICE = 0x20
 

@@ -103,14 +103,22 @@ class Context:
         """Step-kernel tuning knob (see s2d_set_option in include/seis2d.h)."""
         self._check(L.lib().s2d_set_option(self._h, key.encode(), int(value)))
 
-    def model(self, vp, rho, dx: float, dz: float, nb: int = 32, free_surface: bool = False) -> Model:
+    def model(self, vp, rho, dx: float, dz: float, nb: int = 32, free_surface: bool = False,
+              fd_order: int = 4) -> Model:
         """Upload a ``[nx][nz]`` model (numpy or CUDA tensor, float32).
 
         ``free_surface``: the first model row is a pressure-release surface
         (kappa held at 0 on it and on the sponge rows above it), what the job
         card's ``"Free surface" : "1"`` asks for; the reference parses that key
-        and ignores it, so the default keeps its results."""
+        and ignores it, so the default keeps its results.
+        ``fd_order``: 4 (the reference's operator) or 8 (the staggered
+        8th-order operator, job card ``"Order of FD Operator" : "8"``, which
+        the reference parses and never runs); shots of one call share it."""
+        if fd_order not in (4, 8):
+            raise ValueError("fd_order must be 4 or 8")
         flags = L.S2D_MODEL_FREE_SURFACE if free_surface else 0
+        if fd_order == 8:
+            flags |= L.S2D_MODEL_ORDER8
         if _is_torch(vp):
             import torch
             assert vp.is_cuda and rho.is_cuda and vp.dtype == torch.float32 and rho.dtype == torch.float32
@@ -270,12 +278,13 @@ Context.gradient = _gradient
 
 def modelling_module(vp: np.ndarray, rho: np.ndarray, dx: float, dz: float, wave: Wave,
                      geometry: Sequence[Tuple[Tuple[float, float], np.ndarray]], nb: int = 32,
-                     device: int = 0, plain: bool = False, free_surface: bool = False) -> List[np.ndarray]:
+                     device: int = 0, plain: bool = False, free_surface: bool = False,
+                     fd_order: int = 4) -> List[np.ndarray]:
     """The reference seam with explicit arguments: every shot of
     ``geometry`` = ``[((sx, sz), rec_xz), ...]`` on one model, returning the
     per-shot ``[nrec][real_nt]`` seismograms the reference writes to disk
     (src/src_cpu/cpumodelling.cpp:158-383)."""
     with Context(device) as ctx:
-        m = ctx.model(vp, rho, dx, dz, nb, free_surface=free_surface)
+        m = ctx.model(vp, rho, dx, dz, nb, free_surface=free_surface, fd_order=fd_order)
         shots = [Shot(m, src, np.asarray(rec, np.float32)) for src, rec in geometry]
         return [s.copy() for s in ctx.forward(shots, wave, plain=plain)]

@@ -52,6 +52,7 @@ struct Model {
     int nx = 0, nz = 0, nb = 0, nnx = 0, nnz = 0, ld = 0, nxa = 0;
     float dx = 0, dz = 0;
     bool free_surface = false;  // kappa held at 0 on padded rows 0..nb (S2D_MODEL_FREE_SURFACE)
+    int fd_order = 4;            // 8 with S2D_MODEL_ORDER8
     size_t field_elems = 0;  // nxa * ld
     DevBuf vp, rho;          // raw [nx][nz] copies (source amplitude needs vp, rho at the source)
     DevBuf mat;              // kappa, bx, bz in one allocation, field_elems apart (padded layout)
@@ -83,6 +84,7 @@ struct ShotHost {
 struct Batch {
     int nshots = 0;
     bool plain = false;
+    bool order8 = false;             // every shot's model has the 8th-order operator
     RunSteps steps{};
     int kt_next = 0;
     std::vector<ShotHost> shots;
@@ -258,7 +260,7 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
     lc.variant = variant;
     lc.block = std::max(32, std::min(128, block / 32 * 32));
     lc.stages = std::max(2, std::min(16, stages));
-    const bool ldg = lc.variant == kVariantLdg || lc.variant == kVariantLdgProducts || lc.variant == kVariantLdg128;
+    const bool ldg = plain_loads(lc.variant);
     const bool ts = ts_layout(lc.variant);
     if (ldg || ts) {
         lc.block = 128;
@@ -283,7 +285,7 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
 // Key of a batch's shape for the autotuner: run mode and, per model group,
 // padded grid and shot count.
 std::vector<long> tune_key(const Ctx *c, const Batch &b) {
-    std::vector<long> k = {b.plain ? 1L : 0L, (long)c->sm_count};
+    std::vector<long> k = {b.plain ? 1L : 0L, (long)c->sm_count, b.order8 ? 8L : 4L};
     for (size_t g = 0; g < b.groups.size(); ++g) {
         k.push_back(b.group_nnx[g]);
         k.push_back(b.group_nnz[g]);
@@ -297,6 +299,8 @@ std::vector<long> tune_key(const Ctx *c, const Batch &b) {
 // shape, else the built-in default.
 int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
     if (tuned) *tuned = false;
+    // 8th-order batches run the 8th-order kernel whatever the options say
+    if (b.order8 && !c->opt_autotune) return launch_config(c, b.max_tasks, out, kVariantO8, 128, 0);
     if (!c->opt_autotune) return launch_config(c, b.max_tasks, out, c->opt_variant, c->opt_block, c->opt_stages);
     auto it = c->tuned.find(tune_key(c, b));
     if (it != c->tuned.end()) {
@@ -304,7 +308,7 @@ int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
         return launch_config(c, b.max_tasks, out, it->second[0], it->second[1], it->second[2]);
     }
     const LaunchCfg d;
-    return launch_config(c, b.max_tasks, out, d.variant, d.block, d.stages);
+    return launch_config(c, b.max_tasks, out, b.order8 ? kVariantO8 : d.variant, d.block, b.order8 ? 0 : d.stages);
 }
 
 // Segment lengths, segment counts and task ranges of the batch's groups for
@@ -472,6 +476,11 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             return fail(c, S2D_ERR_ARG, "shot %d: bad receiver list", s);
     }
     const Model &m0 = *c->models[shots[0].model_id];
+    for (int s = 1; s < nshots; ++s)
+        if (c->models[shots[s].model_id]->fd_order != m0.fd_order)
+            return fail(c, S2D_ERR_ARG, "shot %d: the shots of one call must share the FD order (%d and %d)", s,
+                        m0.fd_order, c->models[shots[s].model_id]->fd_order);
+    b.order8 = m0.fd_order == 8;
     b.steps = derive_steps(wave, m0.dx, m0.dz);
     const RunSteps &rs = b.steps;
     if (rs.fd_nt < 1 || rs.real_nt < 1 || rs.dt_factor < 1)
@@ -678,15 +687,19 @@ constexpr int kTuneCandidates[][3] = {
     {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
+// Candidates of 8th-order batches: the kernel at 3 blocks per SM (168
+// registers) and at 2 (224 registers, no spills).
+constexpr int kTuneCandidatesO8[][3] = {{kVariantO8, 128, 0}, {kVariantO8r, 128, 0}};
+constexpr int kNumTuneCandidatesO8 = (int)(sizeof(kTuneCandidatesO8) / sizeof(kTuneCandidatesO8[0]));
 constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
 // FD steps the trials take (a two-step candidate advances two per launch).
-constexpr int tune_steps() {
-    int n = 0;
-    for (int i = 0; i < kNumTuneCandidates; ++i)
-        n += (kTuneWarm + kTuneTimed) * (kTuneCandidates[i][0] == kVariantTs2 ? 2 : 1);
-    return n;
+constexpr int tune_steps(const int (*cand)[3], int n) {
+    int steps = 0;
+    for (int i = 0; i < n; ++i) steps += (kTuneWarm + kTuneTimed) * (cand[i][0] == kVariantTs2 ? 2 : 1);
+    return steps;
 }
-constexpr int kTuneSteps = tune_steps();
+constexpr int kTuneSteps = tune_steps(kTuneCandidates, kNumTuneCandidates);
+constexpr int kTuneStepsO8 = tune_steps(kTuneCandidatesO8, kNumTuneCandidatesO8);
 
 // Sum of the task counts of a batched launch sequence.
 int batch_tasks(const Batch &b) {
@@ -704,7 +717,9 @@ int batch_tasks(const Batch &b) {
 // candidate with the lowest median time per FD step is cached for the batch's
 // shape and returned, its segment layout in place.
 int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best) {
-    std::vector<cudaEvent_t> ev(2 * kTuneTimed * kNumTuneCandidates, nullptr);
+    const int (*const cands)[3] = b.order8 ? kTuneCandidatesO8 : kTuneCandidates;
+    const int ncand = b.order8 ? kNumTuneCandidatesO8 : kNumTuneCandidates;
+    std::vector<cudaEvent_t> ev(2 * kTuneTimed * ncand, nullptr);
     for (auto &e : ev) {
         cudaError_t ce = cudaEventCreate(&e);
         if (ce != cudaSuccess) {
@@ -716,10 +731,10 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     auto release = [&]() {
         for (auto &x : ev) cudaEventDestroy(x);
     };
-    std::vector<LaunchCfg> cfg(kNumTuneCandidates), full(kNumTuneCandidates);
-    std::vector<bool> ok(kNumTuneCandidates, false);
-    for (int i = 0; i < kNumTuneCandidates; ++i) {
-        const int *k = kTuneCandidates[i];
+    std::vector<LaunchCfg> cfg(ncand), full(ncand);
+    std::vector<bool> ok(ncand, false);
+    for (int i = 0; i < ncand; ++i) {
+        const int *k = cands[i];
         if (launch_config(c, 1L << 40, &full[i], k[0], k[1], k[2]) == S2D_OK) {
             ok[i] = true;
         } else {
@@ -738,7 +753,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     bool graph_used = false;
     for (int r = 0; r < kTuneWarm + kTuneTimed; ++r) {
         const int t = r - kTuneWarm;
-        for (int i = 0; i < kNumTuneCandidates; ++i) {
+        for (int i = 0; i < ncand; ++i) {
             LaunchCfg lc = full[i];
             int e = layout_groups(c, b, lc);
             if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
@@ -762,7 +777,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     cudaError_t ce = cudaStreamSynchronize(c->stream);
     int pick = 0;
     float pick_ms = 0;
-    for (int i = 0; i < kNumTuneCandidates && ce == cudaSuccess; ++i) {
+    for (int i = 0; i < ncand && ce == cudaSuccess; ++i) {
         float t[kTuneTimed];
         for (int s = 0; s < kTuneTimed && ce == cudaSuccess; ++s)
             ce = cudaEventElapsedTime(&t[s], ev[2 * (i * kTuneTimed + s)], ev[2 * (i * kTuneTimed + s) + 1]);
@@ -775,7 +790,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     }
     release();
     CK(ce);
-    const int *k = kTuneCandidates[pick];
+    const int *k = cands[pick];
     c->tuned[tune_key(c, b)] = {k[0], k[1], k[2]};
     int e = layout_groups(c, b, cfg[pick]);
     if (!e) e = launch_config(c, b.max_tasks, best, k[0], k[1], k[2]);
@@ -907,6 +922,7 @@ int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, cons
     CK(cudaSetDevice(c->device));
     auto m = std::make_unique<Model>();
     m->nx = nx; m->nz = nz; m->nb = nb; m->dx = dx; m->dz = dz;
+    m->fd_order = (flags & S2D_MODEL_ORDER8) ? 8 : 4;
     m->nnx = nx + 2 * nb;
     m->nnz = nz + 2 * nb;
     m->ld = leading_dim(m->nnz);
@@ -1011,12 +1027,13 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     int tuned_now = 0;
     // Batched runs of a shape with no tuned configuration yet tune on their
     // first steps when the call has room for the trials and a run after them.
-    if (c->opt_autotune && !tuned && !b.plain && nsteps >= 2 * kTuneSteps) {
+    const int tune_len = b.order8 ? kTuneStepsO8 : kTuneSteps;
+    if (c->opt_autotune && !tuned && !b.plain && nsteps >= 2 * tune_len) {
         a.groups = b.groups_d.as<GroupDev>();
         a.ngroups = (int)b.groups.size();
         int e = autotune(c, b, a, kt_begin, &launches, &lc);
         if (e) return e;
-        kt_run += kTuneSteps;
+        kt_run += tune_len;
         tuned_now = 1;
     }
     if (b.plain) {
@@ -1167,6 +1184,12 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     for (int s = 1; s < nshots; ++s)
         if (shots[s].model_id != shots[0].model_id)
             return fail(c, S2D_ERR_ARG, "all shots of a gradient call must use one model");
+    {
+        auto it = c->models.find(shots[0].model_id);
+        if (it != c->models.end() && it->second->fd_order != 4)
+            return fail(c, S2D_ERR_ARG, "the gradient exists for the 4th-order operator only (model has order %d)",
+                        it->second->fd_order);
+    }
     if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0))
         return fail(c, S2D_ERR_ARG, "wave parameters must be positive");
     CK(cudaSetDevice(c->device));

@@ -429,7 +429,9 @@ int s2d_check_stability(const s2d_jobcard *J, float vmin, float vmax, char *eb, 
     // check_stability.cpp:8-72
     const float fm = 2.0f * J->wave.dom_freq;
     const float hmin = std::min(J->dx, J->dz), hmax = std::max(J->dx, J->dz);
-    float criteria = (0.606f * hmin) / vmax;
+    // 0.606 = 1 / (sqrt(2) (a0 + |a1|)) of the 4th-order operator; the 8th-order
+    // operator's coefficient sum 1.2863 gives 0.549 (no counterpart in the reference)
+    float criteria = ((J->fdop == 8 ? 0.549f : 0.606f) * hmin) / vmax;
     if (J->wave.fd_dt > criteria)
         return say(eb, el, S2D_ERR_STABILITY, "stability condition violated: dt %g > %g (reference code -5)",
                    J->wave.fd_dt, criteria);
@@ -461,8 +463,10 @@ int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, int namin
     s2d_jobcard J;
     int e = s2d_jobcard_read(jobcard_path, &J, eb, el);
     if (e) return e;
-    if (J.fdop != 4)
-        return say(eb, el, S2D_ERR_JOBCARD, "only the 4th-order FD operator exists (Order of FD Operator = %d)",
+    // 4: the reference's operator; 8: the 8th-order operator (the reference
+    // parses the key and steps only for 4, cpumodelling.cpp:121)
+    if (J.fdop != 4 && J.fdop != 8)
+        return say(eb, el, S2D_ERR_JOBCARD, "FD operators of order 4 and 8 exist (Order of FD Operator = %d)",
                    J.fdop);
     s2d_geometry G;
     e = s2d_geometry_read(&J, &G, eb, el);
@@ -522,7 +526,7 @@ int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, int namin
     // "Free surface" : "1" (parsed and ignored by the reference) turns the
     // first model row into a pressure-release surface
     e = s2d_model_create(ctx, J.nx, J.nz, J.dx, J.dz, nb, vp.data(), rho.data(),
-                         J.frsf ? S2D_MODEL_FREE_SURFACE : 0u, &mid);
+                         (J.frsf ? S2D_MODEL_FREE_SURFACE : 0u) | (J.fdop == 8 ? S2D_MODEL_ORDER8 : 0u), &mid);
     s2d_steps st;
     if (!e) e = s2d_derive_steps(&J.wave, &st);
     // shots per batch: what fits in free device memory (8 wavefield buffers per shot)

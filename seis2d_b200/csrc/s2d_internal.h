@@ -117,12 +117,22 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantLdgProducts = 3 /* plain loads + S2D_STEP_PRODUCTS, gradient runs */,
                    kVariantLdg128 = 4 /* plain loads, compiled for 128 registers */,
                    kVariantTs2 = 5 /* two FD steps per launch (112-row strips) */,
-                   kVariantTs1 = 6 /* one FD step in the two-step kernel's layout (odd remainders) */ };
+                   kVariantTs1 = 6 /* one FD step in the two-step kernel's layout (odd remainders) */,
+                   kVariantO8 = 7 /* 8th-order operator, plain loads (112-row strips), models with
+                                     S2D_MODEL_ORDER8; 3 blocks per SM */,
+                   kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */ };
 
 // FD steps one launch of a variant advances.
 inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
-// Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 halo columns).
-inline bool ts_layout(int variant) { return variant == kVariantTs2 || variant == kVariantTs1; }
+// Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 or 13 halo columns).
+inline bool ts_layout(int variant) {
+    return variant == kVariantTs2 || variant == kVariantTs1 || variant == kVariantO8 || variant == kVariantO8r;
+}
+// Variants that use no dynamic shared memory.
+inline bool plain_loads(int variant) {
+    return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 ||
+           variant == kVariantO8 || variant == kVariantO8r;
+}
 
 // Per-warp shared-memory delay lines of the two-step kernel (4 columns each):
 // the first step's px, pz, vz and vx and the second step's p.

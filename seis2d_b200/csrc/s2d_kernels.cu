@@ -651,6 +651,246 @@ __global__ void __launch_bounds__(128, 4) step_kernel_ts(const StepArgs *__restr
     }
 }
 
+// ------------------------------------------ 8th-order operator (kVariantO8)
+//
+// "Order of FD Operator" = 8, which the reference parses but never runs (its
+// step exists for 4 only, cpumodelling.cpp:121).  Same scheme, sponge, source
+// and receivers as the 4th-order kernels, with the staggered 8th-order
+// operators
+//   D- f[i] = sum_k c_k (f[i+k-1] - f[i-k]),  D+ f[i] = sum_k c_k (f[i+k] - f[i-k+1]),
+// c = (1225/1024, -245/3072, 49/5120, -5/7168), and the reference's 4th-order,
+// plain-difference and zero rows where the 8-tap stencil would leave the grid.
+//
+// One fused pass per step, streamed like the plain-load kernel: the warp keeps
+// vx at P-4 .. P+3 (8 columns), new p at V-3 .. V+4 (8 columns) and vz at
+// V .. P (5 columns) in registers, forms p at P = L-3 and the velocities at
+// V = L-7.  The z-stencils reach 4 rows, one whole neighbouring lane: p is
+// exact on lanes 1..30 and the velocities on lanes 2..29, so strips are 112
+// rows (the two-step kernel's layout, read from 112k-8) and lanes 2..29 write.
+
+constexpr float kC81 = 1225.0f / 1024.0f;
+constexpr float kC82 = -245.0f / 3072.0f;
+constexpr float kC83 = 49.0f / 5120.0f;
+constexpr float kC84 = -5.0f / 7168.0f;
+
+// Coefficients of row i of the 8th-order D- (taps i-4 .. i+3) and D+ (taps
+// i-3 .. i+4); the reference's pairs (a0, a1), (1, 0) or 0 near the edges.
+__device__ __forceinline__ float4 dm8(int i, int n) {
+    if (i >= 4 && i <= n - 4) return make_float4(kC81, kC82, kC83, kC84);
+    float c0, c1;
+    dm_coef(i, n, c0, c1);
+    return make_float4(c0, c1, 0.0f, 0.0f);
+}
+__device__ __forceinline__ float4 dp8(int i, int n) {
+    if (i >= 3 && i <= n - 5) return make_float4(kC81, kC82, kC83, kC84);
+    float c0, c1;
+    dp_coef(i, n, c0, c1);
+    return make_float4(c0, c1, 0.0f, 0.0f);
+}
+// c1 d1 + c2 d2 + c3 d3 + c4 d4 with the rounding fixed (innermost product
+// rounded, then three fused steps).
+__device__ __forceinline__ float dif8(const float4 &c, float d1, float d2, float d3, float d4) {
+    return __fmaf_rn(c.x, d1, __fmaf_rn(c.y, d2, __fmaf_rn(c.z, d3, __fmul_rn(c.w, d4))));
+}
+template <bool FAST>
+__device__ __forceinline__ float4 zdm8(const Lane<FAST> &ln, int i) {
+    if (FAST) return make_float4(kC81, kC82, kC83, kC84);
+    return dm8(ln.z0 + i, ln.nnz);
+}
+template <bool FAST>
+__device__ __forceinline__ float4 zdp8(const Lane<FAST> &ln, int i) {
+    if (FAST) return make_float4(kC81, kC82, kC83, kC84);
+    return dp8(ln.z0 + i, ln.nnz);
+}
+
+// New p at column P from vx at P-4 .. P+3 (w), old px, pz, kappa and vz at P.
+template <bool FAST>
+__device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &xc,
+                                            bool colm, const float4 (&w)[8], const float4 &px, const float4 &pz,
+                                            const float4 &kk, const float4 &vz, float4 &pxn, float4 &pzn) {
+    // vz rows z0-4 .. z0+6: the lane above's four (u), this lane's, the lane below's first three (d)
+    const float u0 = __shfl_up_sync(kFull, vz.x, 1), u1 = __shfl_up_sync(kFull, vz.y, 1);
+    const float u2 = __shfl_up_sync(kFull, vz.z, 1), u3 = __shfl_up_sync(kFull, vz.w, 1);
+    const float d0 = __shfl_down_sync(kFull, vz.x, 1), d1 = __shfl_down_sync(kFull, vz.y, 1);
+    const float d2 = __shfl_down_sync(kFull, vz.z, 1);
+    const float dz0 = dif8(zdm8(ln, 0), vz.x - u3, vz.y - u2, vz.z - u1, vz.w - u0);
+    const float dz1 = dif8(zdm8(ln, 1), vz.y - vz.x, vz.z - u3, vz.w - u2, d0 - u1);
+    const float dz2 = dif8(zdm8(ln, 2), vz.z - vz.y, vz.w - vz.x, d0 - u3, d1 - u2);
+    const float dz3 = dif8(zdm8(ln, 3), vz.w - vz.z, d0 - vz.y, d1 - vz.x, d2 - u3);
+    const float4 cx = dm8(P, S.nnx);
+    const float dx0 = dif8(cx, w[4].x - w[3].x, w[5].x - w[2].x, w[6].x - w[1].x, w[7].x - w[0].x);
+    const float dx1 = dif8(cx, w[4].y - w[3].y, w[5].y - w[2].y, w[6].y - w[1].y, w[7].y - w[0].y);
+    const float dx2 = dif8(cx, w[4].z - w[3].z, w[5].z - w[2].z, w[6].z - w[1].z, w[7].z - w[0].z);
+    const float dx3 = dif8(cx, w[4].w - w[3].w, w[5].w - w[2].w, w[6].w - w[1].w, w[7].w - w[0].w);
+    const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
+    float t0, t1;
+    p_cell(colm && (FAST || r0.x == 1.0f), xc.x, xc.y, r0.x, r0.y, px.x, pz.x, kk.x, dx0, dz0, pxn.x, pzn.x, t0, t1);
+    p_cell(colm && (FAST || r1.x == 1.0f), xc.x, xc.y, r1.x, r1.y, px.y, pz.y, kk.y, dx1, dz1, pxn.y, pzn.y, t0, t1);
+    p_cell(colm && (FAST || r2.x == 1.0f), xc.x, xc.y, r2.x, r2.y, px.z, pz.z, kk.z, dx2, dz2, pxn.z, pzn.z, t0, t1);
+    p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, t0, t1);
+    if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
+        if (ln.sdz == 0) pxn.x += ln.amp;
+        else if (ln.sdz == 1) pxn.y += ln.amp;
+        else if (ln.sdz == 2) pxn.z += ln.amp;
+        else pxn.w += ln.amp;
+    }
+    return make_float4(pxn.x + pzn.x, pxn.y + pzn.y, pxn.z + pzn.z, pxn.w + pzn.w);
+}
+
+// Velocities at column V from new p at V-3 .. V+4 (pw), old vx, vz and bx, bz at V.
+template <bool FAST>
+__device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S, int V, const float4 (&pw)[8],
+                                          const float4 &vx, const float4 &vz, const float4 &bx, const float4 &bz,
+                                          float4 &vxn, float4 &vzn) {
+    const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
+    const float4 cx = dp8(V, S.nnx);
+    const float ex0 = dif8(cx, pw[4].x - pw[3].x, pw[5].x - pw[2].x, pw[6].x - pw[1].x, pw[7].x - pw[0].x);
+    const float ex1 = dif8(cx, pw[4].y - pw[3].y, pw[5].y - pw[2].y, pw[6].y - pw[1].y, pw[7].y - pw[0].y);
+    const float ex2 = dif8(cx, pw[4].z - pw[3].z, pw[5].z - pw[2].z, pw[6].z - pw[1].z, pw[7].z - pw[0].z);
+    const float ex3 = dif8(cx, pw[4].w - pw[3].w, pw[5].w - pw[2].w, pw[6].w - pw[1].w, pw[7].w - pw[0].w);
+    // p rows z0-3 .. z0+7 at V: the lane above's last three (u), this lane's (q), the lane below's four (d)
+    const float4 q = pw[3];
+    const float u1 = __shfl_up_sync(kFull, q.y, 1), u2 = __shfl_up_sync(kFull, q.z, 1);
+    const float u3 = __shfl_up_sync(kFull, q.w, 1);
+    const float d0 = __shfl_down_sync(kFull, q.x, 1), d1 = __shfl_down_sync(kFull, q.y, 1);
+    const float d2 = __shfl_down_sync(kFull, q.z, 1), d3 = __shfl_down_sync(kFull, q.w, 1);
+    const float ez0 = dif8(zdp8(ln, 0), q.y - q.x, q.z - u3, q.w - u2, d0 - u1);
+    const float ez1 = dif8(zdp8(ln, 1), q.z - q.y, q.w - q.x, d0 - u3, d1 - u2);
+    const float ez2 = dif8(zdp8(ln, 2), q.w - q.z, d0 - q.y, d1 - q.x, d2 - u3);
+    const float ez3 = dif8(zdp8(ln, 3), d0 - q.w, d1 - q.z, d2 - q.y, d3 - q.x);
+    vxn.x = upd(xc.z, vx.x, xc.w, bx.x, ex0);
+    vxn.y = upd(xc.z, vx.y, xc.w, bx.y, ex1);
+    vxn.z = upd(xc.z, vx.z, xc.w, bx.z, ex2);
+    vxn.w = upd(xc.z, vx.w, xc.w, bx.w, ex3);
+    float4 r = zrow(ln, 0);
+    vzn.x = upd(r.z, vz.x, r.w, bz.x, ez0);
+    r = zrow(ln, 1);
+    vzn.y = upd(r.z, vz.y, r.w, bz.y, ez1);
+    r = zrow(ln, 2);
+    vzn.z = upd(r.z, vz.z, r.w, bz.z, ez2);
+    r = zrow(ln, 3);
+    vzn.w = upd(r.z, vz.w, r.w, bz.w, ez3);
+}
+
+// One (shot, strip, segment) task of the 8th-order step.  Columns read:
+// vx at xa-7 .. xb+6, px, pz, kappa, vz at xa-3 .. xb+3, bx, bz at xa .. xb-1
+// (inside the 8 ghost columns on each side).
+template <bool FAST>
+__device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len, int kt,
+                                        int par, bool rec_step, int slot, int lane) {
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t ld = (size_t)S.ld;
+    const int c = strip * S2D_TS_OUT - 8;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    ln.owner = lane >= 2 && lane <= 29;
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    const float *__restrict__ pxi = sb + ib;
+    const float *__restrict__ pzi = sb + ib + fs;
+    const float *__restrict__ vxi = sb + ib + 2 * fs;
+    const float *__restrict__ vzi = sb + ib + 3 * fs;
+    float *__restrict__ pxo = sb + ob;
+    float *__restrict__ pzo = sb + ob + fs;
+    float *__restrict__ vxo = sb + ob + 2 * fs;
+    float *__restrict__ vzo = sb + ob + 3 * fs;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = kap + fs;
+    const float *__restrict__ bzp = kap + 2 * fs;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 w[8], pw[8], zq[5];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) pw[i] = zero;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) zq[i] = zero;
+    w[0] = zero;
+#pragma unroll
+    for (int i = 1; i < 8; ++i) w[i] = ld4(vxi + (ptrdiff_t)(xa - 8 + i) * (ptrdiff_t)ld);
+    for (int L = xa; L <= xb + 6; ++L) {
+        const int P = L - 3;
+        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) w[i] = w[i + 1];
+        w[7] = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
+        const float4 vz = ld4(vzi + colP);
+        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = xc.x == 1.0f;
+        const bool pz_live = !(FAST && colm);
+        float4 pxn, pzn;
+        const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
+                                    ld4(kap + colP), vz, pxn, pzn);
+        const bool in_seg = P >= xa && P < xb;
+        if (in_seg && ln.owner) {
+            st4(pxo + colP, pxn);
+            if (pz_live) st4(pzo + colP, pzn);
+        }
+        if (rec && in_seg) record(ln, S, P, pn, slot);
+#pragma unroll
+        for (int i = 0; i < 7; ++i) pw[i] = pw[i + 1];
+        pw[7] = pn;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) zq[i] = zq[i + 1];
+        zq[4] = vz;
+        if (L >= xa + 7) {
+            const int V = L - 7;
+            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+            float4 vxn, vzn;
+            v_update8(ln, S, V, pw, w[0], zq[0], ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+            if (ln.owner) {
+                st4(vxo + colV, vxn);
+                st4(vzo + colV, vzn);
+            }
+        }
+    }
+}
+
+// Debug self-check (S2D_DEVICE_CHECKS) of the 8th-order task's reach.
+__device__ __forceinline__ bool o8_in_bounds(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len) {
+#ifdef S2D_DEVICE_CHECKS
+    const long ld = S.ld;
+    const int xb = min(S.nnx, xa + seg_len);
+    const long c = (long)strip * S2D_TS_OUT - 8;
+    const long F = (long)(S.nnx + 2 * S2D_GX) * ld;
+    const long lo = (long)(xa - 7 + S2D_GX) * ld + (c + S2D_GZ);
+    const long hi = (long)(xb + 6 + S2D_GX) * ld + (c + S2D_GZ) + 127;
+    if (xa - 7 < -S2D_GX || xb + 6 >= S.nnx + S2D_GX || c + S2D_GZ < 0 || c + 127 + S2D_GZ >= ld || lo < 0 ||
+        hi >= F || (size_t)F > S.nfield) {
+        if (a.err) atomicCAS(a.err, 0, (3 << 8) | 1);
+        return false;
+    }
+#endif
+    return true;
+}
+
+// MINB blocks of 4 warps per SM: 3 caps registers at 168 (some spill), 2
+// leaves the 224 the windows (84 registers) and stencils need.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__restrict__ A, int kt_off) {
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base + kt_off;
+    if (kt >= a.fd_nt) return;
+    const int par = a.par0 ^ (kt_off & 1);
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
+        const int c = strip * S2D_TS_OUT - 8;
+        // literal coefficients: every row of the strip 8th-order and undamped in z
+        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
+            o8_task<true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else
+            o8_task<false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+    }
+}
+
 // ---- model preparation (cpumodelling.cpp:207-230, cpu_modelling_kernels.cpp:64-121) ----
 
 // kappa = vp^2 rho in double rounded to float, buoyancy 1/rho (1e10 where
@@ -708,6 +948,10 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_ts<true><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantTs1)
         step_kernel_ts<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantO8)
+        step_kernel_o8<3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantO8r)
+        step_kernel_o8<2><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
         step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
@@ -735,12 +979,14 @@ const void *kernel_of(int variant) {
     if (variant == kVariantLdg128) return (const void *)step_kernel_ldg<false, 4>;
     if (variant == kVariantTs2) return (const void *)step_kernel_ts<true>;
     if (variant == kVariantTs1) return (const void *)step_kernel_ts<false>;
+    if (variant == kVariantO8) return (const void *)step_kernel_o8<3>;
+    if (variant == kVariantO8r) return (const void *)step_kernel_o8<2>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace
 
 int step_kernel_prepare(int variant, size_t smem) {
-    if (variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128) return 0;
+    if (plain_loads(variant)) return 0;
     const void *k = kernel_of(variant);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -748,8 +994,8 @@ int step_kernel_prepare(int variant, size_t smem) {
 }
 
 int step_kernel_occupancy(int variant, int block, size_t smem, int *blocks_per_sm) {
-    const bool ldg = variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128;
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block, ldg ? 0 : smem);
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel_of(variant), block,
+                                                             plain_loads(variant) ? 0 : smem);
 }
 
 int step_kernel_attributes(int variant, int *regs, int *local_bytes) {

@@ -61,7 +61,11 @@ void modelling_module(int my_nsrc, geo2d_t *g) {
     // job_sp->frsf ("Free surface", json_parser.cpp:236-244) is parsed and
     // ignored by the reference's modelling; here 1 gives a pressure-release
     // surface at the first model row
-    const unsigned mflags = job_sp->frsf ? S2D_MODEL_FREE_SURFACE : 0u;
+    // job_sp->fdop ("Order of FD Operator"): the reference steps only for 4
+    // (cpumodelling.cpp:121) and writes zero traces otherwise; here 8 runs the
+    // 8th-order operator and other values stop the job
+    if (job_sp->fdop != 4 && job_sp->fdop != 8) die(ctx, "Order of FD Operator must be 4 or 8");
+    const unsigned mflags = (job_sp->frsf ? S2D_MODEL_FREE_SURFACE : 0u) | (job_sp->fdop == 8 ? S2D_MODEL_ORDER8 : 0u);
     if (s2d_model_create(ctx, nx, nz, mod_sp->dx, mod_sp->dz, nb, vp.data(), rho.data(), mflags, &model) != S2D_OK)
         die(ctx, "model");
 

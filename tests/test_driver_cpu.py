@@ -162,3 +162,21 @@ def test_stability_and_dispersion_checks(in_tmp):
     with pytest.raises(Seis2dError) as e:
         D.check_stability(c3, 1500.0, 4500.0)
     assert e.value.code == S2D_ERR_STABILITY and "dispersion" in str(e.value)
+
+
+def test_fd_order_rules(in_tmp):
+    """Order 8 (the 8th-order operator) has the tighter stability bound
+    0.549 h / vmax; orders other than 4 and 8 stop the job before any device
+    work (the reference parses the key and steps only for 4)."""
+    c8 = D.read_jobcard(_card(in_tmp, **{"Order of FD Operator": 8}))
+    assert c8.fdop == 8
+    c4 = D.read_jobcard(_card(in_tmp))
+    D.check_stability(c4, 1500.0, 5800.0)  # 1 ms <= 0.606 * 10 / 5800
+    with pytest.raises(Seis2dError) as e:  # 1 ms > 0.549 * 10 / 5800
+        D.check_stability(c8, 1500.0, 5800.0)
+    assert e.value.code == S2D_ERR_STABILITY
+    D.check_stability(c8, 1500.0, 5400.0)
+    path = _card(in_tmp, **{"Order of FD Operator": 6})
+    with pytest.raises(Seis2dError) as e:
+        D.run_jobcard(path)
+    assert e.value.code == S2D_ERR_JOBCARD and "order" in str(e.value)
