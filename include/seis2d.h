@@ -154,7 +154,10 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 compiled for 128 registers, 4 plain loads compiled for 128
  *                 registers (default), 5 two FD steps per launch (the state
  *                 crosses HBM once per two steps; odd step counts end with one
- *                 one-step launch); s2d_gradient always runs one step per launch
+ *                 one-step launch); s2d_gradient always runs one step per launch.
+ *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
+ *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in
+ *                 shared memory at 4 (each setting applies to its own order)
  *   "block"       threads per block: 32, 64, 96 or 128 (default 128)
  *   "task_order"  0: consecutive warps take the shots of one tile;
  *                 1: consecutive warps take adjacent strips of one shot (default)

@@ -150,6 +150,7 @@ struct Ctx {
     // tuning options (s2d_set_option)
     // explicit launch configuration, used when autotuning is off
     int opt_variant = kVariantLdg128;
+    int opt_variant8 = kVariantO8;  // 8th-order batches when autotuning is off
     int opt_block = 128;
     int opt_stages = 3;
     int opt_autotune = 1;     // time candidate configurations on a new batch shape
@@ -266,7 +267,9 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
         lc.block = 128;
         lc.stages = 0;
     }
-    lc.smem = ldg ? 0 : ts ? (size_t)(lc.block / 32) * kTsWarpBytes : bulk_smem_bytes(lc.block / 32, lc.stages);
+    lc.smem = ldg ? 0
+              : ts ? (size_t)(lc.block / 32) * (lc.variant == kVariantO8s ? kO8sWarpBytes : kTsWarpBytes)
+                   : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
     if (e) return fail(c, S2D_ERR_ARG, "step kernel does not accept %zu B of shared memory: %s", lc.smem,
                        cudaGetErrorString((cudaError_t)e));
@@ -300,7 +303,7 @@ std::vector<long> tune_key(const Ctx *c, const Batch &b) {
 int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
     if (tuned) *tuned = false;
     // 8th-order batches run the 8th-order kernel whatever the options say
-    if (b.order8 && !c->opt_autotune) return launch_config(c, b.max_tasks, out, kVariantO8, 128, 0);
+    if (b.order8 && !c->opt_autotune) return launch_config(c, b.max_tasks, out, c->opt_variant8, 128, 0);
     if (!c->opt_autotune) return launch_config(c, b.max_tasks, out, c->opt_variant, c->opt_block, c->opt_stages);
     auto it = c->tuned.find(tune_key(c, b));
     if (it != c->tuned.end()) {
@@ -687,9 +690,10 @@ constexpr int kTuneCandidates[][3] = {
     {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
-// Candidates of 8th-order batches: the kernel at 3 blocks per SM (168
-// registers) and at 2 (224 registers, no spills).
-constexpr int kTuneCandidatesO8[][3] = {{kVariantO8, 128, 0}, {kVariantO8r, 128, 0}};
+// Candidates of 8th-order batches: the register-window kernel at 3 blocks per
+// SM (168 registers) and at 2 (224 registers, no spills), and the
+// shared-memory-window kernel at 4 (128 registers).
+constexpr int kTuneCandidatesO8[][3] = {{kVariantO8, 128, 0}, {kVariantO8r, 128, 0}, {kVariantO8s, 128, 0}};
 constexpr int kNumTuneCandidatesO8 = (int)(sizeof(kTuneCandidatesO8) / sizeof(kTuneCandidatesO8[0]));
 constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
 // FD steps the trials take (a two-step candidate advances two per launch).
@@ -809,6 +813,12 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     const std::string k(key);
     // an explicit launch configuration turns the autotuner off
     if (k == "variant") {
+        if (order8_variant((int)value)) {
+            // the 8th-order kernels serve 8th-order batches only
+            c->opt_variant8 = (int)value;
+            c->opt_autotune = 0;
+            return S2D_OK;
+        }
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
             value != kVariantTs2)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);

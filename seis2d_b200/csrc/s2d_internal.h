@@ -120,13 +120,18 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantTs1 = 6 /* one FD step in the two-step kernel's layout (odd remainders) */,
                    kVariantO8 = 7 /* 8th-order operator, plain loads (112-row strips), models with
                                      S2D_MODEL_ORDER8; 3 blocks per SM */,
-                   kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */ };
+                   kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */,
+                   kVariantO8s = 9 /* the same with its windows in shared memory, 4 blocks per SM */ };
 
 // FD steps one launch of a variant advances.
 inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
 // Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 or 13 halo columns).
 inline bool ts_layout(int variant) {
-    return variant == kVariantTs2 || variant == kVariantTs1 || variant == kVariantO8 || variant == kVariantO8r;
+    return variant == kVariantTs2 || variant == kVariantTs1 || variant == kVariantO8 || variant == kVariantO8r ||
+           variant == kVariantO8s;
+}
+inline bool order8_variant(int variant) {
+    return variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8s;
 }
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
@@ -139,6 +144,9 @@ inline bool plain_loads(int variant) {
 constexpr int kTsRing = 4;
 constexpr int kTsFields = 5;
 constexpr int kTsWarpBytes = kTsRing * kTsFields * S2D_STRIP_ROWS * 4;
+// Per-warp shared-memory windows of the 8th-order ring kernel: vx and new p of
+// 8 columns each, vz of 4 (one 128-row column = 32 float4).
+constexpr int kO8sWarpBytes = (8 + 8 + 4) * S2D_STRIP_ROWS * 4;
 
 // Shared memory of one pipeline stage: 7 slots of one 128-row column each
 // (vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3).

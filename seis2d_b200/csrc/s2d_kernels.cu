@@ -847,6 +847,83 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
     }
 }
 
+// The same task with its windows in a per-warp shared-memory ring instead of
+// registers (kVariantO8s, 128 registers, 16 warps per SM): vx of the last 8
+// columns, new p of the last 8, vz of the last 4.  Each lane reads back only
+// the entries it wrote, so the ring needs no synchronisation.
+__device__ __forceinline__ float4 &o8_ring(float4 *ring, int field, int col, int lane) {
+    // field 0: vx (8 slots), 1: new p (8 slots), 2: vz (4 slots)
+    return field == 2 ? ring[(16 + (col & 3)) * 32 + lane] : ring[(field * 8 + (col & 7)) * 32 + lane];
+}
+
+template <bool FAST>
+__device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len, int kt,
+                                         int par, bool rec_step, int slot, int lane, float4 *ring) {
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t ld = (size_t)S.ld;
+    const int c = strip * S2D_TS_OUT - 8;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    ln.owner = lane >= 2 && lane <= 29;
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    const float *__restrict__ pxi = sb + ib;
+    const float *__restrict__ pzi = sb + ib + fs;
+    const float *__restrict__ vxi = sb + ib + 2 * fs;
+    const float *__restrict__ vzi = sb + ib + 3 * fs;
+    float *__restrict__ pxo = sb + ob;
+    float *__restrict__ pzo = sb + ob + fs;
+    float *__restrict__ vxo = sb + ob + 2 * fs;
+    float *__restrict__ vzo = sb + ob + 3 * fs;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = kap + fs;
+    const float *__restrict__ bzp = kap + 2 * fs;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int col = xa - 7; col < xa; ++col) o8_ring(ring, 0, col, lane) = ld4(vxi + (ptrdiff_t)col * (ptrdiff_t)ld);
+    for (int L = xa; L <= xb + 6; ++L) {
+        const int P = L - 3;
+        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+        float4 w[8];
+        w[7] = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
+#pragma unroll
+        for (int i = 0; i < 7; ++i) w[i] = o8_ring(ring, 0, L - 7 + i, lane);
+        o8_ring(ring, 0, L, lane) = w[7];  // the slot of column L-8, no longer needed
+        const float4 vz = ld4(vzi + colP);
+        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = xc.x == 1.0f;
+        const bool pz_live = !(FAST && colm);
+        float4 pxn, pzn;
+        const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
+                                    ld4(kap + colP), vz, pxn, pzn);
+        const bool in_seg = P >= xa && P < xb;
+        if (in_seg && ln.owner) {
+            st4(pxo + colP, pxn);
+            if (pz_live) st4(pzo + colP, pzn);
+        }
+        if (rec && in_seg) record(ln, S, P, pn, slot);
+        const float4 vzV = o8_ring(ring, 2, P - 4, lane);  // read before vz at P takes its slot
+        o8_ring(ring, 2, P, lane) = vz;
+        o8_ring(ring, 1, P, lane) = pn;                    // the slot of column P-8
+        if (L >= xa + 7) {
+            const int V = L - 7;
+            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+            float4 pw[8];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) pw[i] = o8_ring(ring, 1, V - 3 + i, lane);
+            pw[7] = pn;
+            float4 vxn, vzn;
+            v_update8(ln, S, V, pw, w[0], vzV, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+            if (ln.owner) {
+                st4(vxo + colV, vxn);
+                st4(vzo + colV, vzn);
+            }
+        }
+    }
+}
+
 // Debug self-check (S2D_DEVICE_CHECKS) of the 8th-order task's reach.
 __device__ __forceinline__ bool o8_in_bounds(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len) {
 #ifdef S2D_DEVICE_CHECKS
@@ -888,6 +965,32 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__re
             o8_task<true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
         else
             o8_task<false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+    }
+}
+
+// The shared-memory-ring form: 128 registers, 4 blocks of 4 warps per SM,
+// kO8sWarpBytes of dynamic shared memory per warp.
+__global__ void __launch_bounds__(128, 4) step_kernel_o8s(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kO8sWarpBytes);
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base + kt_off;
+    if (kt >= a.fd_nt) return;
+    const int par = a.par0 ^ (kt_off & 1);
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
+        const int c = strip * S2D_TS_OUT - 8;
+        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
+            o8s_task<true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else
+            o8s_task<false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
     }
 }
 
@@ -952,6 +1055,8 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_o8<3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantO8r)
         step_kernel_o8<2><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantO8s)
+        step_kernel_o8s<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
         step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
@@ -981,6 +1086,7 @@ const void *kernel_of(int variant) {
     if (variant == kVariantTs1) return (const void *)step_kernel_ts<false>;
     if (variant == kVariantO8) return (const void *)step_kernel_o8<3>;
     if (variant == kVariantO8r) return (const void *)step_kernel_o8<2>;
+    if (variant == kVariantO8s) return (const void *)step_kernel_o8s;
     return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace

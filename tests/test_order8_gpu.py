@@ -69,7 +69,7 @@ def test_forward_matches_oracle(ctx):
     shots, rec = _shots(m)
     got = ctx.forward(shots, _wave())
     st = ctx.last_stats
-    assert st.variant in (7, 8)
+    assert st.variant in (7, 8, 9)
     for s, g in zip(shots, got):
         assert O.rel_l2(g, _oracle(vp, rho, s.src, rec, O.F64)) <= TOL
         assert O.rel_l2(g, _oracle(vp, rho, s.src, rec, O.F32)) <= 2e-6
@@ -82,10 +82,12 @@ def test_forward_matches_oracle(ctx):
 
 
 def test_tuned_fixed_plain_and_stepwise_runs_agree():
-    """Both launch forms the autotuner chooses between, shot after shot, and
-    launches without a graph compute the same bits."""
+    """The three launch forms the autotuner chooses between (register windows
+    at 3 and 2 blocks per SM, shared-memory windows at 4), shot after shot,
+    and launches without a graph compute the same bits."""
     from seis2d_b200 import Context
     c = Context(0)
+    forced = {}
     try:
         vp, rho = _model(NX, NZ, 2)
         m = c.model(vp, rho, D, D, NB, fd_order=8)
@@ -97,13 +99,20 @@ def test_tuned_fixed_plain_and_stepwise_runs_agree():
         c.set_option("autotune", 0)
         fixed = c.forward(shots, _wave())
         s2 = c.last_stats
+        for v in (7, 8, 9):
+            c.set_option("variant", v)
+            forced[v] = (c.forward(shots, _wave()), c.last_stats.variant)
     finally:
         c.close()
-    assert s1.autotuned == 1 and s1.variant in (7, 8) and s2.variant == 7
+    assert s1.autotuned == 1 and s1.variant in (7, 8, 9) and s2.variant == 7
     for a, b, d, f in zip(tuned, plain, nograph, fixed):
         np.testing.assert_array_equal(a, b)
         np.testing.assert_array_equal(a, d)
         np.testing.assert_array_equal(a, f)
+    for v, (traces, used) in forced.items():
+        assert used == v
+        for a, f in zip(tuned, traces):
+            np.testing.assert_array_equal(a, f)
 
 
 def test_uneven_models_and_continuation(ctx):
