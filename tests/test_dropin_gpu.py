@@ -30,3 +30,27 @@ def test_dropin_writes_the_reference_file(tmp_path, name):
     got = F.read_seismogram(str(tmp_path / "out" / "case_seismogram.bin"), z["rec"].shape[0])
     assert got.shape == z["seis"].shape
     assert O.rel_l2(got, z["seis"]) <= TOL
+
+
+@pytest.mark.parametrize("key,value,fs,order", [("Free surface", "1", 1, 4), ("Order of FD Operator", "8", 0, 8)])
+def test_dropin_honours_free_surface_and_order8(tmp_path, key, value, fs, order):
+    """Keys the reference parses and ignores: through its own host program the
+    drop-in gives the oracle's traces for the free surface and the 8th-order
+    operator (no reference output exists for them)."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("oracle/_ref/seis_dropin not built")
+    from cases import model
+    z, c = stage(tmp_path, "twolayer_split_nb32")
+    card = (tmp_path / "case.json").read_text()
+    old = f'"{key}" : "0"' if key == "Free surface" else f'"{key}" : "4"'
+    assert old in card
+    (tmp_path / "case.json").write_text(card.replace(old, f'"{key}" : "{value}"'))
+    r = subprocess.run([DROPIN, "case.json"], cwd=tmp_path, capture_output=True, text=True,
+                       env=dict(os.environ, S2D_NB=str(c["nb"])))
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = F.read_seismogram(str(tmp_path / "out" / "case_seismogram.bin"), z["rec"].shape[0])
+    vp, rho = model(c["model"], c["nx"], c["nz"], c["dx"], c["dz"])
+    p = O.Params(c["nx"], c["nz"], c["nb"], c["dx"], c["dz"], c["T"], c["dt"], c["ddt"], c["f"], fs, order)
+    ref = O.forward(p, vp, rho, z["src"], z["rec"][:, 0], z["rec"][:, 1], O.F64)
+    assert O.rel_l2(got, ref) <= TOL
+    assert O.rel_l2(got, z["seis"]) > 1e-3
