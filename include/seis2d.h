@@ -2,7 +2,9 @@
  * seis2d.h -- C ABI of libseis2d, the B200 (sm_100a) implementation of
  * SeisAcoMod2D's forward-modelling hot path: the per-shot 2-D acoustic
  * 4th-order staggered-grid time loop with split-field sponge, Ricker source
- * injection and receiver sampling.
+ * injection and receiver sampling (and, as options of a model, the
+ * free surface and 8th-order operator the reference's job card names but
+ * its modelling never implements).
  *
  * Reference seam replaced:
  *   void modelling_module(int my_nsrc, geo2d_t *mygeo2d_sp);

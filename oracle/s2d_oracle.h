@@ -15,6 +15,9 @@
  *                                   the CUDA kernels use (cells where both
  *                                   pressure dampings are 1 carry p = px + pz
  *                                   in px alone).
+ * Two options the reference parses and never implements are restated as this
+ * project defines them (orc_params.free_surface, orc_params.fd_order = 8); with
+ * both at their defaults the oracle is the reference's scheme.
  */
 #ifndef S2D_ORACLE_H
 #define S2D_ORACLE_H
