@@ -744,6 +744,65 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
     }
 }
 
+/* The same four operators and their transposes for the 8th-order operator
+ * (dm8_coef / dp8_coef rows, which include the reference's rows at the
+ * edges): d = D f, and out += D^T mu as the scatter of each forward row. */
+static void op8_apply(int which, const double *f, double *d, int nnz, int nnx) {
+#define F8(ix, iz) ((ix) < 0 || (ix) >= nnx || (iz) < 0 || (iz) >= nnz ? 0.0 : f[(size_t)(iz) + (size_t)(ix) * nnz])
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            float c[4];
+            double v = 0.0;
+            if (which == 0) { /* Gx = D-x */
+                dm8_coef(ix, nnx, c);
+                for (int k = 0; k < 4; k++) v += (double)c[k] * (F8(ix + k, iz) - F8(ix - 1 - k, iz));
+            } else if (which == 1) { /* Gz = D-z */
+                dm8_coef(iz, nnz, c);
+                for (int k = 0; k < 4; k++) v += (double)c[k] * (F8(ix, iz + k) - F8(ix, iz - 1 - k));
+            } else if (which == 2) { /* Hx = D+x */
+                dp8_coef(ix, nnx, c);
+                for (int k = 0; k < 4; k++) v += (double)c[k] * (F8(ix + 1 + k, iz) - F8(ix - k, iz));
+            } else { /* Hz = D+z */
+                dp8_coef(iz, nnz, c);
+                for (int k = 0; k < 4; k++) v += (double)c[k] * (F8(ix, iz + 1 + k) - F8(ix, iz - k));
+            }
+            d[(size_t)iz + (size_t)ix * nnz] = v;
+        }
+#undef F8
+}
+static void op8T_add(int which, const double *mu, double *out, int nnz, int nnx) {
+#define ADD8(ix, iz, v)                                                          \
+    do {                                                                         \
+        if ((ix) >= 0 && (ix) < nnx && (iz) >= 0 && (iz) < nnz)                  \
+            out[(size_t)(iz) + (size_t)(ix) * nnz] += (v);                       \
+    } while (0)
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            const double m = mu[(size_t)iz + (size_t)ix * nnz];
+            float c[4];
+            for (int k = 0; k < 4; k++) {
+                if (which == 0) {
+                    dm8_coef(ix, nnx, c);
+                    ADD8(ix + k, iz, c[k] * m);
+                    ADD8(ix - 1 - k, iz, -c[k] * m);
+                } else if (which == 1) {
+                    dm8_coef(iz, nnz, c);
+                    ADD8(ix, iz + k, c[k] * m);
+                    ADD8(ix, iz - 1 - k, -c[k] * m);
+                } else if (which == 2) {
+                    dp8_coef(ix, nnx, c);
+                    ADD8(ix + 1 + k, iz, c[k] * m);
+                    ADD8(ix - k, iz, -c[k] * m);
+                } else {
+                    dp8_coef(iz, nnz, c);
+                    ADD8(ix, iz + 1 + k, c[k] * m);
+                    ADD8(ix, iz - k, -c[k] * m);
+                }
+            }
+        }
+#undef ADD8
+}
+
 int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                  float sx, float sz, int nrec, const float *gx, const float *gz,
                  const double *wavelet, int nwav, const double *adj,
@@ -751,7 +810,8 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                  double *grad_kappa, double *grad_bx, double *grad_bz,
                  double *src_adj, double *seis64) {
     if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz))) return -1;
-    if (prm->fd_order != 0 && prm->fd_order != 4) return -4; /* the adjoint of the 4th-order scheme only */
+    if (prm->fd_order != 0 && prm->fd_order != 4 && prm->fd_order != 8) return -1;
+    const int o8 = prm->fd_order == 8;
     orc_derived d;
     orc_derive(prm, &d);
     if (d.dt_factor < 1 || d.fd_nt < 1) return -2;
@@ -794,8 +854,13 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
     if (!A || !Cc || !Gg || !Hh) return -4;
     for (int kt = 0; kt < nt; kt++) {
         double *a = A + N * kt, *c = Cc + N * kt, *g = Gg + N * kt, *h = Hh + N * kt;
-        op_apply(0, vx, a, nnz, nnx);
-        op_apply(1, vz, c, nnz, nnx);
+        if (o8) {
+            op8_apply(0, vx, a, nnz, nnx);
+            op8_apply(1, vz, c, nnz, nnx);
+        } else {
+            op_apply(0, vx, a, nnz, nnx);
+            op_apply(1, vz, c, nnz, nnx);
+        }
         for (int ix = 0; ix < nnx; ix++)
             for (int iz = 0; iz < nnz; iz++) {
                 size_t id = (size_t)iz + (size_t)ix * nnz;
@@ -804,8 +869,13 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
             }
         if (kt <= d.nts) px[isrc] = px[isrc] + prm->fd_dt * (kt < nw ? w[kt] : 0.0) * kappa[isrc] / (dxdz);
         for (size_t id = 0; id < N; id++) p[id] = px[id] + pz[id];
-        op_apply(2, p, g, nnz, nnx);
-        op_apply(3, p, h, nnz, nnx);
+        if (o8) {
+            op8_apply(2, p, g, nnz, nnx);
+            op8_apply(3, p, h, nnz, nnx);
+        } else {
+            op_apply(2, p, g, nnz, nnx);
+            op_apply(3, p, h, nnz, nnx);
+        }
         for (int ix = 0; ix < nnx; ix++)
             for (int iz = 0; iz < nnz; iz++) {
                 size_t id = (size_t)iz + (size_t)ix * nnz;
@@ -839,8 +909,13 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
             }
         /* g = Hx p', h = Hz p' ; record */
         memset(q, 0, N * 8);
-        hxT_add(mg, q, nnz, nnx);
-        hzT_add(mh, q, nnz, nnx);
+        if (o8) {
+            op8T_add(2, mg, q, nnz, nnx);
+            op8T_add(3, mh, q, nnz, nnx);
+        } else {
+            hxT_add(mg, q, nnz, nnx);
+            hzT_add(mh, q, nnz, nnx);
+        }
         if (adj && (kt + 1) % d.dt_factor == 0) {
             int it = (kt + 1) / d.dt_factor - 1;
             if (it < d.real_nt)
@@ -865,8 +940,13 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                 mc[id] = kw1[id] * mPZ[id];
             }
         /* a = Gx vx, c = Gz vz */
-        gxT_add(ma, nvx, nnz, nnx);
-        gzT_add(mc, nvz, nnz, nnx);
+        if (o8) {
+            op8T_add(0, ma, nvx, nnz, nnx);
+            op8T_add(1, mc, nvz, nnz, nnx);
+        } else {
+            gxT_add(ma, nvx, nnz, nnx);
+            gzT_add(mc, nvz, nnz, nnx);
+        }
         memcpy(mvx, nvx, N * 8);
         memcpy(mvz, nvz, N * 8);
     }

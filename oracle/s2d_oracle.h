@@ -44,8 +44,8 @@ typedef struct {
     int fd_order;      /* "Order of FD Operator": 0 or 4 the reference's
                           4th-order operator (cpumodelling.cpp:121, NJ == 4);
                           8 the 8th-order staggered operator of this project
-                          (the reference runs no step for NJ != 4).  The
-                          gradient supports order 4 only. */
+                          (the reference runs no step for NJ != 4).
+                          orc_gradient handles both. */
 } orc_params;
 
 typedef struct {
