@@ -383,7 +383,125 @@ __global__ void residual_kernel(const float *seis, const float *obs, float *res,
     if (threadIdx.x == 0) atomicAdd(sumsq, part[0]);
 }
 
+// ---------------------------------------------------------------- 8th order
+//
+// Adjoint step of the 8th-order scheme: the algebra of the header above with
+// the 8-tap operators, in two cell-parallel passes (one thread per padded
+// cell, blockIdx.z = shot; the gathers read their neighbours from memory):
+//   pass 1: q = Hx^T(Lx bx mvx') + Hz^T(Lz bz mvz') (+ the adjoint source),
+//           mPX, mPZ, the new mpx, mpz, dJ/dkappa, and Kx kappa mPX,
+//           Kz kappa mPZ into the shot's two scratch fields;
+//   pass 2: mvx = Dbx mvx' + Gx^T(Kx kappa mPX), mvz likewise, and dJ/db.
+// Gather forms of the transposes, with c(j) the coefficients of forward row j
+// (dm8 / dp8, zero outside the grid):
+//   (G^T m)[i] = sum_k c_k(i-k) m[i-k] - c_k(i+1+k) m[i+1+k]
+//   (H^T m)[i] = sum_k c_k(i-1-k) m[i-1-k] - c_k(i+k) m[i+k]
+// (for the 4th-order pairs these are the gathers of adjoint_task).  The taps
+// reach 4 cells, inside the 8 ghost columns and rows, whose scratch stays 0.
+
+__device__ __forceinline__ size_t cell8(int x, int z, int ld) {
+    return (size_t)(x + S2D_GX) * (size_t)ld + (size_t)(z + S2D_GZ);
+}
+
+__global__ void __launch_bounds__(128) adjoint8_pressure(const StepArgs *__restrict__ A, int kt_off) {
+    const StepArgs a = *A;
+    const int kt = a.kt_base - kt_off;
+    if (kt < 0 || kt >= a.fd_nt) return;
+    const ShotDev &S = a.shots[blockIdx.z];
+    const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
+    if (z >= S.nnz || x >= S.nnx) return;
+    const int ld = S.ld, nnx = S.nnx, nnz = S.nnz;
+    const int pin = (kt + 1) & 1, pout = kt & 1;
+    const size_t id = cell8(x, z, ld);
+    const size_t F = (size_t)(nnx + 2 * S2D_GX) * (size_t)ld;
+    const float *__restrict__ mvx = S.st[pin][2];
+    const float *__restrict__ mvz = S.st[pin][3];
+    float q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j0 = x - 1 - k, j1 = x + k;
+        const size_t i0 = cell8(j0, z, ld), i1 = cell8(j1, z, ld);
+        q += comp(dp8(j0, nnx), k) * ((__ldg(S.xcoef + (j0 + S2D_GX)).w * __ldg(S.bx + i0)) * __ldg(mvx + i0));
+        q -= comp(dp8(j1, nnx), k) * ((__ldg(S.xcoef + (j1 + S2D_GX)).w * __ldg(S.bx + i1)) * __ldg(mvx + i1));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j0 = z - 1 - k, j1 = z + k;
+        const size_t i0 = cell8(x, j0, ld), i1 = cell8(x, j1, ld);
+        q += comp(dp8(j0, nnz), k) * ((__ldg(S.zcoef + (j0 + S2D_GZ)).w * __ldg(S.bz + i0)) * __ldg(mvz + i0));
+        q -= comp(dp8(j1, nnz), k) * ((__ldg(S.zcoef + (j1 + S2D_GZ)).w * __ldg(S.bz + i1)) * __ldg(mvz + i1));
+    }
+    // transpose of the receiver sampling (cpumodelling.cpp:356-360)
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    if (!(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 && slot < S.real_nt) {
+        const int j1 = __ldg(S.rec_ptr + x + 1);
+        for (int j = __ldg(S.rec_ptr + x); j < j1; ++j)
+            if (__ldg(S.rec_z + j) == z) q += __ldg(S.seis + (size_t)__ldg(S.rec_id + j) * S.real_nt + slot);
+    }
+    const float4 xq = __ldg(S.xcoef + (x + S2D_GX));  // Dax, Kx, Dbx, Lx
+    const float4 r = __ldg(S.zcoef + (z + S2D_GZ));   // Daz, Kz, Dbz, Lz
+    const bool merged = xq.x == 1.0f && r.x == 1.0f;   // the forward carried p alone here
+    const float mPX = S.st[pin][0][id] + q;
+    const float mPZ = merged ? mPX : S.st[pin][1][id] + q;
+    S.st[pout][0][id] = xq.x * mPX;
+    S.st[pout][1][id] = merged ? 0.0f : r.x * mPZ;
+    const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F;
+    const float pa = __ldg(pr + id);
+    S.grad[0][id] += merged ? pa * mPX : (xq.y * pa) * mPX + (r.y * __ldg(pr + F + id)) * mPZ;
+    const float k = __ldg(S.kappa + id);
+    S.scr[id] = (xq.y * k) * mPX;
+    S.scr[F + id] = (r.y * k) * mPZ;
+    if (x == S.src_x && z == S.src_z) S.srcadj[kt] = mPX;
+}
+
+__global__ void __launch_bounds__(128) adjoint8_velocity(const StepArgs *__restrict__ A, int kt_off) {
+    const StepArgs a = *A;
+    const int kt = a.kt_base - kt_off;
+    if (kt < 0 || kt >= a.fd_nt) return;
+    const ShotDev &S = a.shots[blockIdx.z];
+    const int z = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
+    if (z >= S.nnz || x >= S.nnx) return;
+    const int ld = S.ld, nnx = S.nnx, nnz = S.nnz;
+    const int pin = (kt + 1) & 1, pout = kt & 1;
+    const size_t id = cell8(x, z, ld);
+    const size_t F = (size_t)(nnx + 2 * S2D_GX) * (size_t)ld;
+    const float *__restrict__ sa = S.scr;
+    const float *__restrict__ sb = S.scr + F;
+    float gx = 0.0f, gz = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gx += comp(dm8(x - k, nnx), k) * __ldg(sa + cell8(x - k, z, ld));
+        gx -= comp(dm8(x + 1 + k, nnx), k) * __ldg(sa + cell8(x + 1 + k, z, ld));
+        gz += comp(dm8(z - k, nnz), k) * __ldg(sb + cell8(x, z - k, ld));
+        gz -= comp(dm8(z + 1 + k, nnz), k) * __ldg(sb + cell8(x, z + 1 + k, ld));
+    }
+    const float4 xq = __ldg(S.xcoef + (x + S2D_GX));
+    const float4 r = __ldg(S.zcoef + (z + S2D_GZ));
+    const float *__restrict__ mvx = S.st[pin][2];
+    const float *__restrict__ mvz = S.st[pin][3];
+    const float vx_in = __ldg(mvx + id), vz_in = __ldg(mvz + id);
+    S.st[pout][2][id] = xq.z * vx_in + gx;
+    S.st[pout][3][id] = r.z * vz_in + gz;
+    // buoyancy imaging: tbx = Lx g mvx', tbz = Lz h mvz' through the averages
+    // bx = (b[x] + b[x+1]) / 2, bz = (b[z] + b[z+1]) / 2
+    const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F;
+    const float tbx = (xq.w * __ldg(pr + 2 * F + id)) * vx_in;
+    const float tbz = (r.w * __ldg(pr + 3 * F + id)) * vz_in;
+    const float tbxm = x >= 1 ? (__ldg(S.xcoef + (x - 1 + S2D_GX)).w * __ldg(pr + 2 * F + id - ld)) * __ldg(mvx + id - ld)
+                              : 0.0f;
+    const float tbzm = z >= 1 ? (__ldg(S.zcoef + (z - 1 + S2D_GZ)).w * __ldg(pr + 3 * F + id - 1)) * __ldg(mvz + id - 1)
+                              : 0.0f;
+    S.grad[1][id] += 0.5f * ((tbx + tbxm) + (tbz + tbzm));
+}
+
 }  // namespace
+
+int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int nshots, void *stream) {
+    const dim3 blk(128), grd((nnz + 127) / 128, nnx, nshots);
+    adjoint8_pressure<<<grd, blk, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    adjoint8_velocity<<<grd, blk, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    return (int)cudaGetLastError();
+}
 
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream) {
     const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;

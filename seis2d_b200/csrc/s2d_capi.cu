@@ -1137,6 +1137,22 @@ int grad_alloc(Ctx *c, GradRun &g, size_t bytes, void **out) {
 
 // Adjoint launches for steps kt_top, kt_top-1, ..., kt_top-n+1, as replays of
 // a graph of `graph_chunk` launches.
+// The 8th-order adjoint over steps kt_top, kt_top-1, ..., kt_top-n+1: two
+// cell-parallel launches per step, direct (no graph).
+int run_adjoint8(Ctx *c, StepArgs args, int kt_top, int n, int nnx, int nnz, int nshots, int *launches) {
+    if (n <= 0) return S2D_OK;
+    StepArgs *args_d = c->args_d.as<StepArgs>();
+    args.kt_base = kt_top;
+    int e = launch_set_args(args, args_d, c->stream);
+    if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+    *launches += 1 + 2 * n;
+    for (int k = 0; k < n; ++k) {
+        e = launch_adjoint8(args_d, k, nnx, nnz, nshots, c->stream);
+        if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    return S2D_OK;
+}
+
 int run_adjoint(Ctx *c, Batch &b, GradRun &g, StepArgs args, int kt_top, int n, int grid, bool use_graph,
                 int *launches) {
     if (n <= 0) return S2D_OK;
@@ -1194,12 +1210,6 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     for (int s = 1; s < nshots; ++s)
         if (shots[s].model_id != shots[0].model_id)
             return fail(c, S2D_ERR_ARG, "all shots of a gradient call must use one model");
-    {
-        auto it = c->models.find(shots[0].model_id);
-        if (it != c->models.end() && it->second->fd_order != 4)
-            return fail(c, S2D_ERR_ARG, "the gradient exists for the 4th-order operator only (model has order %d)",
-                        it->second->fd_order);
-    }
     if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0))
         return fail(c, S2D_ERR_ARG, "wave parameters must be positive");
     CK(cudaSetDevice(c->device));
@@ -1246,6 +1256,13 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         }
         gk[s] = adj[s].grad[0];
         gb[s] = adj[s].grad[1];
+        // 8th-order adjoint: two scratch fields for its velocity gathers (ghosts stay 0)
+        if (b.order8) {
+            int e = grad_alloc(c, g, 2 * fb, &p);
+            if (e) return e;
+            CK(cudaMemsetAsync(p, 0, 2 * fb, c->stream));
+            adj[s].scr = static_cast<float *>(p);
+        }
         int e = grad_alloc(c, g, sizeof(float) * rs.fd_nt, &p);
         if (e) return e;
         CK(cudaMemsetAsync(p, 0, sizeof(float) * rs.fd_nt, c->stream));
@@ -1311,6 +1328,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
                        c->stream));
 
     LaunchCfg lc_fwd, lc_prod;
+    const int prod_variant = b.order8 ? kVariantO8Products : kVariantLdgProducts;
     {
         int e = base_config(c, b, &lc_fwd);
         // the gradient keeps every step's state (checkpoints at kt parity):
@@ -1319,7 +1337,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
             e = launch_config(c, b.max_tasks, &lc_fwd, kVariantLdg128, 128, 0);
         if (!e) e = layout_groups(c, b, lc_fwd);
         if (!e) e = launch_config(c, b.max_tasks, &lc_fwd, lc_fwd.variant, lc_fwd.block, lc_fwd.stages);
-        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts, 128, 0);
+        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, prod_variant, 128, 0);
         if (e) return e;
     }
     StepArgs fa{};
@@ -1345,6 +1363,13 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     // phase then each take whole rounds of tasks.
     int agrid = 1;
     auto backward_layout = [&]() -> int {
+        if (b.order8) {
+            // the 8th-order adjoint runs cell-parallel: the products kernel keeps its own layout
+            int e = layout_groups(c, b, lc_prod);
+            if (!e) e = launch_config(c, b.max_tasks, &lc_prod, prod_variant, 128, 0);
+            fa.total_tasks = batch_tasks(b);
+            return e;
+        }
         int bps = 0;
         if (adjoint_kernel_occupancy(128, c->opt_adj_minb, &bps) || bps < 1) bps = 1;
         const long resident = (long)c->sm_count * bps;
@@ -1410,7 +1435,8 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         }
         StepArgs a = aa;
         a.prod_kt0 = k0;
-        int e = run_adjoint(c, b, g, a, k0 + n - 1, n, agrid, use_graph, &launches);
+        int e = b.order8 ? run_adjoint8(c, a, k0 + n - 1, n, m.nnx, m.nnz, nshots, &launches)
+                         : run_adjoint(c, b, g, a, k0 + n - 1, n, agrid, use_graph, &launches);
         if (e) return e;
     }
     // ---- source term, chain rule, fold ----

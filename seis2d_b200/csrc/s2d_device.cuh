@@ -31,6 +31,28 @@ static __device__ __forceinline__ void dp_coef(int i, int n, float &c0, float &c
     else { c0 = 0.0f; c1 = 0.0f; }
 }
 
+// 8th-order staggered coefficients (1225/1024, -245/3072, 49/5120, -5/7168 in
+// float) and the coefficients of row i of the 8th-order D- (taps i-4 .. i+3,
+// f[i+k] - f[i-1-k] for k = 0..3) and D+ (taps i-3 .. i+4, f[i+1+k] - f[i-k]):
+// the reference's pairs (a0, a1), (1, 0) or 0 where the 8 taps would leave the
+// grid.
+constexpr float kC81 = 1225.0f / 1024.0f;
+constexpr float kC82 = -245.0f / 3072.0f;
+constexpr float kC83 = 49.0f / 5120.0f;
+constexpr float kC84 = -5.0f / 7168.0f;
+static __device__ __forceinline__ float4 dm8(int i, int n) {
+    if (i >= 4 && i <= n - 4) return make_float4(kC81, kC82, kC83, kC84);
+    float c0, c1;
+    dm_coef(i, n, c0, c1);
+    return make_float4(c0, c1, 0.0f, 0.0f);
+}
+static __device__ __forceinline__ float4 dp8(int i, int n) {
+    if (i >= 3 && i <= n - 5) return make_float4(kC81, kC82, kC83, kC84);
+    float c0, c1;
+    dp_coef(i, n, c0, c1);
+    return make_float4(c0, c1, 0.0f, 0.0f);
+}
+
 static __device__ __forceinline__ float comp(const float4 &v, int i) {
     return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }

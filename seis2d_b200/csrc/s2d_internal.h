@@ -60,6 +60,7 @@ struct ShotDev {
     float *prod;                   // [steps][4][field]: D-x vx, D-z vz, D+x p, D+z p of each step
     float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout, grad[1] = grad[0] + fstride)
     float *srcadj;                 // [fd_nt] adjoint pressure at the source after each step
+    float *scr;                    // 8th-order adjoint: Kx kappa mPX, Kz kappa mPZ (2 fields, ghosts 0)
     // element counts of the buffers above (device self-checks, S2D_DEVICE_CHECKS)
     size_t nfield;                 // every per-cell field
     size_t nprod;                  // prod
@@ -121,14 +122,15 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantO8 = 7 /* 8th-order operator, plain loads (112-row strips), models with
                                      S2D_MODEL_ORDER8; 3 blocks per SM */,
                    kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */,
-                   kVariantO8s = 9 /* the same with its windows in shared memory, 4 blocks per SM */ };
+                   kVariantO8s = 9 /* the same with its windows in shared memory, 4 blocks per SM */,
+                   kVariantO8Products = 10 /* kVariantO8 + S2D_STEP_PRODUCTS, gradient runs */ };
 
 // FD steps one launch of a variant advances.
 inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
 // Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 or 13 halo columns).
 inline bool ts_layout(int variant) {
     return variant == kVariantTs2 || variant == kVariantTs1 || variant == kVariantO8 || variant == kVariantO8r ||
-           variant == kVariantO8s;
+           variant == kVariantO8s || variant == kVariantO8Products;
 }
 inline bool order8_variant(int variant) {
     return variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8s;
@@ -136,7 +138,7 @@ inline bool order8_variant(int variant) {
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 ||
-           variant == kVariantO8 || variant == kVariantO8r;
+           variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8Products;
 }
 
 // Per-warp shared-memory delay lines of the two-step kernel (4 columns each):
@@ -163,6 +165,9 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
 // Adjoint FD step (step kt = args.kt_base - kt_off) and the gradient finalisation.
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream);
+// Adjoint FD step of the 8th-order scheme: two cell-parallel passes over
+// `nshots` shots of one nnx x nnz grid.
+int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int nshots, void *stream);
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm);
 // Sum the shots' accumulators (dJ/dkappa, dJ/db), apply the kappa = vp^2 rho,
 // b = 1/rho chain rule and fold the sponge onto the model.  kappa_fixed_rows:

@@ -668,25 +668,6 @@ __global__ void __launch_bounds__(128, 4) step_kernel_ts(const StepArgs *__restr
 // exact on lanes 1..30 and the velocities on lanes 2..29, so strips are 112
 // rows (the two-step kernel's layout, read from 112k-8) and lanes 2..29 write.
 
-constexpr float kC81 = 1225.0f / 1024.0f;
-constexpr float kC82 = -245.0f / 3072.0f;
-constexpr float kC83 = 49.0f / 5120.0f;
-constexpr float kC84 = -5.0f / 7168.0f;
-
-// Coefficients of row i of the 8th-order D- (taps i-4 .. i+3) and D+ (taps
-// i-3 .. i+4); the reference's pairs (a0, a1), (1, 0) or 0 near the edges.
-__device__ __forceinline__ float4 dm8(int i, int n) {
-    if (i >= 4 && i <= n - 4) return make_float4(kC81, kC82, kC83, kC84);
-    float c0, c1;
-    dm_coef(i, n, c0, c1);
-    return make_float4(c0, c1, 0.0f, 0.0f);
-}
-__device__ __forceinline__ float4 dp8(int i, int n) {
-    if (i >= 3 && i <= n - 5) return make_float4(kC81, kC82, kC83, kC84);
-    float c0, c1;
-    dp_coef(i, n, c0, c1);
-    return make_float4(c0, c1, 0.0f, 0.0f);
-}
 // c1 d1 + c2 d2 + c3 d3 + c4 d4 with the rounding fixed (innermost product
 // rounded, then three fused steps).
 __device__ __forceinline__ float dif8(const float4 &c, float d1, float d2, float d3, float d4) {
@@ -703,11 +684,13 @@ __device__ __forceinline__ float4 zdp8(const Lane<FAST> &ln, int i) {
     return dp8(ln.z0 + i, ln.nnz);
 }
 
-// New p at column P from vx at P-4 .. P+3 (w), old px, pz, kappa and vz at P.
+// New p at column P from vx at P-4 .. P+3 (w), old px, pz, kappa and vz at P;
+// the step's first two products (as p_cell forms them) in dxv, dzv.
 template <bool FAST>
 __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &xc,
                                             bool colm, const float4 (&w)[8], const float4 &px, const float4 &pz,
-                                            const float4 &kk, const float4 &vz, float4 &pxn, float4 &pzn) {
+                                            const float4 &kk, const float4 &vz, float4 &pxn, float4 &pzn,
+                                            float4 &dxv, float4 &dzv) {
     // vz rows z0-4 .. z0+6: the lane above's four (u), this lane's, the lane below's first three (d)
     const float u0 = __shfl_up_sync(kFull, vz.x, 1), u1 = __shfl_up_sync(kFull, vz.y, 1);
     const float u2 = __shfl_up_sync(kFull, vz.z, 1), u3 = __shfl_up_sync(kFull, vz.w, 1);
@@ -723,11 +706,14 @@ __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev 
     const float dx2 = dif8(cx, w[4].z - w[3].z, w[5].z - w[2].z, w[6].z - w[1].z, w[7].z - w[0].z);
     const float dx3 = dif8(cx, w[4].w - w[3].w, w[5].w - w[2].w, w[6].w - w[1].w, w[7].w - w[0].w);
     const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
-    float t0, t1;
-    p_cell(colm && (FAST || r0.x == 1.0f), xc.x, xc.y, r0.x, r0.y, px.x, pz.x, kk.x, dx0, dz0, pxn.x, pzn.x, t0, t1);
-    p_cell(colm && (FAST || r1.x == 1.0f), xc.x, xc.y, r1.x, r1.y, px.y, pz.y, kk.y, dx1, dz1, pxn.y, pzn.y, t0, t1);
-    p_cell(colm && (FAST || r2.x == 1.0f), xc.x, xc.y, r2.x, r2.y, px.z, pz.z, kk.z, dx2, dz2, pxn.z, pzn.z, t0, t1);
-    p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, t0, t1);
+    p_cell(colm && (FAST || r0.x == 1.0f), xc.x, xc.y, r0.x, r0.y, px.x, pz.x, kk.x, dx0, dz0, pxn.x, pzn.x, dxv.x,
+           dzv.x);
+    p_cell(colm && (FAST || r1.x == 1.0f), xc.x, xc.y, r1.x, r1.y, px.y, pz.y, kk.y, dx1, dz1, pxn.y, pzn.y, dxv.y,
+           dzv.y);
+    p_cell(colm && (FAST || r2.x == 1.0f), xc.x, xc.y, r2.x, r2.y, px.z, pz.z, kk.z, dx2, dz2, pxn.z, pzn.z, dxv.z,
+           dzv.z);
+    p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, dxv.w,
+           dzv.w);
     if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
         if (ln.sdz == 0) pxn.x += ln.amp;
         else if (ln.sdz == 1) pxn.y += ln.amp;
@@ -737,11 +723,12 @@ __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev 
     return make_float4(pxn.x + pzn.x, pxn.y + pzn.y, pxn.z + pzn.z, pxn.w + pzn.w);
 }
 
-// Velocities at column V from new p at V-3 .. V+4 (pw), old vx, vz and bx, bz at V.
+// Velocities at column V from new p at V-3 .. V+4 (pw), old vx, vz and bx, bz
+// at V; D+x p and D+z p in dxp, dzp.
 template <bool FAST>
 __device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S, int V, const float4 (&pw)[8],
                                           const float4 &vx, const float4 &vz, const float4 &bx, const float4 &bz,
-                                          float4 &vxn, float4 &vzn) {
+                                          float4 &vxn, float4 &vzn, float4 &dxp, float4 &dzp) {
     const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
     const float4 cx = dp8(V, S.nnx);
     const float ex0 = dif8(cx, pw[4].x - pw[3].x, pw[5].x - pw[2].x, pw[6].x - pw[1].x, pw[7].x - pw[0].x);
@@ -758,6 +745,8 @@ __device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S
     const float ez1 = dif8(zdp8(ln, 1), q.z - q.y, q.w - q.x, d0 - u3, d1 - u2);
     const float ez2 = dif8(zdp8(ln, 2), q.w - q.z, d0 - q.y, d1 - q.x, d2 - u3);
     const float ez3 = dif8(zdp8(ln, 3), d0 - q.w, d1 - q.z, d2 - q.y, d3 - q.x);
+    dxp = make_float4(ex0, ex1, ex2, ex3);
+    dzp = make_float4(ez0, ez1, ez2, ez3);
     vxn.x = upd(xc.z, vx.x, xc.w, bx.x, ex0);
     vxn.y = upd(xc.z, vx.y, xc.w, bx.y, ex1);
     vxn.z = upd(xc.z, vx.z, xc.w, bx.z, ex2);
@@ -775,7 +764,7 @@ __device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S
 // One (shot, strip, segment) task of the 8th-order step.  Columns read:
 // vx at xa-7 .. xb+6, px, pz, kappa, vz at xa-3 .. xb+3, bx, bz at xa .. xb-1
 // (inside the 8 ghost columns on each side).
-template <bool FAST>
+template <bool FAST, bool PROD>
 __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len, int kt,
                                         int par, bool rec_step, int slot, int lane) {
     const int xb = min(S.nnx, xa + seg_len);
@@ -800,6 +789,8 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
     const float *__restrict__ kap = S.kappa + off;
     const float *__restrict__ bxp = kap + fs;
     const float *__restrict__ bzp = kap + 2 * fs;
+    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+    float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 w[8], pw[8], zq[5];
 #pragma unroll
@@ -819,13 +810,17 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
         const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
         const bool colm = xc.x == 1.0f;
         const bool pz_live = !(FAST && colm);
-        float4 pxn, pzn;
+        float4 pxn, pzn, dxv, dzv;
         const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
-                                    ld4(kap + colP), vz, pxn, pzn);
+                                    ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
         const bool in_seg = P >= xa && P < xb;
         if (in_seg && ln.owner) {
             st4(pxo + colP, pxn);
             if (pz_live) st4(pzo + colP, pzn);
+            if (PROD) {
+                st4(pr + colP, dxv);
+                if (pz_live) st4(pr + F + colP, dzv);
+            }
         }
         if (rec && in_seg) record(ln, S, P, pn, slot);
 #pragma unroll
@@ -837,11 +832,15 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
         if (L >= xa + 7) {
             const int V = L - 7;
             const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-            float4 vxn, vzn;
-            v_update8(ln, S, V, pw, w[0], zq[0], ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+            float4 vxn, vzn, dxp, dzp;
+            v_update8(ln, S, V, pw, w[0], zq[0], ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
             if (ln.owner) {
                 st4(vxo + colV, vxn);
                 st4(vzo + colV, vzn);
+                if (PROD) {
+                    st4(pr + 2 * F + colV, dxp);
+                    st4(pr + 3 * F + colV, dzp);
+                }
             }
         }
     }
@@ -895,9 +894,9 @@ __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, in
         const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
         const bool colm = xc.x == 1.0f;
         const bool pz_live = !(FAST && colm);
-        float4 pxn, pzn;
+        float4 pxn, pzn, dxv, dzv;
         const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
-                                    ld4(kap + colP), vz, pxn, pzn);
+                                    ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
         const bool in_seg = P >= xa && P < xb;
         if (in_seg && ln.owner) {
             st4(pxo + colP, pxn);
@@ -914,8 +913,8 @@ __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, in
 #pragma unroll
             for (int i = 0; i < 7; ++i) pw[i] = o8_ring(ring, 1, V - 3 + i, lane);
             pw[7] = pn;
-            float4 vxn, vzn;
-            v_update8(ln, S, V, pw, w[0], vzV, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn);
+            float4 vxn, vzn, dxp, dzp;
+            v_update8(ln, S, V, pw, w[0], vzV, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
             if (ln.owner) {
                 st4(vxo + colV, vxn);
                 st4(vzo + colV, vzn);
@@ -944,7 +943,7 @@ __device__ __forceinline__ bool o8_in_bounds(const StepArgs &a, const ShotDev &S
 
 // MINB blocks of 4 warps per SM: 3 caps registers at 168 (some spill), 2
 // leaves the 224 the windows (84 registers) and stencils need.
-template <int MINB>
+template <int MINB, bool PROD>
 __global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
@@ -962,9 +961,9 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__re
         const int c = strip * S2D_TS_OUT - 8;
         // literal coefficients: every row of the strip 8th-order and undamped in z
         if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
-            o8_task<true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+            o8_task<true, PROD>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
         else
-            o8_task<false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+            o8_task<false, PROD>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
     }
 }
 
@@ -1052,9 +1051,11 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
     else if (variant == kVariantTs1)
         step_kernel_ts<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantO8)
-        step_kernel_o8<3><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        step_kernel_o8<3, false><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantO8r)
-        step_kernel_o8<2><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+        step_kernel_o8<2, false><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantO8Products)
+        step_kernel_o8<3, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantO8s)
         step_kernel_o8s<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
@@ -1084,8 +1085,9 @@ const void *kernel_of(int variant) {
     if (variant == kVariantLdg128) return (const void *)step_kernel_ldg<false, 4>;
     if (variant == kVariantTs2) return (const void *)step_kernel_ts<true>;
     if (variant == kVariantTs1) return (const void *)step_kernel_ts<false>;
-    if (variant == kVariantO8) return (const void *)step_kernel_o8<3>;
-    if (variant == kVariantO8r) return (const void *)step_kernel_o8<2>;
+    if (variant == kVariantO8) return (const void *)step_kernel_o8<3, false>;
+    if (variant == kVariantO8r) return (const void *)step_kernel_o8<2, false>;
+    if (variant == kVariantO8Products) return (const void *)step_kernel_o8<3, true>;
     if (variant == kVariantO8s) return (const void *)step_kernel_o8s;
     return (const void *)step_kernel_ldg<false, 1>;
 }
