@@ -214,8 +214,8 @@ S2D_API int s2d_derive_steps(const s2d_wave *wave, s2d_steps *out);
  * the grid; sponge, source and receivers as for order 4.  The reference
  * parses "Order of FD Operator" and steps only for 4 (cpumodelling.cpp:121).
  * All shots of one s2d_forward call must share the order; s2d_gradient
- * rejects order-8 models.  Stable for vmax dt / min(dx, dz) <= 0.549 (0.606
- * for order 4).
+ * returns the gradient of the 8th-order scheme for order-8 models.  Stable
+ * for vmax dt / min(dx, dz) <= 0.549 (0.606 for order 4).
  */
 S2D_API int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb,
                      const float *vp, const float *rho, unsigned flags, int *model_id);
