@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -196,14 +197,32 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch(workload):
-    """DRAM bytes per step launch from the committed ncu summary, if any."""
+def traffic_per_launch(workload, nshots):
+    """Measured DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum)
+    of one step launch over ``nshots`` shots, from the committed ncu summary
+    (profiles/traffic.json), scaled from the captured shot count by the
+    bytes that grow with the shot count (the state) plus the per-model part
+    that does not (the materials), as that file records them."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        t = json.load(open(p)).get(workload)
-        if t:
-            return float(t["dram_bytes_per_launch"])
-    return None
+    if not os.path.exists(p):
+        return None
+    t = json.load(open(p)).get(workload)
+    if not t:
+        return None
+    b = float(t["per_shot_bytes"]) * nshots + float(t.get("per_model_bytes", 0.0))
+    return {"bytes": b, "source": t["source"]}
+
+
+def dram_minimal_bytes(w, nshots):
+    """DRAM bytes per padded-cell update if the state crosses HBM once per FD
+    step and the materials once per launch for all shots of the model:
+    state 32 B per cell (24 B where the cell carries p alone), materials
+    12 B / nshots.  Cells carry p alone where both pressure dampings are 1:
+    columns and rows [nb-1, n+nb] of the padded grid."""
+    nnx, nnz, nb = w["nx"] + 2 * w["nb"], w["nz"] + 2 * w["nb"], w["nb"]
+    inner = (nnx - 2 * (nb - 1)) * (nnz - 2 * (nb - 1))
+    frac = inner / (nnx * nnz)
+    return 24.0 * frac + 32.0 * (1 - frac) + 12.0 / max(1, nshots)
 
 
 # ---------------------------------------------------------------------------
@@ -371,10 +390,36 @@ def extra_legs(device):
 # ---------------------------------------------------------------------------
 # reference CPU path (oracle/_ref, the reference's own src/src_cpu)
 
+def _ref_fd_nt(T, dt):
+    """FD steps of a run as the reference derives them: ceil of the float32
+    quotient Time / FD DT (src/src_cpu/cpumodelling.cpp:174)."""
+    return int(math.ceil(float(np.float32(T) / np.float32(dt))))
+
+
+def _write_ref_job(wd, w, vp, rho, src, T):
+    """The reference's input files for one shot of workload ``w``: raw float32
+    [nx][nz] models, a one-line shot file (split spread) and a job card
+    (src/src_cpu/json_parser.cpp:122-300, create_geometry.cpp:72-143)."""
+    np.ascontiguousarray(vp, np.float32).tofile(os.path.join(wd, "vp.bin"))
+    np.ascontiguousarray(rho, np.float32).tofile(os.path.join(wd, "rho.bin"))
+    with open(os.path.join(wd, "shots.txt"), "w") as f:
+        f.write(f"{src[0]:.6f},{src[1]:.6f},{int(w['nrec'])},0,{w['d']:.6f},1\n")
+    card = {"Velocity": "vp.bin", "Density": "rho.bin", "NX": w["nx"], "NZ": w["nz"], "DX": w["d"],
+            "DZ": w["d"], "Time": T, "FD DT": w["dt"], "DATA DT": w["dt"], "Frequency": w["f"],
+            "Read source receiver flag": 1, "if choice=0, Geometry file": "NA",
+            "if choice=1, Shot file": "shots.txt", "Output Directory": "out", "Free surface": 0,
+            "Job type New or Restart": "New", "Order of FD Operator": 4}
+    with open(os.path.join(wd, "job.json"), "w") as f:
+        f.write('"Model" : "comment"\n')
+        for k, v in card.items():
+            f.write(f'    "{k}" : "{v!r}"\n' if isinstance(v, float) else f'    "{k}" : "{v}"\n')
+
+
 def ref_cpu_rate(w, nsteps_pair=(4, 84), threads=None, tmpdir=None):
     """Gcell/s of the reference CPU time loop on one shot of workload ``w``:
-    two runs of nsteps_pair FD steps, rate from the difference (set-up cancels)."""
-    from seis2d_b200 import formats as F
+    two runs of nsteps_pair FD steps, rate from the difference (set-up cancels).
+    Runs only the reference binary (oracle/_ref); imports nothing of the
+    modelling package."""
     nb = w["nb"]
     binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref" if nb == 32 else f"seis_ref_nb{nb}")
     if not os.path.exists(binary):
@@ -385,27 +430,16 @@ def ref_cpu_rate(w, nsteps_pair=(4, 84), threads=None, tmpdir=None):
     threads = threads or os.cpu_count()
     env["OMP_NUM_THREADS"] = str(threads)
     with tempfile.TemporaryDirectory(dir=tmpdir) as wd:
-        F.write_model(os.path.join(wd, "vp.bin"), vp)
-        F.write_model(os.path.join(wd, "rho.bin"), rho)
-        F.write_shotfile(os.path.join(wd, "shots.txt"),
-                         [(src[0][0], src[0][1], w["nrec"], 0, w["d"], 1)])
         os.makedirs(os.path.join(wd, "out"))
         for n in nsteps_pair:
             T = n * w["dt"]
-            F.write_jobcard(os.path.join(wd, "job.json"), {
-                "Velocity": "vp.bin", "Density": "rho.bin", "NX": w["nx"], "NZ": w["nz"], "DX": w["d"],
-                "DZ": w["d"], "Time": T, "FD DT": w["dt"], "DATA DT": w["dt"], "Frequency": w["f"],
-                "Read source receiver flag": 1, "if choice=0, Geometry file": "NA",
-                "if choice=1, Shot file": "shots.txt", "Output Directory": "out", "Free surface": 0,
-                "Job type New or Restart": "New", "Order of FD Operator": 4})
+            _write_ref_job(wd, w, vp, rho, src[0], T)
             r = subprocess.run([binary, "--no-stability", "--time", "job.json"], cwd=wd, env=env,
                                capture_output=True, text=True)
             if r.returncode != 0:
                 return None, f"reference exited {r.returncode}"
             t = [float(l.split()[1]) for l in r.stdout.splitlines() if l.startswith("ORACLE_TIME")]
-            from seis2d_b200 import Wave, derive_steps
-            nsteps = derive_steps(Wave(T, w["dt"], w["dt"], w["f"]))["fd_nt"]
-            times.append((t[0], nsteps))
+            times.append((t[0], _ref_fd_nt(T, w["dt"])))
     (t0, n0), (t1, n1) = times
     cells = (w["nx"] + 2 * nb) * (w["nz"] + 2 * nb)
     rate = cells * (n1 - n0) / max(t1 - t0, 1e-9) / 1e9
@@ -536,11 +570,20 @@ def main():
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    loop_ms = alg_bytes = 0.0
+    fd_launches = 0
+    variants = set()
     ev0.record()
     for _ in range(args.steps):
         ctx.forward(shots, wave, kt_begin=kt, kt_count=chunk, out=seis_dev, sync=False)
         st = ctx.last_stats
         launches += st.kernel_launches
+        # the library's own CUDA events around its step launches, on the
+        # stream it launches them on, and the algorithmic bytes of those steps
+        loop_ms += st.loop_ms
+        alg_bytes += st.alg_bytes
+        fd_launches += -(-chunk // (2 if st.variant == 5 else 1))
+        variants.add(int(st.variant))
         kt += chunk
     ev1.record()
     barrier()
@@ -554,27 +597,19 @@ def main():
     value = total_cells / (ms * 1e-3) / 1e9
     ms_per_step = ms / args.steps
 
-    # per-launch roofline of the step kernel (one launch per FD step), timed
-    # by the library's CUDA events on the stream it launches on
-    kt_r = kt
-    n_r = min(chunk, fd_nt - kt_r)
-    roof = None
-    if n_r > 0:
-        ctx.forward(shots, wave, kt_begin=kt_r, kt_count=n_r, out=seis_dev)
-        st = ctx.last_stats
-        # one launch per FD step (two for the two-step variant, whose
-        # algorithmic bytes the library counts per pass)
-        spl = 2 if st.variant == 5 else 1
-        n_launch = max(1, n_r // spl)
-        per_launch_s = st.loop_ms * 1e-3 / n_launch
-        bytes_launch = st.alg_bytes / n_launch
-        peak, peak_kind = measured_peak()
-        achieved = st.alg_bytes / (st.loop_ms * 1e-3) / 1e9
-        tr = traffic_per_launch(args.workload)
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": tr, "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
-                "bytes_per_cell_update": st.alg_bytes / st.cell_updates, "launch_ms": per_launch_s * 1e3,
-                "fd_steps_per_launch": spl}
+    # roofline of the step kernel over exactly the timed calls: algorithmic
+    # bytes of the launches / their device time (library events on its stream)
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (loop_ms * 1e-3) / 1e9
+    tr = traffic_per_launch(args.workload, nshots)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tr["bytes"] if tr else None, "traffic_source": tr["source"] if tr else None,
+            "peak_source": peak_kind, "bytes_per_launch": alg_bytes / max(1, fd_launches),
+            "bytes_per_cell_update": alg_bytes / (cells_step * chunk * args.steps),
+            "dram_minimal_bytes_per_cell_update": dram_minimal_bytes(w, nshots),
+            "launch_ms": loop_ms / max(1, fd_launches), "launches": fd_launches,
+            "fd_steps_per_launch": 2 if variants == {5} else 1,
+            "timed_region": f"the {args.steps} timed calls ({fd_launches} step launches)"}
 
     # ---- end to end through the C ABI from pinned host memory ----
     e2e = None

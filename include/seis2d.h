@@ -373,6 +373,11 @@ S2D_API int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, i
 /* Size of the device scratch s2d_forward_static works in (32 MiB). */
 #define S2D_STATIC_SCRATCH_BYTES (32u << 20)
 
+/* flags for s2d_forward_static (bits of their own: no other flag of this
+ * header is accepted there) */
+#define S2D_STATIC_MODEL_DEVICE 0x100u /* vp and rho are device pointers       */
+#define S2D_STATIC_SEIS_DEVICE 0x200u  /* seis_out is a device pointer         */
+
 /*
  * One shot of forward modelling that allocates no device memory.  No
  * counterpart in the reference.
@@ -388,13 +393,17 @@ S2D_API int s2d_run_jobcard_rank(const char *jobcard_path, int device, int nb, i
  * that needs more returns S2D_ERR_NOMEM with the size it needs in errbuf.
  *
  * Same scheme, numbers and output layout as s2d_forward for one shot with the
- * reference Ricker wavelet: model [nx][nz] (vp, rho), sponge width nb, wave,
- * shot->src and shot->rec (shot->model_id is ignored), seis_out
- * [nrec][real_nt].  flags: S2D_MODEL_DEVICE (vp, rho are device pointers),
- * S2D_SEIS_DEVICE (seis_out is a device pointer); otherwise host pointers.
- * stream: a cudaStream_t, NULL for the legacy default stream; the call returns
- * when the shot is done.  errbuf (optional, errlen bytes) receives a message
- * on failure.
+ * reference Ricker wavelet and the reference's 4th-order operator without a
+ * free surface: model [nx][nz] (vp, rho), sponge width nb, wave, shot->src and
+ * shot->rec (shot->model_id is ignored), seis_out [nrec][real_nt].  flags:
+ * S2D_STATIC_MODEL_DEVICE (vp, rho are device pointers) and
+ * S2D_STATIC_SEIS_DEVICE (seis_out is a device pointer), independently;
+ * otherwise host pointers.  Any other bit (S2D_MODEL_FREE_SURFACE and
+ * S2D_MODEL_ORDER8 included: this entry has neither option) returns
+ * S2D_ERR_ARG.  stream: a cudaStream_t, NULL for the legacy default stream;
+ * the call returns when the shot is done.  A failed device self-check (builds
+ * with S2D_DEVICE_CHECKS) returns S2D_ERR_CUDA.  errbuf (optional, errlen
+ * bytes) receives a message on failure.
  *
  * Every call on a device shares the one scratch array, which keeps the last
  * call's contents; each call clears what must start at zero.  Calls whose

@@ -34,6 +34,8 @@ S2D_MODEL_FREE_SURFACE = 0x2
 S2D_MODEL_ORDER8 = 0x4
 S2D_GRAD_MISFIT = 0x10
 S2D_GRAD_DEVICE = 0x20
+S2D_STATIC_MODEL_DEVICE = 0x100
+S2D_STATIC_SEIS_DEVICE = 0x200
 
 
 class Coord(C.Structure):

@@ -101,6 +101,11 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     if (!(wave->fd_dt > 0) || !(wave->real_dt > 0) || !(wave->rec_len > 0) || !(wave->dom_freq > 0))
         return say(eb, el, S2D_ERR_ARG, "wave parameters must be positive");
     if (shot->nrec < 0 || (shot->nrec > 0 && !shot->rec)) return say(eb, el, S2D_ERR_ARG, "bad receiver list");
+    if (flags & ~(S2D_STATIC_MODEL_DEVICE | S2D_STATIC_SEIS_DEVICE))
+        return say(eb, el, S2D_ERR_ARG,
+                   "s2d_forward_static: unsupported flag bits 0x%x (accepted: S2D_STATIC_MODEL_DEVICE, "
+                   "S2D_STATIC_SEIS_DEVICE; no free surface or 8th-order operator here)",
+                   flags & ~(S2D_STATIC_MODEL_DEVICE | S2D_STATIC_SEIS_DEVICE));
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
         cudaGetLastError();
@@ -114,7 +119,7 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     const int ld = leading_dim(nnz), nxa = nnx + 2 * S2D_GX;
     const size_t F = (size_t)nxa * ld;
     const int nrec = shot->nrec;
-    const bool host_model = !(flags & S2D_MODEL_DEVICE), host_seis = !(flags & S2D_SEIS_DEVICE);
+    const bool host_model = !(flags & S2D_STATIC_MODEL_DEVICE), host_seis = !(flags & S2D_STATIC_SEIS_DEVICE);
 
     // positions (reference float rules) and receiver tables grouped by column
     int sx, sz;
@@ -260,6 +265,9 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     sd.rec_id = reinterpret_cast<const int *>(at(o_rid));
     sd.seis = host_seis ? reinterpret_cast<float *>(at(o_seis)) : seis_out;
     sd.real_nt = rs.real_nt;
+    sd.nfield = F;          // sizes for the kernels' self-checks (S2D_DEVICE_CHECKS builds)
+    sd.nrec = nrec;
+    sd.nseis = seis_n;
     sd.zfast_lo = sd.zfast_hi = 0;  // every strip takes the general row path
     int bps = 1;
     if (rc == S2D_OK && (step_kernel_occupancy(kVariantLdg, 128, 0, &bps) || bps < 1)) bps = 1;
@@ -309,6 +317,12 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     if (host_seis && seis_n)
         SCK(cudaMemcpyAsync(seis_out, at(o_seis), seis_n * sizeof(float), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
+    // the step kernel's device error word: nonzero only when a self-check of a
+    // S2D_DEVICE_CHECKS build skipped a task (the plain-load kernel has no waits)
+    int dev_err = 0;
+    SCK(cudaMemcpy(&dev_err, at(o_err), sizeof(int), cudaMemcpyDeviceToHost));
+    if (rc == S2D_OK && dev_err)
+        rc = say(eb, el, S2D_ERR_CUDA, "s2d_forward_static: device self-check failed (error word 0x%x)", dev_err);
 #undef SCK
     if (prev >= 0) cudaSetDevice(prev);
     return rc;
