@@ -16,6 +16,11 @@ Needs the reference tree (to build the binary), so it runs in the development
 container; the committed .npz files are what the tests use everywhere.
 Usage: python tests/golden/make_golden.py [case ...]
        python tests/golden/make_golden.py --geometry   (geometry_cases.json)
+       python tests/golden/make_golden.py --shipped    (shipped/: the reference's
+           own two job cards and shot files, copied as they are, with the
+           reference binary's parse, every shot's geometry and its stability
+           verdicts for a few velocity bounds; the model files those cards
+           name are not distributed, and the parse and geometry need none)
 """
 from __future__ import annotations
 
@@ -36,13 +41,23 @@ from cases import CASES, explicit_geometry, model  # noqa: E402
 from seis2d_b200 import formats as F  # noqa: E402
 
 
-def run_case(name: str, c: dict) -> dict:
-    nb = c["nb"]
-    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref" if nb == 32 else f"seis_ref_nb{nb}")
-    args = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"]
+def _ref_root():
+    """SeisAcoMod2D checkout: $SEISACOMOD2D_REF, else ``reference`` beside the repository."""
+    return os.environ.get("SEISACOMOD2D_REF") or os.path.join(os.path.dirname(ROOT), "reference")
+
+
+def _make_ref(nb=32):
+    args = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
+            f"REF_SRC={os.path.join(_ref_root(), 'src', 'src_cpu')}"]
     if nb != 32:
         args.append(f"NB={nb}")
     subprocess.run(args, check=True)
+
+
+def run_case(name: str, c: dict) -> dict:
+    nb = c["nb"]
+    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref" if nb == 32 else f"seis_ref_nb{nb}")
+    _make_ref(nb)
     vp, rho = model(c["model"], c["nx"], c["nz"], c["dx"], c["dz"])
     with tempfile.TemporaryDirectory() as wd:
         F.write_model(os.path.join(wd, "vp.bin"), vp)
@@ -105,7 +120,7 @@ GEOMETRY_CASES = [
 
 
 def run_geometry_cases():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    _make_ref()
     binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref")
     out = []
     for (nx, nz, dx, dz, sx, sz, nrec, near, sp, gt) in GEOMETRY_CASES:
@@ -132,7 +147,55 @@ def run_geometry_cases():
     return len(out)
 
 
+# The reference's shipped cards (input/*.json) and the shot files they name
+# (geometry/*.json), and velocity bounds (vmin, vmax) around each card's
+# stability (dt <= 0.606 h_min / v_max) and dispersion (2 f <= v_min / (5 h_max))
+# limits: check_stability.cpp:8-72.
+SHIPPED = {
+    "sigsbee2a_3201x1201z.json": [(1500.0, 4500.0), (1500.0, 4700.0), (1300.0, 4500.0), (1371.0, 4600.0)],
+    "twoLayer_model_5000x5000z.json": [(1500.0, 3000.0), (1499.0, 3000.0), (2000.0, 6100.0), (1500.0, 6060.0)],
+}
+
+
+def run_shipped(ref_root):
+    import shutil
+    _make_ref()
+    binary = os.path.join(ROOT, "oracle", "_ref", "seis_ref")
+    dest = os.path.join(HERE, "shipped")
+    for sub in ("input", "geometry"):
+        os.makedirs(os.path.join(dest, sub), exist_ok=True)
+    out = {}
+    for card, bounds in SHIPPED.items():
+        shutil.copyfile(os.path.join(ref_root, "input", card), os.path.join(dest, "input", card))
+        text = open(os.path.join(dest, "input", card)).read()
+        shotfile = [l.split(":", 1)[1].strip().strip('"') for l in text.splitlines() if "Shot file" in l][0]
+        shutil.copyfile(os.path.join(ref_root, "input", shotfile), os.path.join(dest, "input", shotfile))
+        verdicts = []
+        with tempfile.TemporaryDirectory() as wd:
+            for sub in ("input", "geometry"):
+                shutil.copytree(os.path.join(dest, sub), os.path.join(wd, sub))
+            cwd = os.path.join(wd, "input")
+            r = subprocess.run([binary, "--dump-job", "dump.txt", card], cwd=cwd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"{card}: reference exited {r.returncode}\n{r.stdout[-2000:]}")
+            dump = open(os.path.join(cwd, "dump.txt")).read()
+            for vmin, vmax in bounds:
+                r = subprocess.run([binary, "--dump-job", "chk.txt", "--check", repr(vmin), repr(vmax), card],
+                                   cwd=cwd, capture_output=True, text=True)
+                stable = r.returncode == 0 and open(os.path.join(cwd, "chk.txt")).read().endswith("STABLE\n")
+                verdicts.append({"vmin": vmin, "vmax": vmax, "stable": stable, "exit": r.returncode})
+        with open(os.path.join(dest, card.replace(".json", ".dump.txt")), "w") as f:
+            f.write(dump)
+        out[card] = verdicts
+    with open(os.path.join(dest, "stability.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    return {k: len(v) for k, v in out.items()}
+
+
 def main(argv):
+    if argv[:1] == ["--shipped"]:
+        print(json.dumps(run_shipped(argv[1] if len(argv) > 1 else _ref_root())))
+        return
     if argv == ["--geometry"]:
         print(json.dumps({"geometry_cases": run_geometry_cases()}))
         return
