@@ -144,8 +144,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 72 steps
- *                 spends 36 of them on 8 candidate configurations, one untimed
+ *                 shape (models, grids, shot counts) with at least 80 steps
+ *                 spends 40 of them on 9 candidate configurations, one untimed
  *                 and three timed launches each, in rounds (the results do not
  *                 change: every candidate computes the same bits), times them
  *                 with events and keeps the fastest per FD step for that shape
@@ -156,7 +156,10 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 compiled for 128 registers, 4 plain loads compiled for 128
  *                 registers (default), 5 two FD steps per launch (the state
  *                 crosses HBM once per two steps; odd step counts end with one
- *                 one-step launch); s2d_gradient always runs one step per launch.
+ *                 one-step launch), 11 a CTA of 8 warps on adjacent strips fed
+ *                 by a producer warp's 2-D TMA tensor loads through a 4-stage
+ *                 shared-memory ring (one block of 288 threads per SM);
+ *                 s2d_gradient always runs one step per launch.
  *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in
  *                 shared memory at 4 (each setting applies to its own order)

@@ -15,7 +15,13 @@
 // and accumulates the imaging terms
 //   dJ/dkappa += Kx a mPX + Kz c mPZ,  dJ/dbx += Lx g mvx',  dJ/dbz += Lz h mvz'
 // with a, c, g, h of step kt saved by the forward (S2D_STEP_PRODUCTS); the
-// last two go straight into dJ/db through the buoyancy averages.
+// last two go straight into dJ/db through the buoyancy averages.  All shots of
+// a gradient call share one model, so they share one accumulator pair
+// (dJ/dkappa, dJ/db): the terms are added with vector atomics (red.global
+// .add.v4.f32), which keeps the pair in L2 instead of reading and writing a
+// pair per shot from DRAM every step.  The order in which the shots' terms
+// of one step arrive is not fixed, so gradients of several shots are
+// reproducible to rounding, not bit for bit; one shot's are bit-exact.
 //
 // The transposes are the gather forms of the reference's operators, edge rows
 // included: with (c0(j), c1(j)) the coefficient pair of forward row j,
@@ -36,7 +42,6 @@ __device__ __forceinline__ float xc1m(int i, int n) { float c0, c1; dm_coef(i, n
 __device__ __forceinline__ float xc0p(int i, int n) { float c0, c1; dp_coef(i, n, c0, c1); return c0; }
 __device__ __forceinline__ float xc1p(int i, int n) { float c0, c1; dp_coef(i, n, c0, c1); return c1; }
 
-__device__ __forceinline__ float4 ldrw(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
 // (H^T m) at the lane's 4 rows from m at those rows and the neighbours' edge
 // values (up_z = m[z0-2], up_w = m[z0-1], dn_x = m[z0+4]); pairs of rows z0-2 .. z0+4.
@@ -115,7 +120,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     lane_setup(ln, S, c, lane, kt);
     const int z0 = ln.z0;
     const int pin = (kt + 1) & 1, pout = kt & 1;
-    const size_t off = (size_t)(z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t off = (size_t)(ln.zl + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
     // Every buffer below is distinct: restrict lets the compiler issue the
     // accumulator and product loads ahead of the state stores.  (Per-field
@@ -168,8 +173,6 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         if (upd) {
             pa = ld4(pr + colQ);
             if (pz_live) pc = ld4(pr + F + colQ);
-            tk = ldrw(gk + colQ);
-            tb = ldrw(gb + colQ);
         }
         if (img) {
             pg = ld4(pr + 2 * F + colQ);
@@ -223,7 +226,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             tk.y += m1 ? pa.y * mPX.y : (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
             tk.z += m2 ? pa.z * mPX.z : (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
             tk.w += m3 ? pa.w * mPX.w : (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
-            st4(gk + colQ, tk);
+            atomicAdd(reinterpret_cast<float4 *>(gk + colQ), tk);
             if (Q == S.src_x && ln.sdz >= 0 && ln.sdz < 4) S.srcadj[kt] = comp(mPX, ln.sdz);
         }
         adj_ring(ring, 2, Q, lane) = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
@@ -252,7 +255,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
                 tb.y += 0.5f * ((tbx.y + px.y) + (tbz.y + tbz.x));
                 tb.z += 0.5f * ((tbx.z + px.z) + (tbz.z + tbz.y));
                 tb.w += 0.5f * ((tbx.w + px.w) + (tbz.w + tbz.z));
-                st4(gb + colQ, tb);
+                atomicAdd(reinterpret_cast<float4 *>(gb + colQ), tb);
             }
             tbp = tbx;
         }
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(128) adjoint8_pressure(const StepArgs *__restr
     S.st[pout][1][id] = merged ? 0.0f : r.x * mPZ;
     const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F;
     const float pa = __ldg(pr + id);
-    S.grad[0][id] += merged ? pa * mPX : (xq.y * pa) * mPX + (r.y * __ldg(pr + F + id)) * mPZ;
+    atomicAdd(S.grad[0] + id, merged ? pa * mPX : (xq.y * pa) * mPX + (r.y * __ldg(pr + F + id)) * mPZ);
     const float k = __ldg(S.kappa + id);
     S.scr[id] = (xq.y * k) * mPX;
     S.scr[F + id] = (r.y * k) * mPZ;
@@ -491,7 +494,7 @@ __global__ void __launch_bounds__(128) adjoint8_velocity(const StepArgs *__restr
                               : 0.0f;
     const float tbzm = z >= 1 ? (__ldg(S.zcoef + (z - 1 + S2D_GZ)).w * __ldg(pr + 3 * F + id - 1)) * __ldg(mvz + id - 1)
                               : 0.0f;
-    S.grad[1][id] += 0.5f * ((tbx + tbxm) + (tbz + tbzm));
+    atomicAdd(S.grad[1] + id, 0.5f * ((tbx + tbxm) + (tbz + tbzm)));
 }
 
 }  // namespace
@@ -521,7 +524,7 @@ int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
         smem);
 }
 
-int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
+int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, int nacc, const int *src_cells,
                              const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
                              int ld, int kappa_fixed_rows, float *tmp2, float *gvp_pad, float *grho_pad,
                              float *grad_vp, float *grad_rho, void *stream) {
@@ -530,7 +533,7 @@ int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, con
     const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
     add_source_terms<<<1, 1, 0, st>>>(gk, src_cells, src_vals, nshots);
     dim3 blk(256), grd((nnz + 255) / 256, nnx);
-    sum_shots<<<grd, blk, 0, st>>>(gk, gb, nshots, nnx, nnz, ld, tmp2, tmp2 + F);
+    sum_shots<<<grd, blk, 0, st>>>(gk, gb, nacc, nnx, nnz, ld, tmp2, tmp2 + F);
     chain_rule<<<grd, blk, 0, st>>>(tmp2, tmp2 + F, vp, rho, nx, nz, nb, ld, kappa_fixed_rows, gvp_pad, grho_pad);
     dim3 grd2((nz + 255) / 256, nx);
     fold_sponge<<<grd2, blk, 0, st>>>(gvp_pad, grho_pad, nx, nz, nb, ld, grad_vp, grad_rho);

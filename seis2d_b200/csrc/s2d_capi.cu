@@ -5,6 +5,7 @@
 // shot loop of cpumodelling.cpp:326-380 becomes either one batched launch per
 // FD step covering all shots (default) or the reference's shot-after-shot
 // order (S2D_PLAIN).  The per-step launches are captured as a CUDA graph.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -101,6 +102,9 @@ struct Batch {
     float *seis_d = nullptr;         // where the kernels record
     size_t seis_elems = 0;
     long max_tasks = 0;              // largest task count of one launch sequence
+    bool layout_tma = false;         // the groups are laid out in TMA tasks (kTmaWarps pairs each)
+    std::vector<int> table;          // caller's shot index of each slot of the device shot table
+    DevBuf tmaps_d;                  // TMA kernel: state maps per table slot, then material maps
 };
 
 // Device buffers of finished batches, kept for reuse by the next batch of
@@ -263,11 +267,17 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
     lc.stages = std::max(2, std::min(16, stages));
     const bool ldg = plain_loads(lc.variant);
     const bool ts = ts_layout(lc.variant);
+    const bool tma = tma_variant(lc.variant);
     if (ldg || ts) {
         lc.block = 128;
         lc.stages = 0;
     }
+    if (tma) {
+        lc.block = kTmaThreads;
+        lc.stages = 0;
+    }
     lc.smem = ldg ? 0
+              : tma ? kTmaSmemBytes
               : ts ? (size_t)(lc.block / 32) * (lc.variant == kVariantO8s ? kO8sWarpBytes : kTsWarpBytes)
                    : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
@@ -279,7 +289,8 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
         return fail(c, S2D_ERR_ARG, "launch configuration (variant %d, block %d, stages %d) cannot run", lc.variant,
                     lc.block, lc.stages);
     const long resident = (long)c->sm_count * bps;
-    const long needed = (max_tasks * 32 + lc.block - 1) / lc.block;
+    // warp tasks, or CTA tasks for the TMA kernel
+    const long needed = tma ? max_tasks : (max_tasks * 32 + lc.block - 1) / lc.block;
     lc.grid = (int)std::max<long>(1, std::min<long>(resident, std::max<long>(needed, 1)));
     *out = lc;
     return S2D_OK;
@@ -317,28 +328,34 @@ int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
 // Segment lengths, segment counts and task ranges of the batch's groups for
 // `resident_warps` warps looping over the tasks of a launch; uploaded when
 // `key` differs from the layout in place.
-int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<long> &key, bool ts = false) {
+// With `tma` a task is a CTA's: kTmaWarps (shot, strip) pairs of a group
+// over one segment, and `resident_warps` counts resident CTAs.
+int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<long> &key, bool ts = false,
+                      bool tma = false) {
     if (b.layout == key) return S2D_OK;
     for (size_t gi = 0; gi < b.groups.size(); ++gi)
         b.groups[gi].nstrips = ts ? num_strips_ts(b.group_nnz[gi]) : num_strips(b.group_nnz[gi]);
+    auto per_seg = [&](const GroupDev &g, int nshots) {
+        return tma ? (long)tma_blocks(nshots, g.nstrips) : (long)nshots * g.nstrips;
+    };
     long per_seg_total = 0;
-    for (auto &g : b.groups) per_seg_total += (long)g.nshots * g.nstrips;
+    for (auto &g : b.groups) per_seg_total += per_seg(g, g.nshots);
     long max_tasks = 0;
     int task = 0;
     for (size_t gi = 0; gi < b.groups.size(); ++gi) {
         GroupDev &g = b.groups[gi];
         const int nnx = b.group_nnx[gi];
         // plain mode: every shot is a group of its own and runs alone
-        const long tasks_per_seg = b.plain ? (long)g.nstrips : per_seg_total;
+        const long tasks_per_seg = b.plain ? per_seg(g, 1) : per_seg_total;
         g.seg_len = c->opt_seg_len > 0 ? std::min(c->opt_seg_len, nnx)
                                        : choose_seg_len(nnx, tasks_per_seg, resident_warps, ts ? 12 : 6);
         g.nsegs = (nnx + g.seg_len - 1) / g.seg_len;
         if (b.plain) {
             g.task_begin = 0;
-            max_tasks = std::max<long>(max_tasks, (long)g.nstrips * g.nsegs);
+            max_tasks = std::max<long>(max_tasks, per_seg(g, 1) * g.nsegs);
         } else {
             g.task_begin = task;
-            task += g.nshots * g.nstrips * g.nsegs;
+            task += (int)(per_seg(g, g.nshots) * g.nsegs);
             max_tasks = task;
         }
     }
@@ -349,6 +366,7 @@ int layout_groups_for(Ctx *c, Batch &b, long resident_warps, const std::vector<l
     CK(cudaStreamSynchronize(c->stream));
     b.max_tasks = max_tasks;
     b.layout = key;
+    b.layout_tma = tma;
     return S2D_OK;
 }
 
@@ -358,10 +376,12 @@ int layout_groups(Ctx *c, Batch &b, const LaunchCfg &lc) {
     const int v = lc.variant == kVariantTs1 ? kVariantTs2 : lc.variant;
     const std::vector<long> key = {v, lc.block, lc.stages, c->opt_seg_len};
     if (b.layout == key) return S2D_OK;
-    // resident warps of the configuration (its grid when the work is smaller)
+    // resident warps of the configuration (its grid when the work is smaller);
+    // resident CTAs for the TMA kernel, whose tasks are CTA tasks
     LaunchCfg full;
     int e = launch_config(c, 1L << 40, &full, v, lc.block, lc.stages);
     if (e) return e;
+    if (tma_variant(v)) return layout_groups_for(c, b, (long)full.grid, key, false, true);
     return layout_groups_for(c, b, (long)full.grid * (full.block / 32), key, ts_layout(v));
 }
 
@@ -412,6 +432,25 @@ void fast_rows(const Model &m, float fd_dt, int *lo, int *hi, float *kz) {
     *kz = kzi;
 }
 
+// Columns whose coefficients are the interior constants (ShotDev::xfast_lo):
+// damp2a = damp2b = 1, kx*damp2a1 = kx*damp2b1 = (float)kx and both operator
+// pairs (a0, a1), columns [2, nnx-3].
+void fast_cols(const Model &m, float fd_dt, int *lo, int *hi, float *kx) {
+    const double dtdx = (double)(fd_dt * (1.0f / m.dx));  // as build_coef forms it
+    const float kxi = (float)(dtdx * 1.0f);
+    auto ok = [&](int x) {
+        return x >= 2 && x <= m.nnx - 3 && m.damp2a[x] == 1.0f && m.damp2b[x] == 1.0f &&
+               (float)(dtdx * m.damp2a1[x]) == kxi && (float)(dtdx * m.damp2b1[x]) == kxi;
+    };
+    int a = 0;
+    while (a < m.nnx && !ok(a)) ++a;
+    int b = a;
+    while (b < m.nnx && ok(b)) ++b;
+    *lo = a;
+    *hi = b;  // empty when a == b
+    *kx = kxi;
+}
+
 // One pass over `nsteps` FD steps starting at kt_begin, for the launch
 // arguments `args` (a whole batch, or one shot of a plain run), as replays of
 // a graph of `graph_chunk` launches.  The state at kt_begin is in buffer
@@ -460,6 +499,61 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
         *launches += 2;
         b.cur ^= 1;
     }
+    return S2D_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of `planes` per-cell fields of one grid, `fstride` elements
+// apart from `base` (ghost origin): dims (row z + S2D_GZ, column x + S2D_GX,
+// plane), boxes of 128 rows x kTmaCols columns.  The row extent stops at the
+// grid's last row: boxes reaching past it read zeros without touching memory.
+int encode_fields(Ctx *c, CUtensorMap *out, const float *base, int planes, const Model &m, size_t fstride) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return fail(c, S2D_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)(m.nnz + S2D_GZ), (cuuint64_t)m.nxa, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)m.ld * sizeof(float), (cuuint64_t)fstride * sizeof(float)};
+    const cuuint32_t box[3] = {S2D_STRIP_ROWS, kTmaCols, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
+                           es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, S2D_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return S2D_OK;
+}
+
+// Tensor maps of a batch for the TMA step kernel, in device-table order: the
+// 8 state planes of every shot, then the 3 material planes of every shot's
+// model.
+int build_tmaps(Ctx *c, Batch &b) {
+    const int n = (int)b.table.size();
+    static_assert(sizeof(CUtensorMap) == kTmaMapBytes, "tensor map size");
+    std::vector<CUtensorMap> maps(2 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        const int s = b.table[i];
+        const Model &m = *c->models[b.shots[s].model_id];
+        int e = encode_fields(c, &maps[i], b.shot_dev[s].st[0][0], 8, m, (size_t)b.shot_dev[s].fstride);
+        if (!e) e = encode_fields(c, &maps[n + i], m.kappa(), 3, m, m.field_elems);
+        if (e) return e;
+    }
+    CK(b.tmaps_d.alloc(sizeof(CUtensorMap) * maps.size()));
+    CK(cudaMemcpy(b.tmaps_d.p, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
     return S2D_OK;
 }
 
@@ -560,7 +654,8 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         d.nrec = h.nrec;
         d.nseis = (size_t)h.nrec * rs.real_nt;
         fast_rows(m, wave.fd_dt, &d.zfast_lo, &d.zfast_hi, &d.kz_in);
-        if (!c->opt_fast_rows) d.zfast_lo = d.zfast_hi = 0;
+        fast_cols(m, wave.fd_dt, &d.xfast_lo, &d.xfast_hi, &d.kx_in);
+        if (!c->opt_fast_rows) d.zfast_lo = d.zfast_hi = d.xfast_lo = d.xfast_hi = 0;
         // source amplitude per step: fd_dt * w[kt] * kappa[src] / (dx*dz)
         // (cpumodelling.cpp:136-140), kappa = vp^2 rho in double at the source
         const int mx = std::min(std::max(h.src_x - m.nb, 0), m.nx - 1);
@@ -583,6 +678,12 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             if (rx[g] < 0 || rx[g] >= m.nnx || rz[g] < 0 || rz[g] >= m.nnz)
                 return fail(c, S2D_ERR_GEOM, "shot %d receiver %d: (%g, %g) m is outside the grid", s, g,
                             shots[s].rec[g].x, shots[s].rec[g].z);
+        }
+        d.rec_zlo = m.nnz;
+        d.rec_zhi = -1;
+        for (int g = 0; g < h.nrec; ++g) {
+            d.rec_zlo = std::min(d.rec_zlo, rz[g]);
+            d.rec_zhi = std::max(d.rec_zhi, rz[g]);
         }
         std::vector<int> ptr(m.nnx + 1, 0), ez(h.nrec), eid(h.nrec);
         for (int g = 0; g < h.nrec; ++g) ptr[rx[g] + 1]++;
@@ -626,6 +727,7 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
         by_model[shots[s].model_id].push_back(s);
     }
     if (b.plain) {
+        for (int s = 0; s < nshots; ++s) b.table.push_back(s);
         for (int s = 0; s < nshots; ++s) {
             const Model &m = *c->models[shots[s].model_id];
             GroupDev g{};
@@ -651,9 +753,16 @@ int setup_batch(Ctx *c, const s2d_shot *shots, int nshots, const s2d_wave &wave,
             b.groups.push_back(g);
             b.group_nnx.push_back(m.nnx);
             b.group_nnz.push_back(m.nnz);
-            for (int s : ss) reordered.push_back(b.shot_dev[s]);
+            for (int s : ss) {
+                reordered.push_back(b.shot_dev[s]);
+                b.table.push_back(s);
+            }
         }
         CK(cudaMemcpy(b.shots_d.p, reordered.data(), sizeof(ShotDev) * nshots, cudaMemcpyHostToDevice));
+    }
+    {
+        int e = build_tmaps(c, b);
+        if (e) return e;
     }
     // segment lengths for the configuration the run starts with
     {
@@ -688,6 +797,7 @@ int check_device_error(Ctx *c) {
 constexpr int kTuneCandidates[][3] = {
     {kVariantBulk128, 128, 3}, {kVariantBulk128, 128, 2}, {kVariantBulk128, 64, 3}, {kVariantBulk128, 64, 4},
     {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
+    {kVariantTma, kTmaThreads, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
@@ -708,8 +818,14 @@ constexpr int kTuneStepsO8 = tune_steps(kTuneCandidatesO8, kNumTuneCandidatesO8)
 // Sum of the task counts of a batched launch sequence.
 int batch_tasks(const Batch &b) {
     int t = 0;
-    for (auto &g : b.groups) t += g.nshots * g.nstrips * g.nsegs;
+    for (auto &g : b.groups)
+        t += (b.layout_tma ? tma_blocks(g.nshots, g.nstrips) : g.nshots * g.nstrips) * g.nsegs;
     return t;
+}
+// Tasks of shot s's own group in a plain run.
+int plain_tasks(const Batch &b, int s) {
+    const GroupDev &g = b.groups[s];
+    return (b.layout_tma ? tma_blocks(1, g.nstrips) : g.nstrips) * g.nsegs;
 }
 
 // Autotuner: advance the batch by kTuneSteps real FD steps from kt_begin,
@@ -820,7 +936,7 @@ int s2d_set_option(void *ctx, const char *key, long value) {
             return S2D_OK;
         }
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
-            value != kVariantTs2)
+            value != kVariantTs2 && value != kVariantTma)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;
@@ -1033,6 +1149,8 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     a.shots = b.shots_d.as<ShotDev>();
     a.dt_factor = rs.dt_factor;
     a.fd_nt = rs.fd_nt;
+    a.tmaps = b.tmaps_d.p;
+    a.tmap_mat0 = b.nshots;
     int kt_run = kt_begin;  // first step left after tuning
     int tuned_now = 0;
     // Batched runs of a shape with no tuned configuration yet tune on their
@@ -1052,7 +1170,7 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         for (int s = 0; s < nshots; ++s) {
             a.groups = b.groups_d.as<GroupDev>() + s;
             a.ngroups = 1;
-            a.total_tasks = b.groups[s].nstrips * b.groups[s].nsegs;
+            a.total_tasks = plain_tasks(b, s);
             b.cur = cur0;
             int e = run_loop(c, b, lc, a, kt_begin, nsteps, use_graph, &launches, &graph_used);
             if (e) return e;
@@ -1233,9 +1351,19 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     CK(cudaEventRecord(c->ev0, c->stream));
     int launches = 0;
 
-    // per-shot adjoint state, accumulators and source-adjoint trace
+    // per-shot adjoint state and source-adjoint trace; one accumulator pair
+    // dJ/dkappa, dJ/db shared by every shot (they share the model): the
+    // adjoint kernels add into it atomically
     std::vector<ShotDev> adj = b.shot_dev;
     std::vector<float *> gk(nshots), gb(nshots), sadj(nshots);
+    float *acc_pair = nullptr;
+    {
+        void *p;
+        int e = grad_alloc(c, g, 2 * fb, &p);
+        if (e) return e;
+        CK(cudaMemsetAsync(p, 0, 2 * fb, c->stream));
+        acc_pair = static_cast<float *>(p);
+    }
     for (int s = 0; s < nshots; ++s) {
         // adjoint state: 8 fields in one allocation, as the forward state
         void *p;
@@ -1246,14 +1374,8 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
             for (int par = 0; par < 2; ++par)
                 for (int f = 0; f < 4; ++f) adj[s].st[par][f] = static_cast<float *>(p) + (size_t)(par * 4 + f) * F;
         }
-        // accumulators dJ/dkappa, dJ/db, one allocation
-        {
-            int e = grad_alloc(c, g, 2 * fb, &p);
-            if (e) return e;
-            CK(cudaMemsetAsync(p, 0, 2 * fb, c->stream));
-            adj[s].grad[0] = static_cast<float *>(p);
-            adj[s].grad[1] = static_cast<float *>(p) + F;
-        }
+        adj[s].grad[0] = acc_pair;
+        adj[s].grad[1] = acc_pair + F;
         gk[s] = adj[s].grad[0];
         gb[s] = adj[s].grad[1];
         // 8th-order adjoint: two scratch fields for its velocity gathers (ghosts stay 0)
@@ -1308,6 +1430,9 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         void *p;
         int e = grad_alloc(c, g, (size_t)C * 4 * fb, &p);
         if (e) return e;
+        // ghost rows and the second product slot of merged cells are never
+        // written; the adjoint reads them (times zero): they must hold zeros
+        CK(cudaMemsetAsync(p, 0, (size_t)C * 4 * fb, c->stream));
         prod[s] = static_cast<float *>(p);
         ckpt[s] = nullptr;
         if (nseg > 1) {
@@ -1342,6 +1467,8 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     }
     StepArgs fa{};
     fa.shots = b.shots_d.as<ShotDev>();
+    fa.tmaps = b.tmaps_d.p;
+    fa.tmap_mat0 = b.nshots;
     fa.groups = b.groups_d.as<GroupDev>();
     fa.ngroups = (int)b.groups.size();
     fa.total_tasks = batch_tasks(b);
@@ -1496,7 +1623,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     float *out_vp = dev_grad ? grad_vp : static_cast<float *>(p_out);
     float *out_rho = dev_grad ? grad_rho : static_cast<float *>(p_out) + (size_t)m.nx * m.nz;
     {
-        int e = launch_gradient_finalize(dptrs, dptrs + nshots, nshots,
+        int e = launch_gradient_finalize(dptrs, dptrs + nshots, nshots, 1,
                                          static_cast<int *>(p_cells), static_cast<double *>(p_vals),
                                          m.vp.as<float>(), m.rho.as<float>(), m.nx, m.nz, m.nb, m.ld,
                                          m.free_surface ? m.nb + 1 : 0,

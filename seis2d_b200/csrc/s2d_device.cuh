@@ -64,10 +64,13 @@ static __device__ __forceinline__ float comp(const float4 &v, int i) {
 template <bool FAST>
 struct Lane {
     int z0;          // first row of the lane
-    bool owner;      // writes its rows (lanes 1..30)
+    int zl;          // row the lane's loads start at: z0, or -S2D_GZ for a ghost lane
+    bool owner;      // writes its rows (lanes 1..30 whose rows are in the grid)
     int sdz;         // source row - z0
+    int src_x;       // source column
     float amp;       // source term of this step
     float kz;        // interior kz (FAST)
+    float kx;        // interior kx (x-interior columns)
     int nnz;
     const float4 *zc;  // zcoef + z0 + GZ (not FAST)
 };
@@ -75,10 +78,19 @@ struct Lane {
 template <bool FAST>
 static __device__ __forceinline__ void lane_setup(Lane<FAST> &ln, const ShotDev &S, int c, int lane, int kt) {
     ln.z0 = c + S2D_ZPT * lane;
-    ln.owner = lane >= 1 && lane <= 30;
+    // A ghost lane (all 4 rows above or below the grid: the first lane of the
+    // first strip, the lanes of the last strip past nnz) holds only ghost
+    // cells, which are zero and stay zero.  It loads the column's first ghost
+    // row instead (zeros: one 16-byte piece shared by all such lanes of a warp
+    // instead of DRAM traffic of its own) and writes nothing.
+    const bool ghost = ln.z0 < 0 || ln.z0 >= S.nnz;
+    ln.zl = ghost ? -S2D_GZ : ln.z0;
+    ln.owner = lane >= 1 && lane <= 30 && !ghost;
     ln.sdz = S.src_z - ln.z0;
+    ln.src_x = S.src_x;
     ln.amp = __ldg(S.amp + kt);
     ln.kz = S.kz_in;
+    ln.kx = S.kx_in;
     ln.nnz = S.nnz;
     ln.zc = S.zcoef + (ln.z0 + S2D_GZ);
 }

@@ -19,6 +19,12 @@
 #define S2D_STRIP_OUT 120   // rows a one-step warp writes; strip k writes [120k, 120k+120), reads from 120k-4
 #define S2D_TS_OUT 112      // rows a two-step warp writes; strip k writes [112k, 112k+112), reads from 112k-8
 
+#if defined(__CUDACC__)
+#define S2D_HD __host__ __device__
+#else
+#define S2D_HD
+#endif
+
 namespace s2d {
 
 constexpr float kA0 = 1.125f;              // cpu_modelling_kernels.cpp:9
@@ -58,7 +64,7 @@ struct ShotDev {
     int fstride;                   // elements between consecutive fields (8 * fstride < 2^31)
     // gradient runs only
     float *prod;                   // [steps][4][field]: D-x vx, D-z vz, D+x p, D+z p of each step
-    float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout, grad[1] = grad[0] + fstride)
+    float *grad[2];                // accumulators dJ/dkappa, dJ/db (padded layout), one pair shared by the shots of a call
     float *srcadj;                 // [fd_nt] adjoint pressure at the source after each step
     float *scr;                    // 8th-order adjoint: Kx kappa mPX, Kz kappa mPZ (2 fields, ghosts 0)
     // element counts of the buffers above (device self-checks, S2D_DEVICE_CHECKS)
@@ -70,6 +76,12 @@ struct ShotDev {
     // damp1b = 1, kz*damp1a1 = kz*damp1b1 = kz_in, operator pair (a0, a1).
     int zfast_lo, zfast_hi;
     float kz_in;
+    // Columns [xfast_lo, xfast_hi) have the interior column constants:
+    // damp2a = damp2b = 1, kx*damp2a1 = kx*damp2b1 = kx_in and both operator
+    // pairs (a0, a1) (columns [2, nnx-3]).
+    int xfast_lo, xfast_hi;
+    float kx_in;
+    int rec_zlo, rec_zhi;          // rows of the shot's receivers (rec_zlo > rec_zhi: none)
 };
 
 // Shots that share one grid shape; their tasks are interleaved so that the
@@ -104,6 +116,11 @@ struct StepArgs {
     int task_order;       // 0: shot fastest, 1: strip fastest (see task_of)
     int flags;            // S2D_STEP_* bits
     int prod_kt0;         // FD step stored in plane 0 of ShotDev::prod
+    // TMA step kernel: tensor maps (CUtensorMap, 128 B each) of every shot's
+    // 8 state planes in shot-table order, then of the 3 material planes of
+    // every shot's model, in the same order; null for the other kernels
+    const void *tmaps;
+    int tmap_mat0;        // index of table slot 0's material map in tmaps
 };
 
 #define S2D_STEP_NO_RECORD 1  // forward: do not sample receivers; adjoint: do not inject the adjoint source
@@ -123,7 +140,27 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                                      S2D_MODEL_ORDER8; 3 blocks per SM */,
                    kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */,
                    kVariantO8s = 9 /* the same with its windows in shared memory, 4 blocks per SM */,
-                   kVariantO8Products = 10 /* kVariantO8 + S2D_STEP_PRODUCTS, gradient runs */ };
+                   kVariantO8Products = 10 /* kVariantO8 + S2D_STEP_PRODUCTS, gradient runs */,
+                   kVariantTma = 11 /* CTA of kTmaWarps consumer warps fed by a TMA producer warp */ };
+
+// TMA step kernel: a CTA of kTmaWarps consumer warps (one 128-row strip of
+// one shot each) and one producer warp that brings kTmaCols columns of the 7
+// input slots of every consumer warp into a kTmaStages-deep shared-memory ring
+// as 2-D tensor boxes of 128 rows x kTmaCols columns.
+constexpr int kTmaWarps = 8;
+constexpr int kTmaCols = 2;
+constexpr int kTmaStages = 4;
+constexpr int kTmaSlots = 7;  // vx at L; px, pz, kappa, vz at L-1; bx, bz at L-3
+constexpr int kTmaBoxBytes = S2D_STRIP_ROWS * kTmaCols * 4;
+constexpr int kTmaStageBytes = kTmaSlots * kTmaWarps * kTmaBoxBytes;
+constexpr int kTmaThreads = (kTmaWarps + 1) * 32;
+// ring, barriers and the slack that aligns the ring to 1 KB
+constexpr size_t kTmaSmemBytes = (size_t)kTmaStages * kTmaStageBytes + 2 * kTmaStages * 8 + 1024;
+constexpr int kTmaMapBytes = 128;  // sizeof(CUtensorMap)
+
+// Tasks of a TMA launch: per group, blocks of kTmaWarps (shot, strip) pairs
+// times x-segments.
+S2D_HD inline int tma_blocks(int nshots, int nstrips) { return (nshots * nstrips + kTmaWarps - 1) / kTmaWarps; }
 
 // FD steps one launch of a variant advances.
 inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
@@ -135,6 +172,7 @@ inline bool ts_layout(int variant) {
 inline bool order8_variant(int variant) {
     return variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8s;
 }
+inline bool tma_variant(int variant) { return variant == kVariantTma; }
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 ||
@@ -169,11 +207,13 @@ int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, in
 // `nshots` shots of one nnx x nnz grid.
 int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int nshots, void *stream);
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm);
-// Sum the shots' accumulators (dJ/dkappa, dJ/db), apply the kappa = vp^2 rho,
-// b = 1/rho chain rule and fold the sponge onto the model.  kappa_fixed_rows:
-// padded rows [0, kappa_fixed_rows) whose kappa is held at 0 (free surface),
-// so their dJ/dkappa does not reach vp or rho.
-int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, const int *src_cells,
+// Add each shot's source term to its accumulator gk[s] (the entries may all
+// be the one shared pair), sum the nacc accumulator pairs gk[0..nacc),
+// gb[0..nacc) (dJ/dkappa, dJ/db), apply the kappa = vp^2 rho, b = 1/rho chain
+// rule and fold the sponge onto the model.  kappa_fixed_rows: padded rows
+// [0, kappa_fixed_rows) whose kappa is held at 0 (free surface), so their
+// dJ/dkappa does not reach vp or rho.
+int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, int nacc, const int *src_cells,
                              const double *src_vals, const float *vp, const float *rho, int nx, int nz, int nb,
                              int ld, int kappa_fixed_rows, float *tmp2, float *gvp_pad, float *grho_pad, float *grad_vp, float *grad_rho,
                              void *stream);

@@ -79,13 +79,14 @@ __device__ __forceinline__ void p_cell(bool merged, float dax, float kx, float d
 // xc = (Dax, Kx, Dbx, Lx) of column P; colm: Dax == 1 (FAST tasks then have
 // every cell merged and pz is not read).  Returns new p; new px, pz in pxn,
 // pzn; the step's products in dxv, dzv.
-template <bool FAST>
+// XF: column P lies in the shot's x-interior (operator pair (a0, a1)).
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &xc,
                                            bool colm, const float4 &q0, const float4 &q1, const float4 &q2,
                                            const float4 &q3, const float4 &px, const float4 &pz, const float4 &kk,
                                            const float4 &vz, float4 &pxn, float4 &pzn, float4 &dxv, float4 &dzv) {
-    float cx0, cx1;
-    dm_coef(P, S.nnx, cx0, cx1);
+    float cx0 = kA0, cx1 = kA1;
+    if (!XF) dm_coef(P, S.nnx, cx0, cx1);
     const float up_z = __shfl_up_sync(kFull, vz.z, 1);
     const float up_w = __shfl_up_sync(kFull, vz.w, 1);
     const float dn_x = __shfl_down_sync(kFull, vz.x, 1);
@@ -112,7 +113,7 @@ __device__ __forceinline__ float4 p_update(const Lane<FAST> &ln, const ShotDev &
            dzv.z);
     p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, dxv.w,
            dzv.w);
-    if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
+    if (P == ln.src_x && ln.sdz >= 0 && ln.sdz < 4) {
         if (ln.sdz == 0) pxn.x += ln.amp;
         else if (ln.sdz == 1) pxn.y += ln.amp;
         else if (ln.sdz == 2) pxn.z += ln.amp;
@@ -135,14 +136,16 @@ __device__ __forceinline__ void record(const Lane<FAST> &ln, const ShotDev &S, i
 // Velocities at column V from new p at V-1..V+2 (p0..p3), old vx, vz at V and
 // bx, bz at V (cpu_modelling_kernels.cpp:260-316 and 353-368); D+x p and D+z p
 // in dxp, dzp.
-template <bool FAST>
+// XF: column V lies in the shot's x-interior: x-dampings 1, Lx = kx_in,
+// operator pair (a0, a1), no coefficient load.
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ void v_update(const Lane<FAST> &ln, const ShotDev &S, int V, const float4 &p0,
                                          const float4 &p1, const float4 &p2, const float4 &p3, const float4 &vx,
                                          const float4 &vz, const float4 &bx, const float4 &bz, float4 &vxn,
                                          float4 &vzn, float4 &dxp, float4 &dzp) {
-    const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
-    float ux0, ux1;
-    dp_coef(V, S.nnx, ux0, ux1);
+    const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (V + S2D_GX));
+    float ux0 = kA0, ux1 = kA1;
+    if (!XF) dp_coef(V, S.nnx, ux0, ux1);
     const float ex0 = dif(ux0, p2.x - p1.x, ux1, p3.x - p0.x);
     const float ex1 = dif(ux0, p2.y - p1.y, ux1, p3.y - p0.y);
     const float ex2 = dif(ux0, p2.z - p1.z, ux1, p3.z - p0.z);
@@ -189,7 +192,7 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     Lane<FAST> ln;
     lane_setup(ln, S, c, lane, kt);
     const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
-    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t off = (size_t)(ln.zl + S2D_GZ) + (size_t)S2D_GX * ld;
     const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
     float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
     // every field from one base and a 32-bit stride (fewer live registers
@@ -714,7 +717,7 @@ __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev 
            dzv.z);
     p_cell(colm && (FAST || r3.x == 1.0f), xc.x, xc.y, r3.x, r3.y, px.w, pz.w, kk.w, dx3, dz3, pxn.w, pzn.w, dxv.w,
            dzv.w);
-    if (P == S.src_x && ln.sdz >= 0 && ln.sdz < 4) {
+    if (P == ln.src_x && ln.sdz >= 0 && ln.sdz < 4) {
         if (ln.sdz == 0) pxn.x += ln.amp;
         else if (ln.sdz == 1) pxn.y += ln.amp;
         else if (ln.sdz == 2) pxn.z += ln.amp;
@@ -1034,6 +1037,301 @@ __global__ void prepare_staggered(const float *__restrict__ bue, int nnx, int nn
 
 __global__ void set_args_kernel(StepArgs v, StepArgs *dst) { *dst = v; }
 
+// ---------------------------------------------------------------- TMA variant
+//
+// A CTA is kTmaWarps consumer warps and one producer warp.  A task is one
+// x-segment of kTmaWarps consecutive (shot, strip) pairs of a model group
+// (consecutive strips of one shot, wrapping into the next shot), so the
+// consumer warps of a CTA stream adjacent 128-row strips of the same columns.
+// The producer brings the columns in as 2-D tensor boxes (128 rows x kTmaCols
+// columns, cp.async.bulk.tensor from this GPU's own memory, no multicast)
+// into a kTmaStages-deep ring in shared memory, one full barrier (transaction
+// bytes) and one empty barrier (one arrival per consumer warp) per stage, so
+// that up to kTmaStages * kTmaStageBytes of loads are in flight per SM while
+// the consumer warps compute from shared memory.  Stage k of a task holds, for
+// the consumer iterations L = xa-3+2k and L+1 (the loop of ldg_task), vx at L,
+// px, pz, kappa, vz at L-1 and bx, bz at L-3; boxes a task does not need are
+// not loaded, nor pz where every cell of both columns carries p alone.  The
+// tensor maps end at row nnz of the grid: the rows of the last strip past the
+// grid arrive as zeros (the ghost rows hold zeros) without DRAM traffic.  The
+// update arithmetic is ldg_task's (p_update, v_update, record): the same bits.
+//
+// Every wait is bounded (StepArgs::spin_limit polls).  A consumer that gives
+// up records S2D_DEV_ERR_WAIT and leaves; the producer, when its own wait for
+// a free stage gives up, stops issuing, records the error and waits (bounded)
+// for its copies in flight before it leaves, so no copy lands in released
+// shared memory.
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int z, int x, int plane, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(z), "r"(x), "r"(plane), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// The (shot, strip) pair consumer warp w of task t works on.
+struct TmaPair {
+    int group, shot, strip, xa, seg_len;
+    bool live;  // false when the task's block has fewer pairs than warps
+};
+__device__ __forceinline__ TmaPair tma_pair(const StepArgs &a, int t, int w) {
+    int g = 0;
+    while (g + 1 < a.ngroups && __ldg(&a.groups[g + 1].task_begin) <= t) ++g;
+    const GroupDev &G = a.groups[g];
+    const int nblk = tma_blocks(G.nshots, G.nstrips);
+    const int tl = t - G.task_begin;
+    const int p = (tl % nblk) * kTmaWarps + w;
+    TmaPair r;
+    r.group = g;
+    r.live = p < G.nshots * G.nstrips;
+    r.shot = G.shot0 + (r.live ? p / G.nstrips : 0);
+    r.strip = r.live ? p % G.nstrips : 0;
+    r.seg_len = G.seg_len;
+    r.xa = (tl / nblk) * G.seg_len;
+    return r;
+}
+// Consumer iterations of a task (L = xa-3 .. xb+2) in stages of kTmaCols.
+__device__ __forceinline__ int tma_stages(int xa, int xb) { return (xb - xa + 6 + kTmaCols - 1) / kTmaCols; }
+
+// Producer warp: lane w < kTmaWarps issues the boxes of consumer warp w.
+__device__ void tma_produce(const StepArgs &a, int par, unsigned char *ring, uint64_t *full, uint64_t *empty,
+                            int lane) {
+    const char *maps = static_cast<const char *>(a.tmaps);
+    const int drain_limit = a.spin_limit < kDrainLimit / 64 ? a.spin_limit * 64 : kDrainLimit;
+    unsigned ph_of[kTmaStages];
+    bool pending[kTmaStages];
+#pragma unroll
+    for (int i = 0; i < kTmaStages; ++i) {
+        ph_of[i] = 0;
+        pending[i] = false;
+    }
+    int s = 0, it = 0;
+    unsigned ph = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < a.total_tasks && ok; t += gridDim.x) {
+        const TmaPair pr = tma_pair(a, t, lane < kTmaWarps ? lane : 0);
+        const bool mine = lane < kTmaWarps && pr.live;
+        const ShotDev &S = a.shots[pr.shot];
+        const int xa = pr.xa, xb = min(S.nnx, xa + pr.seg_len);
+        const int nst = tma_stages(xa, xb);
+        const int c = pr.strip * S2D_STRIP_OUT - 4;
+        const int z = c + S2D_GZ;
+        const bool fast = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        const void *smap = maps + (size_t)pr.shot * kTmaMapBytes;
+        const void *mmap = maps + (size_t)(a.tmap_mat0 + pr.shot) * kTmaMapBytes;
+        for (int k = 0; k < nst; ++k, ++it) {
+            const int L0 = xa - 3 + kTmaCols * k;
+            const bool pbox = L0 >= xa - 1 && L0 <= xb + 2;
+            const bool bbox = L0 >= xa + 2 && L0 <= xb + 2;
+            bool pz = false;
+            if (mine && pbox) {
+                pz = !fast;
+#pragma unroll
+                for (int j = 0; j < kTmaCols; ++j) pz = pz || __ldg(S.xcoef + (L0 - 1 + j + S2D_GX)).x != 1.0f;
+            }
+            unsigned bytes =
+                mine ? (unsigned)kTmaBoxBytes * (1u + (pbox ? 3u + (pz ? 1u : 0u) : 0u) + (bbox ? 2u : 0u)) : 0u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(kFull, bytes, o);
+            // a free stage: its previous contents consumed by every consumer warp
+            bool got = false;
+            if (lane == 0) {
+                for (int i = 0; i < a.spin_limit && !got; ++i) got = mbar_try_wait(&empty[s], ph ^ 1u);
+                if (got) mbar_expect_tx(&full[s], bytes);
+            }
+            got = __shfl_sync(kFull, got, 0);
+            if (!got) {
+                ok = false;
+                break;
+            }
+            __syncwarp();
+            if (mine && it != a.fault_iter) {
+                unsigned char *st = ring + (size_t)s * kTmaStageBytes + (size_t)lane * kTmaBoxBytes;
+                const int pa = par * 4;
+                tma_load_3d(st, smap, z, L0 + S2D_GX, pa + 2, &full[s]);  // vx
+                if (pbox) {
+                    const int xp = L0 - 1 + S2D_GX;
+                    tma_load_3d(st + 1 * kTmaWarps * kTmaBoxBytes, smap, z, xp, pa + 0, &full[s]);  // px
+                    if (pz) tma_load_3d(st + 2 * kTmaWarps * kTmaBoxBytes, smap, z, xp, pa + 1, &full[s]);
+                    tma_load_3d(st + 3 * kTmaWarps * kTmaBoxBytes, mmap, z, xp, 0, &full[s]);       // kappa
+                    tma_load_3d(st + 4 * kTmaWarps * kTmaBoxBytes, smap, z, xp, pa + 3, &full[s]);  // vz
+                }
+                if (bbox) {
+                    const int xv = L0 - 3 + S2D_GX;
+                    tma_load_3d(st + 5 * kTmaWarps * kTmaBoxBytes, mmap, z, xv, 1, &full[s]);  // bx
+                    tma_load_3d(st + 6 * kTmaWarps * kTmaBoxBytes, mmap, z, xv, 2, &full[s]);  // bz
+                }
+            }
+            ph_of[s] = ph;
+            pending[s] = true;
+            if (++s == kTmaStages) {
+                s = 0;
+                ph ^= 1u;
+            }
+        }
+    }
+    if (lane != 0) return;
+    if (!ok) atomicOr(a.err, S2D_DEV_ERR_WAIT);
+    // copies still in flight must land before the CTA's shared memory is released
+#pragma unroll
+    for (int i = 0; i < kTmaStages; ++i) {
+        if (!pending[i]) continue;
+        bool done = false;
+        for (int n = 0; n < drain_limit && !done; ++n) done = mbar_try_wait(&full[i], ph_of[i]);
+        if (!done) atomicOr(a.err, S2D_DEV_ERR_DRAIN);
+    }
+}
+
+// One task of a consumer warp; returns false when a wait gave up.  XF: every
+// column the task updates or differentiates lies in the shot's x-interior.
+template <bool PROD, bool FAST, bool XF>
+__device__ __forceinline__ bool tma_task(const StepArgs &a, const ShotDev &S, const TmaPair &pr, int kt, int par,
+                                         bool rec_step, int slot, int warp, int lane, const unsigned char *ring,
+                                         uint64_t *full, uint64_t *empty, int &s, unsigned &ph) {
+    const int xa = pr.xa, xb = min(S.nnx, xa + pr.seg_len);
+    const int nst = tma_stages(xa, xb);
+    const size_t ld = (size_t)S.ld;
+    const int c = pr.strip * S2D_STRIP_OUT - 4;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    // receivers only where the strip's rows hold some
+    const bool rec = pr.live && rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD) &&
+                     c + S2D_STRIP_ROWS > S.rec_zlo && c <= S.rec_zhi;
+    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+    float *__restrict__ pr_ = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off + (par ^ 1) * 4 * fs;
+    float *__restrict__ pxo = sb;
+    float *__restrict__ pzo = sb + fs;
+    float *__restrict__ vxo = sb + 2 * fs;
+    float *__restrict__ vzo = sb + 3 * fs;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 vq0 = zero, vq1 = zero, vq2 = zero, vq3 = zero;
+    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+    float4 zq0 = zero, zq1 = zero, zq2 = zero;
+    for (int k = 0; k < nst; ++k) {
+        if (!wait_stage(&full[s], ph, a.spin_limit)) {
+            if (lane == 0) atomicOr(a.err, S2D_DEV_ERR_WAIT);
+            return false;
+        }
+        if (pr.live) {
+            const float4 *stg =
+                reinterpret_cast<const float4 *>(ring + (size_t)s * kTmaStageBytes + (size_t)warp * kTmaBoxBytes) +
+                lane;
+            // slot f, column j of the stage: float4 index (f * kTmaWarps * kTmaCols + j) * 32 past stg
+#pragma unroll
+            for (int j = 0; j < kTmaCols; ++j) {
+                const int L = xa - 3 + kTmaCols * k + j;
+                if (L > xb + 2) break;
+                auto slotv = [&](int f) { return stg[(f * kTmaWarps * kTmaCols + j) * 32]; };
+                vq0 = vq1; vq1 = vq2; vq2 = vq3;
+                vq3 = slotv(0);
+                if (L < xa) continue;
+                const int P = L - 1;
+                const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+                const float4 vz = slotv(4);
+                const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+                const bool colm = XF || xc.x == 1.0f;
+                const bool pz_live = !(FAST && colm);
+                float4 pxn, pzn, dxv, dzv;
+                const float4 pn = p_update<FAST, XF>(ln, S, P, xc, colm, vq0, vq1, vq2, vq3, slotv(1),
+                                                     pz_live ? slotv(2) : zero, slotv(3), vz, pxn, pzn, dxv, dzv);
+                const bool in_seg = P >= xa && P < xb;
+                if (in_seg && ln.owner) {
+                    st4(pxo + colP, pxn);
+                    if (pz_live) st4(pzo + colP, pzn);
+                    if (PROD) {
+                        st4(pr_ + colP, dxv);
+                        if (pz_live) st4(pr_ + F + colP, dzv);
+                    }
+                }
+                if (rec && in_seg) record(ln, S, P, pn, slot);
+                pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+                zq0 = zq1; zq1 = zq2; zq2 = vz;
+                if (L >= xa + 3) {
+                    const int V = L - 3;
+                    const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+                    float4 vxn, vzn, dxp, dzp;
+                    v_update<FAST, XF>(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, slotv(5), slotv(6), vxn, vzn, dxp,
+                                       dzp);
+                    if (ln.owner) {
+                        st4(vxo + colV, vxn);
+                        st4(vzo + colV, vzn);
+                        if (PROD) {
+                            st4(pr_ + 2 * F + colV, dxp);
+                            st4(pr_ + 3 * F + colV, dzp);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (++s == kTmaStages) {
+            s = 0;
+            ph ^= 1u;
+        }
+    }
+    return true;
+}
+
+template <bool PROD>
+__global__ void __launch_bounds__(kTmaThreads, 1) step_kernel_tma(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ unsigned char smem_raw[];
+    // the boxes need 128-byte aligned destinations: align the ring to 1 KB
+    unsigned char *ring = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + (size_t)kTmaStages * kTmaStageBytes);
+    uint64_t *empty = full + kTmaStages;
+    const StepArgs a = *A;
+    const int kt = a.kt_base + kt_off;
+    if (kt >= a.fd_nt) return;
+    // an earlier launch of this sequence gave up: its wavefields are not valid
+    if (*reinterpret_cast<volatile int *>(a.err) != 0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kTmaStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kTmaWarps);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const int par = a.par0 ^ (kt_off & 1);
+    if (warp == kTmaWarps) {
+        tma_produce(a, par, ring, full, empty, lane);
+        return;
+    }
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    int s = 0;
+    unsigned ph = 0;
+    for (int t = blockIdx.x; t < a.total_tasks; t += gridDim.x) {
+        const TmaPair pr = tma_pair(a, t, warp);
+        const ShotDev &S = a.shots[pr.shot];
+        const int c = pr.strip * S2D_STRIP_OUT - 4;
+        const int xa = pr.xa, xb = min(S.nnx, xa + pr.seg_len);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        // columns xa-1 .. xb+1 take part (p there, v on xa .. xb-1)
+        const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;
+        bool ok;
+        if (zf && xf)
+            ok = tma_task<PROD, true, true>(a, S, pr, kt, par, rec_step, slot, warp, lane, ring, full, empty, s, ph);
+        else if (zf)
+            ok = tma_task<PROD, true, false>(a, S, pr, kt, par, rec_step, slot, warp, lane, ring, full, empty, s, ph);
+        else if (xf)
+            ok = tma_task<PROD, false, true>(a, S, pr, kt, par, rec_step, slot, warp, lane, ring, full, empty, s, ph);
+        else
+            ok = tma_task<PROD, false, false>(a, S, pr, kt, par, rec_step, slot, warp, lane, ring, full, empty, s, ph);
+        if (!ok) return;
+    }
+}
+
 }  // namespace
 
 int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int block, size_t smem,
@@ -1058,6 +1356,8 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_o8<3, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantO8s)
         step_kernel_o8s<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantTma)
+        step_kernel_tma<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
         step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
@@ -1089,6 +1389,7 @@ const void *kernel_of(int variant) {
     if (variant == kVariantO8r) return (const void *)step_kernel_o8<2, false>;
     if (variant == kVariantO8Products) return (const void *)step_kernel_o8<3, true>;
     if (variant == kVariantO8s) return (const void *)step_kernel_o8s;
+    if (variant == kVariantTma) return (const void *)step_kernel_tma<false>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace

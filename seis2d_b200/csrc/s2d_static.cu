@@ -269,6 +269,9 @@ extern "C" int s2d_forward_static(int device, int nx, int nz, float dx, float dz
     sd.nrec = nrec;
     sd.nseis = seis_n;
     sd.zfast_lo = sd.zfast_hi = 0;  // every strip takes the general row path
+    sd.xfast_lo = sd.xfast_hi = 0;  // and every column the general column path
+    sd.rec_zlo = 0;                 // receivers anywhere
+    sd.rec_zhi = nnz - 1;
     int bps = 1;
     if (rc == S2D_OK && (step_kernel_occupancy(kVariantLdg, 128, 0, &bps) || bps < 1)) bps = 1;
     int sms = 1;

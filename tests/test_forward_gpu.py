@@ -40,7 +40,7 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
-VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5}
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5, "tma": 11}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -206,16 +206,18 @@ def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
     np.testing.assert_array_equal(got, base)
 
 
-def test_bounded_wait_reports_timeout_and_context_survives(ctx):
-    """A pipeline barrier whose bytes never arrive: every wait is bounded, the
-    kernel records the error and returns, the call reports S2D_ERR_TIMEOUT and
-    the next call on the same context is correct."""
+@pytest.mark.parametrize("variant", [0, 11])
+def test_bounded_wait_reports_timeout_and_context_survives(ctx, variant):
+    """A pipeline barrier whose bytes never arrive (the per-warp bulk-copy
+    pipeline, and the TMA kernel's producer/consumer ring): every wait is
+    bounded, the kernel records the error and returns, the call reports
+    S2D_ERR_TIMEOUT and the next call on the same context is correct."""
     from seis2d_b200 import Shot
     from seis2d_b200._lib import Seis2dError, S2D_ERR_TIMEOUT
     z, c, vp, rho = _golden("edges_explicit_nb32")
     m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
     shot = [Shot(m, tuple(z["src"]), z["rec"])]
-    ctx.set_option("variant", 0)
+    ctx.set_option("variant", variant)
     ctx.set_option("spin_limit", 256)
     ctx.set_option("inject_wait_fault", 1)
     try:
@@ -330,7 +332,7 @@ def test_autotuner_tunes_once_per_shape_and_keeps_the_bits():
         c.close()
     assert s1.autotuned == 1 and s2.autotuned == 0 and s3.autotuned == 0
     assert (s1.variant, s1.block, s1.stages) == (s2.variant, s2.block, s2.stages)
-    assert s1.variant in (0, 1, 2, 4, 5) and s3.variant == 1
+    assert s1.variant in (0, 1, 2, 4, 5, 11) and s3.variant == 1
     for a, b, f in zip(first, again, fixed):
         np.testing.assert_array_equal(a, f)
         np.testing.assert_array_equal(b, f)
