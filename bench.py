@@ -206,11 +206,12 @@ def traffic_per_launch(workload, nshots):
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    t = json.load(open(p)).get(workload)
-    if not t:
+    try:
+        t = json.load(open(p)).get(workload)
+        b = float(t["per_shot_bytes"]) * nshots + float(t.get("per_model_bytes", 0.0))
+        return {"bytes": b, "source": t["source"]}
+    except (TypeError, KeyError, ValueError):
         return None
-    b = float(t["per_shot_bytes"]) * nshots + float(t.get("per_model_bytes", 0.0))
-    return {"bytes": b, "source": t["source"]}
 
 
 def dram_minimal_bytes(w, nshots):

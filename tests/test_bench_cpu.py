@@ -29,3 +29,31 @@ def test_reference_arm_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "Gcell/s"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "reference"
+
+
+def test_reference_arm_loads_no_product_code():
+    """The reference arm times the reference binary alone: after one sample
+    no module of the modelling package (which would map libseis2d.so) is
+    imported."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "seis_ref_nb40")):
+        pytest.skip("reference binary for the 1000 x 1000 workload (nb 40) not built")
+    code = ("import sys, bench; info, err = bench.ref_cpu_rate(bench.WORKLOADS['c1'], (2, 6), threads=2); "
+            "assert info and info['value'] > 0, err; "
+            "print(sorted(m for m in sys.modules if m.startswith('seis2d_b200')))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "[]"
+
+
+def test_roofline_traffic_and_minimal_bytes():
+    """The measured-traffic record scales to a launch's shot count, and the
+    DRAM-minimal bytes per cell-update lie between the merged-cell 24 B and
+    the split-cell 32 B plus the shots' share of the materials."""
+    sys.path.insert(0, ROOT)
+    import bench
+    t2, t64 = bench.traffic_per_launch("c2", 2), bench.traffic_per_launch("c2", 64)
+    assert t2 and t64 and t64["bytes"] > 30 * t2["bytes"] / 2 * 0.9
+    assert abs(t2["bytes"] - 1.613e9) < 0.01e9
+    for n in (1, 64):
+        b = bench.dram_minimal_bytes(bench.WORKLOADS["c2"], n)
+        assert 24.0 + 12.0 / n <= b <= 32.0 + 12.0 / n

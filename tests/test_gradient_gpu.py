@@ -195,7 +195,8 @@ def test_torch_autograd(ctx):
 
 def test_gradient_allreduce_through_nccl(ctx):
     """seis2d_b200.sharding.gradient_allreduce on a one-rank NCCL group: the
-    device images and the misfit go through the all-reduce unchanged."""
+    device images and the misfit go through the all-reduce unchanged (to the
+    rounding of the shots' atomic accumulation)."""
     import datetime
     import socket
     import torch
@@ -218,6 +219,8 @@ def test_gradient_allreduce_through_nccl(ctx):
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
-    np.testing.assert_allclose(gv.cpu().numpy(), ref.grad_vp, rtol=0, atol=0)
-    np.testing.assert_allclose(gr.cpu().numpy(), ref.grad_rho, rtol=0, atol=0)
+    # the shots' imaging terms meet in one accumulator pair through atomics
+    # whose order is not fixed: two runs agree to rounding
+    assert O.rel_l2(gv.cpu().numpy(), ref.grad_vp) <= 1e-6
+    assert O.rel_l2(gr.cpu().numpy(), ref.grad_rho) <= 1e-6
     assert abs(mis - ref.misfit) <= 1e-9 * ref.misfit
