@@ -144,8 +144,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 80 steps
- *                 spends 40 of them on 9 candidate configurations, one untimed
+ *                 shape (models, grids, shot counts) with at least 88 steps
+ *                 spends 44 of them on 10 candidate configurations, one untimed
  *                 and three timed launches each, in rounds (the results do not
  *                 change: every candidate computes the same bits), times them
  *                 with events and keeps the fastest per FD step for that shape
@@ -158,7 +158,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 crosses HBM once per two steps; odd step counts end with one
  *                 one-step launch), 11 a CTA of 8 warps on adjacent strips fed
  *                 by a producer warp's 2-D TMA tensor loads through a 4-stage
- *                 shared-memory ring (one block of 288 threads per SM);
+ *                 shared-memory ring (one block of 288 threads per SM),
+ *                 12 the plain-load loop fed by per-lane asynchronous copies
+ *                 (cp.async) into a 3-column per-warp ring;
  *                 s2d_gradient always runs one step per launch.
  *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in

@@ -268,7 +268,8 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
     const bool ldg = plain_loads(lc.variant);
     const bool ts = ts_layout(lc.variant);
     const bool tma = tma_variant(lc.variant);
-    if (ldg || ts) {
+    const bool asy = async_variant(lc.variant);
+    if (ldg || ts || asy) {
         lc.block = 128;
         lc.stages = 0;
     }
@@ -278,6 +279,7 @@ int launch_config(Ctx *c, long max_tasks, LaunchCfg *out, int variant, int block
     }
     lc.smem = ldg ? 0
               : tma ? kTmaSmemBytes
+              : asy ? (size_t)(lc.block / 32) * kAsyncWarpBytes
               : ts ? (size_t)(lc.block / 32) * (lc.variant == kVariantO8s ? kO8sWarpBytes : kTsWarpBytes)
                    : bulk_smem_bytes(lc.block / 32, lc.stages);
     int e = step_kernel_prepare(lc.variant, lc.smem);
@@ -797,7 +799,7 @@ int check_device_error(Ctx *c) {
 constexpr int kTuneCandidates[][3] = {
     {kVariantBulk128, 128, 3}, {kVariantBulk128, 128, 2}, {kVariantBulk128, 64, 3}, {kVariantBulk128, 64, 4},
     {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
-    {kVariantTma, kTmaThreads, 0},
+    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
@@ -936,7 +938,7 @@ int s2d_set_option(void *ctx, const char *key, long value) {
             return S2D_OK;
         }
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
-            value != kVariantTs2 && value != kVariantTma)
+            value != kVariantTs2 && value != kVariantTma && value != kVariantAsync)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;

@@ -141,7 +141,15 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantO8r = 8 /* the same at 2 blocks per SM (no register cap below 224) */,
                    kVariantO8s = 9 /* the same with its windows in shared memory, 4 blocks per SM */,
                    kVariantO8Products = 10 /* kVariantO8 + S2D_STEP_PRODUCTS, gradient runs */,
-                   kVariantTma = 11 /* CTA of kTmaWarps consumer warps fed by a TMA producer warp */ };
+                   kVariantTma = 11 /* CTA of kTmaWarps consumer warps fed by a TMA producer warp */,
+                   kVariantAsync = 12 /* plain-load loop fed by per-lane cp.async into a per-warp ring */,
+                   kVariantAsyncProducts = 13 /* kVariantAsync + S2D_STEP_PRODUCTS, gradient runs */ };
+
+// Per-warp ring of the async variant: kAsyncStages iterations of kAsyncSlots
+// 128-row column slices (vx; px, pz, kappa, vz; bx, bz).
+constexpr int kAsyncStages = 3;
+constexpr int kAsyncSlots = 7;
+constexpr int kAsyncWarpBytes = kAsyncStages * kAsyncSlots * S2D_STRIP_ROWS * 4;
 
 // TMA step kernel: a CTA of kTmaWarps consumer warps (one 128-row strip of
 // one shot each) and one producer warp that brings kTmaCols columns of the 7
@@ -173,6 +181,7 @@ inline bool order8_variant(int variant) {
     return variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8s;
 }
 inline bool tma_variant(int variant) { return variant == kVariantTma; }
+inline bool async_variant(int variant) { return variant == kVariantAsync || variant == kVariantAsyncProducts; }
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 ||

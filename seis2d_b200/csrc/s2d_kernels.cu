@@ -1037,6 +1037,164 @@ __global__ void prepare_staggered(const float *__restrict__ bue, int nnx, int nn
 
 __global__ void set_args_kernel(StepArgs v, StepArgs *dst) { *dst = v; }
 
+// ------------------------------------------------------------ async variant
+//
+// The plain-load kernel's loop with every column load replaced by a per-lane
+// asynchronous copy (cp.async, 16 bytes: the lane's four rows) into a
+// per-warp ring of kAsyncStages iterations in shared memory, issued
+// kAsyncStages - 1 iterations ahead: the loads of the next columns are in
+// flight while the warp computes, without holding registers.  Each lane reads
+// back only the 16 bytes it copied itself (z-neighbours still come by
+// shuffles), so the ring needs no barrier: cp.async.wait_group on the lane's
+// own copy groups is the whole synchronisation.  A ghost lane's copies are
+// zero-fills that read nothing.  The arithmetic is ldg_task's: the same bits.
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool read) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(read ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <bool PROD, bool FAST, bool XF>
+__device__ __forceinline__ void async_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                           int kt, int par, bool rec_step, int slot, int lane, float4 *ring) {
+    const int xb = min(S.nnx, xa + seg_len);
+    const size_t ld = (size_t)S.ld;
+    const int c = strip * S2D_STRIP_OUT - 4;
+    Lane<FAST> ln;
+    lane_setup(ln, S, c, lane, kt);
+    const bool ghost = ln.z0 < 0 || ln.z0 >= S.nnz;
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD) &&
+                     c + S2D_STRIP_ROWS > S.rec_zlo && c <= S.rec_zhi;
+    const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
+    float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    const float *pxi = sb + ib;
+    const float *pzi = sb + ib + fs;
+    const float *vxi = sb + ib + 2 * fs;
+    const float *vzi = sb + ib + 3 * fs;
+    float *__restrict__ pxo = sb + ob;
+    float *__restrict__ pzo = sb + ob + fs;
+    float *__restrict__ vxo = sb + ob + 2 * fs;
+    float *__restrict__ vzo = sb + ob + 3 * fs;
+    const float *kap = S.kappa + off;
+    const float *bxp = kap + fs;
+    const float *bzp = kap + 2 * fs;
+    // iteration i = 0 .. n_it-1 is column L = xa-3+i; its slots: vx at L,
+    // px, pz, kappa, vz at L-1, bx, bz at L-3 (ring float4 index
+    // ((i % kAsyncStages) * kAsyncSlots + f) * 32 + lane)
+    const int n_it = xb - xa + 6;
+    auto issue = [&](int i) {
+        float4 *st = ring + (i % kAsyncStages) * kAsyncSlots * 32 + lane;
+        const int L = xa - 3 + i;
+        const ptrdiff_t cL = (ptrdiff_t)L * (ptrdiff_t)ld, cP = cL - (ptrdiff_t)ld, cV = cL - 3 * (ptrdiff_t)ld;
+        const bool live = !ghost;
+        cp_async16(st, vxi + cL, live);
+        if (L >= xa) {
+            const bool pz_live = !(FAST && (XF || __ldg(S.xcoef + (L - 1 + S2D_GX)).x == 1.0f));
+            cp_async16(st + 1 * 32, pxi + cP, live);
+            if (pz_live) cp_async16(st + 2 * 32, pzi + cP, live);
+            cp_async16(st + 3 * 32, kap + cP, live);
+            cp_async16(st + 4 * 32, vzi + cP, live);
+        }
+        if (L >= xa + 3) {
+            cp_async16(st + 5 * 32, bxp + cV, live);
+            cp_async16(st + 6 * 32, bzp + cV, live);
+        }
+    };
+#pragma unroll
+    for (int i = 0; i < kAsyncStages - 1; ++i) {
+        if (i < n_it) issue(i);
+        cp_async_commit();
+    }
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 vq0 = zero, vq1 = zero, vq2 = zero, vq3 = zero;
+    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
+    float4 zq0 = zero, zq1 = zero, zq2 = zero;
+    for (int i = 0; i < n_it; ++i) {
+        if (i + kAsyncStages - 1 < n_it) issue(i + kAsyncStages - 1);
+        cp_async_commit();
+        cp_async_wait<kAsyncStages - 1>();  // iteration i's copies have landed
+        const float4 *st = ring + (i % kAsyncStages) * kAsyncSlots * 32 + lane;
+        const int L = xa - 3 + i;
+        vq0 = vq1; vq1 = vq2; vq2 = vq3;
+        vq3 = st[0];
+        if (L < xa) continue;
+        const int P = L - 1;
+        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
+        const float4 vz = st[4 * 32];
+        const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = XF || xc.x == 1.0f;
+        const bool pz_live = !(FAST && colm);
+        float4 pxn, pzn, dxv, dzv;
+        const float4 pn = p_update<FAST, XF>(ln, S, P, xc, colm, vq0, vq1, vq2, vq3, st[1 * 32],
+                                             pz_live ? st[2 * 32] : zero, st[3 * 32], vz, pxn, pzn, dxv, dzv);
+        const bool in_seg = P >= xa && P < xb;
+        if (in_seg && ln.owner) {
+            st4(pxo + colP, pxn);
+            if (pz_live) st4(pzo + colP, pzn);
+            if (PROD) {
+                st4(pr + colP, dxv);
+                if (pz_live) st4(pr + F + colP, dzv);
+            }
+        }
+        if (rec && in_seg) record(ln, S, P, pn, slot);
+        pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
+        zq0 = zq1; zq1 = zq2; zq2 = vz;
+        if (L >= xa + 3) {
+            const int V = L - 3;
+            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
+            float4 vxn, vzn, dxp, dzp;
+            v_update<FAST, XF>(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, st[5 * 32], st[6 * 32], vxn, vzn, dxp, dzp);
+            if (ln.owner) {
+                st4(vxo + colV, vxn);
+                st4(vzo + colV, vzn);
+                if (PROD) {
+                    st4(pr + 2 * F + colV, dxp);
+                    st4(pr + 3 * F + colV, dzp);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+template <bool PROD, int MINB>
+__global__ void __launch_bounds__(128, MINB) step_kernel_async(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kAsyncWarpBytes);
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base + kt_off;
+    if (kt >= a.fd_nt) return;
+    const int par = a.par0 ^ (kt_off & 1);
+    const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
+        const int c = strip * S2D_STRIP_OUT - 4;
+        const int xb = min(S.nnx, xa + seg_len);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;
+        if (zf && xf) async_task<PROD, true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else if (zf) async_task<PROD, true, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else if (xf) async_task<PROD, false, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else async_task<PROD, false, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+    }
+}
+
 // ---------------------------------------------------------------- TMA variant
 //
 // A CTA is kTmaWarps consumer warps and one producer warp.  A task is one
@@ -1358,6 +1516,10 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_o8s<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantTma)
         step_kernel_tma<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantAsync)
+        step_kernel_async<false, 4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantAsyncProducts)
+        step_kernel_async<true, 3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
         step_kernel_ldg<false, 1><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
@@ -1390,6 +1552,8 @@ const void *kernel_of(int variant) {
     if (variant == kVariantO8Products) return (const void *)step_kernel_o8<3, true>;
     if (variant == kVariantO8s) return (const void *)step_kernel_o8s;
     if (variant == kVariantTma) return (const void *)step_kernel_tma<false>;
+    if (variant == kVariantAsync) return (const void *)step_kernel_async<false, 4>;
+    if (variant == kVariantAsyncProducts) return (const void *)step_kernel_async<true, 3>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
 }  // namespace
