@@ -160,7 +160,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 by a producer warp's 2-D TMA tensor loads through a 4-stage
  *                 shared-memory ring (one block of 288 threads per SM),
  *                 12 the plain-load loop fed by per-lane asynchronous copies
- *                 (cp.async) into a 3-column per-warp ring;
+ *                 (cp.async) into a 3-column per-warp ring, 14 variant 4 with
+ *                 its column loop unrolled by 4;
  *                 s2d_gradient always runs one step per launch.
  *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in

@@ -143,7 +143,8 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantO8Products = 10 /* kVariantO8 + S2D_STEP_PRODUCTS, gradient runs */,
                    kVariantTma = 11 /* CTA of kTmaWarps consumer warps fed by a TMA producer warp */,
                    kVariantAsync = 12 /* plain-load loop fed by per-lane cp.async into a per-warp ring */,
-                   kVariantAsyncProducts = 13 /* kVariantAsync + S2D_STEP_PRODUCTS, gradient runs */ };
+                   kVariantAsyncProducts = 13 /* kVariantAsync + S2D_STEP_PRODUCTS, gradient runs */,
+                   kVariantLdgU4 = 14 /* kVariantLdg128 with its column loop unrolled by 4 */ };
 
 // Per-warp ring of the async variant: kAsyncStages iterations of kAsyncSlots
 // 128-row column slices (vx; px, pz, kappa, vz; bx, bz).
@@ -184,7 +185,7 @@ inline bool tma_variant(int variant) { return variant == kVariantTma; }
 inline bool async_variant(int variant) { return variant == kVariantAsync || variant == kVariantAsyncProducts; }
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
-    return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 ||
+    return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 || variant == kVariantLdgU4 ||
            variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8Products;
 }
 

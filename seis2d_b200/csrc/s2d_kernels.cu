@@ -181,87 +181,147 @@ __device__ __forceinline__ void v_update(const Lane<FAST> &ln, const ShotDev &S,
 
 // ---------------------------------------------------------------- LDG variant
 
-// One (shot, strip, segment) task of the plain-load kernel.  PROD: also write
-// the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).
+// Per-task constants of the plain-load loop.
 template <bool PROD, bool FAST>
-__device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
-                                         int kt, int par, bool rec_step, int slot, int lane) {
-    const int xb = min(S.nnx, xa + seg_len);
-    const size_t ld = (size_t)S.ld;
-    const int c = strip * S2D_STRIP_OUT - 4;
+struct LdgTask {
     Lane<FAST> ln;
-    lane_setup(ln, S, c, lane, kt);
-    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
-    const size_t off = (size_t)(ln.zl + S2D_GZ) + (size_t)S2D_GX * ld;
-    const size_t F = (size_t)(S.nnx + 2 * S2D_GX) * ld;
-    float *__restrict__ pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off : nullptr;
-    // every field from one base and a 32-bit stride (fewer live registers
-    // than eleven 64-bit pointers)
-    const int fs = S.fstride;
-    float *const sb = S.st[0][0] + off;
-    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
-    const float *__restrict__ pxi = sb + ib;
-    const float *__restrict__ pzi = sb + ib + fs;
-    const float *__restrict__ vxi = sb + ib + 2 * fs;
-    const float *__restrict__ vzi = sb + ib + 3 * fs;
-    float *__restrict__ pxo = sb + ob;
-    float *__restrict__ pzo = sb + ob + fs;
-    float *__restrict__ vxo = sb + ob + 2 * fs;
-    float *__restrict__ vzo = sb + ob + 3 * fs;
-    const float *__restrict__ kap = S.kappa + off;
-    const float *__restrict__ bxp = kap + fs;
-    const float *__restrict__ bzp = kap + 2 * fs;
+    int xa, xb, slot;
+    bool rec;
+    ptrdiff_t ld;
+    size_t F;
+    const float *__restrict__ pxi;
+    const float *__restrict__ pzi;
+    const float *__restrict__ vxi;
+    const float *__restrict__ vzi;
+    float *__restrict__ pxo;
+    float *__restrict__ pzo;
+    float *__restrict__ vxo;
+    float *__restrict__ vzo;
+    const float *__restrict__ kap;
+    const float *__restrict__ bxp;
+    const float *__restrict__ bzp;
+    float *__restrict__ pr;
+};
+
+// One column L of the loop: vx(L) into vo (the window vx(L-3 .. L) is then
+// v1, v2, v3, vo), new p at P = L-1 into po (p(P-3 .. P) is p1, p2, p3, po),
+// vz(P) into zo (z2 holds vz(P-2)), velocities at V = L-3.  The caller
+// passes the window registers in rotated order, so the windows slide without
+// moves.  XF: every column of the task lies in the shot's x-interior.
+template <bool PROD, bool FAST, bool XF>
+__device__ __forceinline__ void ldg_column(const LdgTask<PROD, FAST> &k, const ShotDev &S, int L, float4 &vo,
+                                           const float4 &v1, const float4 &v2, const float4 &v3, float4 &po,
+                                           const float4 &p1, const float4 &p2, const float4 &p3, float4 &zo,
+                                           const float4 &z2) {
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 vq0 = zero, vq1, vq2, vq3;
-    float4 pq0 = zero, pq1 = zero, pq2 = zero, pq3 = zero;
-    float4 zq0 = zero, zq1 = zero, zq2 = zero;
-    vq1 = ld4(vxi + (ptrdiff_t)(xa - 3) * (ptrdiff_t)ld);
-    vq2 = ld4(vxi + (ptrdiff_t)(xa - 2) * (ptrdiff_t)ld);
-    vq3 = ld4(vxi + (ptrdiff_t)(xa - 1) * (ptrdiff_t)ld);
-    for (int L = xa; L <= xb + 2; ++L) {
-        const int P = L - 1;
-        const ptrdiff_t colP = (ptrdiff_t)P * (ptrdiff_t)ld;
-        vq0 = vq1; vq1 = vq2; vq2 = vq3;
-        vq3 = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
-        const float4 vz = ld4(vzi + colP);
-        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
-        const bool colm = xc.x == 1.0f;
-        const bool pz_live = !(FAST && colm);  // some cell of the column keeps pz
-        float4 pxn, pzn, dxv, dzv;
-        const float4 pn = p_update(ln, S, P, xc, colm, vq0, vq1, vq2, vq3, ld4(pxi + colP),
-                                   pz_live ? ld4(pzi + colP) : zero, ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
-        const bool in_seg = P >= xa && P < xb;
-        if (in_seg && ln.owner) {
-            st4(pxo + colP, pxn);
-            if (pz_live) st4(pzo + colP, pzn);
-            if (PROD) {
-                st4(pr + colP, dxv);
-                if (pz_live) st4(pr + F + colP, dzv);
-            }
+    const int P = L - 1;
+    const ptrdiff_t colP = (ptrdiff_t)P * k.ld;
+    vo = ld4(k.vxi + (ptrdiff_t)L * k.ld);
+    const float4 vz = ld4(k.vzi + colP);
+    const float4 xc = XF ? make_float4(1.0f, k.ln.kx, 1.0f, k.ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+    const bool colm = XF || xc.x == 1.0f;
+    const bool pz_live = !(FAST && colm);  // some cell of the column keeps pz
+    float4 pxn, pzn, dxv, dzv;
+    const float4 pn = p_update<FAST, XF>(k.ln, S, P, xc, colm, v1, v2, v3, vo, ld4(k.pxi + colP),
+                                         pz_live ? ld4(k.pzi + colP) : zero, ld4(k.kap + colP), vz, pxn, pzn, dxv,
+                                         dzv);
+    const bool in_seg = P >= k.xa && P < k.xb;
+    if (in_seg && k.ln.owner) {
+        st4(k.pxo + colP, pxn);
+        if (pz_live) st4(k.pzo + colP, pzn);
+        if (PROD) {
+            st4(k.pr + colP, dxv);
+            if (pz_live) st4(k.pr + k.F + colP, dzv);
         }
-        if (rec && in_seg) record(ln, S, P, pn, slot);
-        pq0 = pq1; pq1 = pq2; pq2 = pq3; pq3 = pn;
-        zq0 = zq1; zq1 = zq2; zq2 = vz;
-        if (L >= xa + 3) {
-            const int V = L - 3;
-            const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
-            float4 vxn, vzn, dxp, dzp;
-            v_update(ln, S, V, pq0, pq1, pq2, pq3, vq0, zq0, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
-            if (ln.owner) {
-                st4(vxo + colV, vxn);
-                st4(vzo + colV, vzn);
-                if (PROD) {
-                    st4(pr + 2 * F + colV, dxp);
-                    st4(pr + 3 * F + colV, dzp);
-                }
+    }
+    if (k.rec && in_seg) record(k.ln, S, P, pn, k.slot);
+    po = pn;
+    zo = vz;
+    if (L >= k.xa + 3) {
+        const int V = L - 3;
+        const ptrdiff_t colV = (ptrdiff_t)V * k.ld;
+        float4 vxn, vzn, dxp, dzp;
+        v_update<FAST, XF>(k.ln, S, V, p1, p2, p3, po, v1, z2, ld4(k.bxp + colV), ld4(k.bzp + colV), vxn, vzn,
+                           dxp, dzp);
+        if (k.ln.owner) {
+            st4(k.vxo + colV, vxn);
+            st4(k.vzo + colV, vzn);
+            if (PROD) {
+                st4(k.pr + 2 * k.F + colV, dxp);
+                st4(k.pr + 3 * k.F + colV, dzp);
             }
         }
     }
 }
 
+// One (shot, strip, segment) task of the plain-load kernel.  PROD: also write
+// the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).  U4: the
+// column loop unrolled by 4 with the windows rotating through the register
+// names (no moves); otherwise one column per iteration.
+template <bool PROD, bool FAST, bool XF, bool U4>
+__device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                         int kt, int par, bool rec_step, int slot, int lane) {
+    LdgTask<PROD, FAST> k;
+    k.xa = xa;
+    k.xb = min(S.nnx, xa + seg_len);
+    k.ld = (ptrdiff_t)S.ld;
+    const int c = strip * S2D_STRIP_OUT - 4;
+    lane_setup(k.ln, S, c, lane, kt);
+    // receivers only where the strip's rows hold some
+    k.rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD) && c + S2D_STRIP_ROWS > S.rec_zlo &&
+            c <= S.rec_zhi;
+    k.slot = slot;
+    const size_t off = (size_t)(k.ln.zl + S2D_GZ) + (size_t)S2D_GX * (size_t)S.ld;
+    k.F = (size_t)(S.nnx + 2 * S2D_GX) * (size_t)S.ld;
+    k.pr = PROD ? S.prod + (size_t)(kt - a.prod_kt0) * 4 * k.F + off : nullptr;
+    // every field from one base and a 32-bit stride (fewer live registers
+    // than eleven 64-bit pointers)
+    const int fs = S.fstride;
+    float *const sb = S.st[0][0] + off;
+    const int ib = par * 4 * fs, ob = (par ^ 1) * 4 * fs;
+    k.pxi = sb + ib;
+    k.pzi = sb + ib + fs;
+    k.vxi = sb + ib + 2 * fs;
+    k.vzi = sb + ib + 3 * fs;
+    k.pxo = sb + ob;
+    k.pzo = sb + ob + fs;
+    k.vxo = sb + ob + 2 * fs;
+    k.vzo = sb + ob + 3 * fs;
+    k.kap = S.kappa + off;
+    k.bxp = k.kap + fs;
+    k.bzp = k.kap + 2 * fs;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    // windows: vx(L-4 .. L-1), p(P-4 .. P-1), vz(P-4 .. P-1) before column L
+    float4 vA = zero, vB, vC, vD;
+    float4 pA = zero, pB = zero, pC = zero, pD = zero;
+    float4 zA = zero, zB = zero, zC = zero, zD = zero;
+    vB = ld4(k.vxi + (ptrdiff_t)(xa - 3) * k.ld);
+    vC = ld4(k.vxi + (ptrdiff_t)(xa - 2) * k.ld);
+    vD = ld4(k.vxi + (ptrdiff_t)(xa - 1) * k.ld);
+    const int Lend = k.xb + 2;
+    int L = xa;
+    if (U4) {
+        for (; L + 3 <= Lend; L += 4) {
+            ldg_column<PROD, FAST, XF>(k, S, L, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
+            ldg_column<PROD, FAST, XF>(k, S, L + 1, vB, vC, vD, vA, pB, pC, pD, pA, zB, zD);
+            ldg_column<PROD, FAST, XF>(k, S, L + 2, vC, vD, vA, vB, pC, pD, pA, pB, zC, zA);
+            ldg_column<PROD, FAST, XF>(k, S, L + 3, vD, vA, vB, vC, pD, pA, pB, pC, zD, zB);
+        }
+    }
+    for (; L <= Lend; ++L) {
+        ldg_column<PROD, FAST, XF>(k, S, L, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
+        float4 t = vA;
+        vA = vB; vB = vC; vC = vD; vD = t;
+        t = pA;
+        pA = pB; pB = pC; pC = pD; pD = t;
+        t = zA;
+        zA = zB; zB = zC; zC = zD; zD = t;
+    }
+}
+
 // MINB = 4 caps registers at 128 (4 blocks of 4 warps per SM, some spill);
 // MINB = 3 keeps the product-writing instance at 3 blocks per SM.
-template <bool PROD, int MINB>
+template <bool PROD, int MINB, bool U4 = false>
 __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
@@ -277,10 +337,14 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__r
         const ShotDev &S = task_of(a, t, strip, xa, seg_len);
         if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
         const int c = strip * S2D_STRIP_OUT - 4;
-        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1))
-            ldg_task<PROD, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
-        else
-            ldg_task<PROD, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        const int xb = min(S.nnx, xa + seg_len);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        // columns xa-1 .. xb+1 take part (p there, v on xa .. xb-1)
+        const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;
+        if (zf && xf) ldg_task<PROD, true, true, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (zf) ldg_task<PROD, true, false, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (xf) ldg_task<PROD, false, true, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else ldg_task<PROD, false, false, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
     }
 }
 
@@ -1518,6 +1582,8 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_tma<false><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantAsync)
         step_kernel_async<false, 4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgU4)
+        step_kernel_ldg<false, 4, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantAsyncProducts)
         step_kernel_async<true, 3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
@@ -1553,6 +1619,7 @@ const void *kernel_of(int variant) {
     if (variant == kVariantO8s) return (const void *)step_kernel_o8s;
     if (variant == kVariantTma) return (const void *)step_kernel_tma<false>;
     if (variant == kVariantAsync) return (const void *)step_kernel_async<false, 4>;
+    if (variant == kVariantLdgU4) return (const void *)step_kernel_ldg<false, 4, true>;
     if (variant == kVariantAsyncProducts) return (const void *)step_kernel_async<true, 3>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
