@@ -938,7 +938,8 @@ int s2d_set_option(void *ctx, const char *key, long value) {
             return S2D_OK;
         }
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
-            value != kVariantTs2 && value != kVariantTma && value != kVariantAsync && value != kVariantLdgU4)
+            value != kVariantTs2 && value != kVariantTma && value != kVariantAsync && value != kVariantLdgU4 &&
+            value != kVariantLdgPf && value != kVariantLdgPf4)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;

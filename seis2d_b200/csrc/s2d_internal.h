@@ -144,7 +144,9 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantTma = 11 /* CTA of kTmaWarps consumer warps fed by a TMA producer warp */,
                    kVariantAsync = 12 /* plain-load loop fed by per-lane cp.async into a per-warp ring */,
                    kVariantAsyncProducts = 13 /* kVariantAsync + S2D_STEP_PRODUCTS, gradient runs */,
-                   kVariantLdgU4 = 14 /* kVariantLdg128 with its column loop unrolled by 4 */ };
+                   kVariantLdgU4 = 14 /* kVariantLdg128 with its column loop unrolled by 4 */,
+                   kVariantLdgPf = 15 /* plain loads, next column prefetched, 3 blocks per SM */,
+                   kVariantLdgPf4 = 16 /* the same compiled for 4 blocks per SM */ };
 
 // Per-warp ring of the async variant: kAsyncStages iterations of kAsyncSlots
 // 128-row column slices (vx; px, pz, kappa, vz; bx, bz).
@@ -186,6 +188,7 @@ inline bool async_variant(int variant) { return variant == kVariantAsync || vari
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 || variant == kVariantLdgU4 ||
+           variant == kVariantLdgPf || variant == kVariantLdgPf4 ||
            variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8Products;
 }
 

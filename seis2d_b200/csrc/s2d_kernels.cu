@@ -203,6 +203,68 @@ struct LdgTask {
     float *__restrict__ pr;
 };
 
+// The loads of one column L: vx(L); px, pz, kappa, vz at L-1; bx, bz at L-3.
+struct ColIn {
+    float4 vx, px, pz, k, vz, bx, bz;
+};
+template <bool PROD, bool FAST, bool XF>
+__device__ __forceinline__ void ldg_load(const LdgTask<PROD, FAST> &k, const ShotDev &S, int L, ColIn &in) {
+    const ptrdiff_t colL = (ptrdiff_t)L * k.ld, colP = colL - k.ld, colV = colL - 3 * k.ld;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    in.vx = ld4(k.vxi + colL);
+    in.px = ld4(k.pxi + colP);
+    const bool pz_live = !(FAST && (XF || __ldg(S.xcoef + (L - 1 + S2D_GX)).x == 1.0f));
+    in.pz = pz_live ? ld4(k.pzi + colP) : zero;
+    in.k = ld4(k.kap + colP);
+    in.vz = ld4(k.vzi + colP);
+    in.bx = ld4(k.bxp + colV);
+    in.bz = ld4(k.bzp + colV);
+}
+
+// One column L of the loop from its loaded inputs (the prefetching form of
+// ldg_column below; same arithmetic).
+template <bool PROD, bool FAST, bool XF>
+__device__ __forceinline__ void ldg_column_in(const LdgTask<PROD, FAST> &k, const ShotDev &S, int L,
+                                              const ColIn &in, float4 &vo, const float4 &v1, const float4 &v2,
+                                              const float4 &v3, float4 &po, const float4 &p1, const float4 &p2,
+                                              const float4 &p3, float4 &zo, const float4 &z2) {
+    const int P = L - 1;
+    const ptrdiff_t colP = (ptrdiff_t)P * k.ld;
+    vo = in.vx;
+    const float4 xc = XF ? make_float4(1.0f, k.ln.kx, 1.0f, k.ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+    const bool colm = XF || xc.x == 1.0f;
+    const bool pz_live = !(FAST && colm);
+    float4 pxn, pzn, dxv, dzv;
+    const float4 pn = p_update<FAST, XF>(k.ln, S, P, xc, colm, v1, v2, v3, vo, in.px, in.pz, in.k, in.vz, pxn, pzn,
+                                         dxv, dzv);
+    const bool in_seg = P >= k.xa && P < k.xb;
+    if (in_seg && k.ln.owner) {
+        st4(k.pxo + colP, pxn);
+        if (pz_live) st4(k.pzo + colP, pzn);
+        if (PROD) {
+            st4(k.pr + colP, dxv);
+            if (pz_live) st4(k.pr + k.F + colP, dzv);
+        }
+    }
+    if (k.rec && in_seg) record(k.ln, S, P, pn, k.slot);
+    po = pn;
+    zo = in.vz;
+    if (L >= k.xa + 3) {
+        const int V = L - 3;
+        const ptrdiff_t colV = (ptrdiff_t)V * k.ld;
+        float4 vxn, vzn, dxp, dzp;
+        v_update<FAST, XF>(k.ln, S, V, p1, p2, p3, po, v1, z2, in.bx, in.bz, vxn, vzn, dxp, dzp);
+        if (k.ln.owner) {
+            st4(k.vxo + colV, vxn);
+            st4(k.vzo + colV, vzn);
+            if (PROD) {
+                st4(k.pr + 2 * k.F + colV, dxp);
+                st4(k.pr + 3 * k.F + colV, dzp);
+            }
+        }
+    }
+}
+
 // One column L of the loop: vx(L) into vo (the window vx(L-3 .. L) is then
 // v1, v2, v3, vo), new p at P = L-1 into po (p(P-3 .. P) is p1, p2, p3, po),
 // vz(P) into zo (z2 holds vz(P-2)), velocities at V = L-3.  The caller
@@ -257,8 +319,10 @@ __device__ __forceinline__ void ldg_column(const LdgTask<PROD, FAST> &k, const S
 // One (shot, strip, segment) task of the plain-load kernel.  PROD: also write
 // the step's four derivatives (gradient runs, S2D_STEP_PRODUCTS).  U4: the
 // column loop unrolled by 4 with the windows rotating through the register
-// names (no moves); otherwise one column per iteration.
-template <bool PROD, bool FAST, bool XF, bool U4>
+// names (no moves); otherwise one column per iteration.  PF: the loads of
+// column L+1 are issued before column L is computed (two columns of loads in
+// flight per warp).
+template <bool PROD, bool FAST, bool XF, bool U4, bool PF = false>
 __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                          int kt, int par, bool rec_step, int slot, int lane) {
     LdgTask<PROD, FAST> k;
@@ -300,6 +364,22 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     vD = ld4(k.vxi + (ptrdiff_t)(xa - 1) * k.ld);
     const int Lend = k.xb + 2;
     int L = xa;
+    if (PF) {
+        ColIn cur, nxt;
+        ldg_load<PROD, FAST, XF>(k, S, L, nxt);
+        for (; L <= Lend; ++L) {
+            cur = nxt;
+            if (L < Lend) ldg_load<PROD, FAST, XF>(k, S, L + 1, nxt);
+            ldg_column_in<PROD, FAST, XF>(k, S, L, cur, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
+            float4 t = vA;
+            vA = vB; vB = vC; vC = vD; vD = t;
+            t = pA;
+            pA = pB; pB = pC; pC = pD; pD = t;
+            t = zA;
+            zA = zB; zB = zC; zC = zD; zD = t;
+        }
+        return;
+    }
     if (U4) {
         for (; L + 3 <= Lend; L += 4) {
             ldg_column<PROD, FAST, XF>(k, S, L, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
@@ -321,7 +401,7 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
 
 // MINB = 4 caps registers at 128 (4 blocks of 4 warps per SM, some spill);
 // MINB = 3 keeps the product-writing instance at 3 blocks per SM.
-template <bool PROD, int MINB, bool U4 = false>
+template <bool PROD, int MINB, bool U4 = false, bool PF = false>
 __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__restrict__ A, int kt_off) {
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
@@ -341,10 +421,10 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__r
         const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
         // columns xa-1 .. xb+1 take part (p there, v on xa .. xb-1)
         const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;
-        if (zf && xf) ldg_task<PROD, true, true, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
-        else if (zf) ldg_task<PROD, true, false, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
-        else if (xf) ldg_task<PROD, false, true, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
-        else ldg_task<PROD, false, false, U4>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        if (zf && xf) ldg_task<PROD, true, true, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (zf) ldg_task<PROD, true, false, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (xf) ldg_task<PROD, false, true, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else ldg_task<PROD, false, false, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
     }
 }
 
@@ -1343,6 +1423,7 @@ __device__ void tma_produce(const StepArgs &a, int par, unsigned char *ring, uin
         const int c = pr.strip * S2D_STRIP_OUT - 4;
         const int z = c + S2D_GZ;
         const bool fast = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;  // every column merged in x
         const void *smap = maps + (size_t)pr.shot * kTmaMapBytes;
         const void *mmap = maps + (size_t)(a.tmap_mat0 + pr.shot) * kTmaMapBytes;
         for (int k = 0; k < nst; ++k, ++it) {
@@ -1352,8 +1433,10 @@ __device__ void tma_produce(const StepArgs &a, int par, unsigned char *ring, uin
             bool pz = false;
             if (mine && pbox) {
                 pz = !fast;
+                if (!pz && !xf) {
 #pragma unroll
-                for (int j = 0; j < kTmaCols; ++j) pz = pz || __ldg(S.xcoef + (L0 - 1 + j + S2D_GX)).x != 1.0f;
+                    for (int j = 0; j < kTmaCols; ++j) pz = pz || __ldg(S.xcoef + (L0 - 1 + j + S2D_GX)).x != 1.0f;
+                }
             }
             unsigned bytes =
                 mine ? (unsigned)kTmaBoxBytes * (1u + (pbox ? 3u + (pz ? 1u : 0u) : 0u) + (bbox ? 2u : 0u)) : 0u;
@@ -1584,6 +1667,10 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_async<false, 4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantLdgU4)
         step_kernel_ldg<false, 4, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgPf)
+        step_kernel_ldg<false, 3, false, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgPf4)
+        step_kernel_ldg<false, 4, false, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantAsyncProducts)
         step_kernel_async<true, 3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
@@ -1620,6 +1707,8 @@ const void *kernel_of(int variant) {
     if (variant == kVariantTma) return (const void *)step_kernel_tma<false>;
     if (variant == kVariantAsync) return (const void *)step_kernel_async<false, 4>;
     if (variant == kVariantLdgU4) return (const void *)step_kernel_ldg<false, 4, true>;
+    if (variant == kVariantLdgPf) return (const void *)step_kernel_ldg<false, 3, false, true>;
+    if (variant == kVariantLdgPf4) return (const void *)step_kernel_ldg<false, 4, false, true>;
     if (variant == kVariantAsyncProducts) return (const void *)step_kernel_async<true, 3>;
     return (const void *)step_kernel_ldg<false, 1>;
 }
