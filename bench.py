@@ -501,6 +501,8 @@ def main():
                     help="gradient: only the FWI gradient leg (--shots shots, --grad-time seconds)")
     ap.add_argument("--grad-time", type=float, default=3.0, help="record length of the gradient leg (s)")
     ap.add_argument("--grad-segment", type=int, default=0, help="checkpoint interval of the gradient leg (0: auto)")
+    ap.add_argument("--products-variant", type=int, default=0,
+                    help="gradient leg: s2d_set_option 'products_variant' (0: library default)")
     ap.add_argument("--fd-order", type=int, default=4, choices=[4, 8],
                     help="FD operator of the main leg: 4 (the reference's) or 8 (Order of FD Operator = 8)")
     args = ap.parse_args()
@@ -511,6 +513,8 @@ def main():
             ctx.set_option("grad_segment", args.grad_segment)
             if args.variant >= 0:
                 ctx.set_option("variant", args.variant)
+            if args.products_variant:
+                ctx.set_option("products_variant", args.products_variant)
             print(json.dumps({"leg": "c5_gradient", **gradient_leg(ctx, args.shots or 32, args.grad_time)}))
         return 0
 

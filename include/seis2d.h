@@ -178,6 +178,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 (same results, a check of the fast path)
  *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
  *                 run needs (default 64)
+ *   "products_variant" s2d_gradient's forward recompute that keeps the step
+ *                 derivatives: 3 plain loads (default), 19 plain loads with the
+ *                 next column prefetched
  *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 (default) or 4
  *                 blocks of 128 threads per SM
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the

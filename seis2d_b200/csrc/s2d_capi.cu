@@ -166,6 +166,7 @@ struct Ctx {
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
     int opt_adj_minb = 3;     // adjoint kernel compiled for 2, 3 or 4 blocks per SM
+    int opt_prod_variant = kVariantLdgProducts;  // s2d_gradient's product-writing forward (4th order)
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     // Launch-argument block read by every step launch, and the graphs of step
@@ -939,7 +940,8 @@ int s2d_set_option(void *ctx, const char *key, long value) {
         }
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
             value != kVariantTs2 && value != kVariantTma && value != kVariantAsync && value != kVariantLdgU4 &&
-            value != kVariantLdgPf && value != kVariantLdgPf4)
+            value != kVariantLdgPf && value != kVariantLdgPf4 && value != kVariantLdgPfU4 &&
+            value != kVariantLdgPfU3)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;
@@ -961,6 +963,10 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "products_variant") {
+        if (value != kVariantLdgProducts && value != kVariantLdgPfProducts)
+            return fail(c, S2D_ERR_ARG, "products_variant must be %d or %d", kVariantLdgProducts, kVariantLdgPfProducts);
+        c->opt_prod_variant = (int)value;
     } else if (k == "adjoint_blocks") {
         if (value < 2 || value > 4) return fail(c, S2D_ERR_ARG, "adjoint_blocks must be 2, 3 or 4");
         c->opt_adj_minb = (int)value;
@@ -1456,7 +1462,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
                        c->stream));
 
     LaunchCfg lc_fwd, lc_prod;
-    const int prod_variant = b.order8 ? kVariantO8Products : kVariantLdgProducts;
+    const int prod_variant = b.order8 ? kVariantO8Products : c->opt_prod_variant;
     {
         int e = base_config(c, b, &lc_fwd);
         // the gradient keeps every step's state (checkpoints at kt parity):
@@ -1504,7 +1510,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         if (adjoint_kernel_occupancy(128, c->opt_adj_minb, &bps) || bps < 1) bps = 1;
         const long resident = (long)c->sm_count * bps;
         int e = layout_groups_for(c, b, resident * 4, {-1, resident, c->opt_seg_len});
-        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, kVariantLdgProducts, 128, 0);
+        if (!e) e = launch_config(c, b.max_tasks, &lc_prod, c->opt_prod_variant, 128, 0);
         if (e) return e;
         agrid = (int)std::max<long>(1, std::min<long>(resident, (b.max_tasks * 32 + 127) / 128));
         fa.total_tasks = batch_tasks(b);

@@ -146,7 +146,10 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantAsyncProducts = 13 /* kVariantAsync + S2D_STEP_PRODUCTS, gradient runs */,
                    kVariantLdgU4 = 14 /* kVariantLdg128 with its column loop unrolled by 4 */,
                    kVariantLdgPf = 15 /* plain loads, next column prefetched, 3 blocks per SM */,
-                   kVariantLdgPf4 = 16 /* the same compiled for 4 blocks per SM */ };
+                   kVariantLdgPf4 = 16 /* the same compiled for 4 blocks per SM */,
+                   kVariantLdgPfU4 = 17 /* prefetch into two buffers in turn, unrolled by 4, 4 blocks per SM */,
+                   kVariantLdgPfU3 = 18 /* the same compiled for 3 blocks per SM */,
+                   kVariantLdgPfProducts = 19 /* kVariantLdgPf + S2D_STEP_PRODUCTS, gradient runs */ };
 
 // Per-warp ring of the async variant: kAsyncStages iterations of kAsyncSlots
 // 128-row column slices (vx; px, pz, kappa, vz; bx, bz).
@@ -188,7 +191,8 @@ inline bool async_variant(int variant) { return variant == kVariantAsync || vari
 // Variants that use no dynamic shared memory.
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 || variant == kVariantLdgU4 ||
-           variant == kVariantLdgPf || variant == kVariantLdgPf4 ||
+           variant == kVariantLdgPf || variant == kVariantLdgPf4 || variant == kVariantLdgPfU4 ||
+           variant == kVariantLdgPfU3 || variant == kVariantLdgPfProducts ||
            variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8Products;
 }
 

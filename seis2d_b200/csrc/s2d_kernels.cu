@@ -364,6 +364,35 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     vD = ld4(k.vxi + (ptrdiff_t)(xa - 1) * k.ld);
     const int Lend = k.xb + 2;
     int L = xa;
+    if (PF && U4) {
+        // two load buffers in turn and the windows rotating through the
+        // register names: no moves in the unrolled body
+        ColIn X, Y;
+        ldg_load<PROD, FAST, XF>(k, S, L, X);
+        for (; L + 3 <= Lend; L += 4) {
+            ldg_load<PROD, FAST, XF>(k, S, L + 1, Y);
+            ldg_column_in<PROD, FAST, XF>(k, S, L, X, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
+            ldg_load<PROD, FAST, XF>(k, S, L + 2, X);
+            ldg_column_in<PROD, FAST, XF>(k, S, L + 1, Y, vB, vC, vD, vA, pB, pC, pD, pA, zB, zD);
+            ldg_load<PROD, FAST, XF>(k, S, L + 3, Y);
+            ldg_column_in<PROD, FAST, XF>(k, S, L + 2, X, vC, vD, vA, vB, pC, pD, pA, pB, zC, zA);
+            if (L + 4 <= Lend) ldg_load<PROD, FAST, XF>(k, S, L + 4, X);
+            ldg_column_in<PROD, FAST, XF>(k, S, L + 3, Y, vD, vA, vB, vC, pD, pA, pB, pC, zD, zB);
+        }
+        // X holds column L's loads
+        for (; L <= Lend; ++L) {
+            const ColIn cur = X;
+            if (L < Lend) ldg_load<PROD, FAST, XF>(k, S, L + 1, X);
+            ldg_column_in<PROD, FAST, XF>(k, S, L, cur, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
+            float4 t = vA;
+            vA = vB; vB = vC; vC = vD; vD = t;
+            t = pA;
+            pA = pB; pB = pC; pC = pD; pD = t;
+            t = zA;
+            zA = zB; zB = zC; zC = zD; zD = t;
+        }
+        return;
+    }
     if (PF) {
         ColIn cur, nxt;
         ldg_load<PROD, FAST, XF>(k, S, L, nxt);
@@ -1671,6 +1700,12 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
         step_kernel_ldg<false, 3, false, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantLdgPf4)
         step_kernel_ldg<false, 4, false, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgPfU4)
+        step_kernel_ldg<false, 4, true, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgPfU3)
+        step_kernel_ldg<false, 3, true, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
+    else if (variant == kVariantLdgPfProducts)
+        step_kernel_ldg<true, 3, false, true><<<grid, block, 0, (cudaStream_t)stream>>>(args_dev, kt_off);
     else if (variant == kVariantAsyncProducts)
         step_kernel_async<true, 3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     else
@@ -1709,6 +1744,9 @@ const void *kernel_of(int variant) {
     if (variant == kVariantLdgU4) return (const void *)step_kernel_ldg<false, 4, true>;
     if (variant == kVariantLdgPf) return (const void *)step_kernel_ldg<false, 3, false, true>;
     if (variant == kVariantLdgPf4) return (const void *)step_kernel_ldg<false, 4, false, true>;
+    if (variant == kVariantLdgPfU4) return (const void *)step_kernel_ldg<false, 4, true, true>;
+    if (variant == kVariantLdgPfU3) return (const void *)step_kernel_ldg<false, 3, true, true>;
+    if (variant == kVariantLdgPfProducts) return (const void *)step_kernel_ldg<true, 3, false, true>;
     if (variant == kVariantAsyncProducts) return (const void *)step_kernel_async<true, 3>;
     return (const void *)step_kernel_ldg<false, 1>;
 }

@@ -40,7 +40,7 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
-VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5, "tma": 11, "async": 12, "ldgu4": 14, "ldgpf": 15, "ldgpf4": 16}
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5, "tma": 11, "async": 12, "ldgu4": 14, "ldgpf": 15, "ldgpf4": 16, "ldgpfu4": 17, "ldgpfu3": 18}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
