@@ -144,25 +144,29 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 88 steps
- *                 spends 44 of them on 10 candidate configurations, one untimed
- *                 and three timed launches each, in rounds (the results do not
- *                 change: every candidate computes the same bits), times them
- *                 with events and keeps the fastest per FD step for that shape
- *                 in the context; runs that do not tune (shorter calls, S2D_PLAIN)
- *                 use variant 4.  0: use "variant", "block" and "stages".
+ *                 shape (models, grids, shot counts) with at least 64 steps
+ *                 spends 32 of them on 7 candidate configurations (variants
+ *                 4, 16, 15, 2, 5, 11, 12), one untimed and three timed launches
+ *                 each, in rounds (the results do not change: every candidate
+ *                 computes the same bits), times them with events and keeps the
+ *                 fastest per FD step for that shape in the context; runs that
+ *                 do not tune (shorter calls, S2D_PLAIN) use variant 16.
+ *                 0: use "variant", "block" and "stages".
  *                 Setting any of those three turns autotuning off.
  *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline
  *                 compiled for 128 registers, 4 plain loads compiled for 128
- *                 registers (default), 5 two FD steps per launch (the state
- *                 crosses HBM once per two steps; odd step counts end with one
- *                 one-step launch), 11 a CTA of 8 warps on adjacent strips fed
- *                 by a producer warp's 2-D TMA tensor loads through a 4-stage
+ *                 registers, 5 two FD steps per launch (the state crosses HBM
+ *                 once per two steps; odd step counts end with one one-step
+ *                 launch), 11 a CTA of 8 warps on adjacent strips fed by a
+ *                 producer warp's 2-D TMA tensor loads through a 4-stage
  *                 shared-memory ring (one block of 288 threads per SM),
  *                 12 the plain-load loop fed by per-lane asynchronous copies
  *                 (cp.async) into a 3-column per-warp ring, 14 variant 4 with
- *                 its column loop unrolled by 4;
- *                 s2d_gradient always runs one step per launch.
+ *                 its column loop unrolled by 4, 15 plain loads with the next
+ *                 column's loads issued before the current column is computed
+ *                 (3 blocks per SM), 16 the same at 4 blocks per SM (default),
+ *                 17 and 18 the prefetch with the loop unrolled by 4 at 4 and
+ *                 3 blocks per SM; s2d_gradient always runs one step per launch.
  *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in
  *                 shared memory at 4 (each setting applies to its own order)
@@ -179,8 +183,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
  *                 run needs (default 64)
  *   "products_variant" s2d_gradient's forward recompute that keeps the step
- *                 derivatives: 3 plain loads (default), 19 plain loads with the
- *                 next column prefetched
+ *                 derivatives: 3 plain loads, 19 plain loads with the next
+ *                 column prefetched (default)
  *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 (default) or 4
  *                 blocks of 128 threads per SM
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the

@@ -141,7 +141,7 @@ struct Pool {
 
 // Launch configuration of the step kernel.
 struct LaunchCfg {
-    int variant = kVariantLdg128;  // the fastest single configuration on the c2 and c5 workloads
+    int variant = kVariantLdgPf4;  // the fastest single configuration on the 64-shot 5000 x 5000 batch
     int block = 128;      // threads per block (whole warps)
     int stages = 3;       // bulk-copy ring depth per warp (bulk-copy variants)
     size_t smem = 0;
@@ -153,7 +153,7 @@ struct Ctx {
     int sm_count = 0;
     // tuning options (s2d_set_option)
     // explicit launch configuration, used when autotuning is off
-    int opt_variant = kVariantLdg128;
+    int opt_variant = kVariantLdgPf4;
     int opt_variant8 = kVariantO8;  // 8th-order batches when autotuning is off
     int opt_block = 128;
     int opt_stages = 3;
@@ -166,7 +166,7 @@ struct Ctx {
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
     int opt_adj_minb = 3;     // adjoint kernel compiled for 2, 3 or 4 blocks per SM
-    int opt_prod_variant = kVariantLdgProducts;  // s2d_gradient's product-writing forward (4th order)
+    int opt_prod_variant = kVariantLdgPfProducts;  // s2d_gradient's product-writing forward (4th order)
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
     // Launch-argument block read by every step launch, and the graphs of step
@@ -798,9 +798,8 @@ int check_device_error(Ctx *c) {
 
 // Candidate launch configurations of the autotuner: (variant, block, stages).
 constexpr int kTuneCandidates[][3] = {
-    {kVariantBulk128, 128, 3}, {kVariantBulk128, 128, 2}, {kVariantBulk128, 64, 3}, {kVariantBulk128, 64, 4},
-    {kVariantLdg128, 128, 0},  {kVariantLdg, 128, 0},     {kVariantBulk, 128, 3},     {kVariantTs2, 128, 0},
-    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
+    {kVariantLdg128, 128, 0}, {kVariantLdgPf4, 128, 0}, {kVariantLdgPf, 128, 0},      {kVariantBulk128, 128, 3},
+    {kVariantTs2, 128, 0},    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
@@ -1468,7 +1467,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         // the gradient keeps every step's state (checkpoints at kt parity):
         // one step per launch
         if (!e && steps_per_launch(lc_fwd.variant) != 1)
-            e = launch_config(c, b.max_tasks, &lc_fwd, kVariantLdg128, 128, 0);
+            e = launch_config(c, b.max_tasks, &lc_fwd, kVariantLdgPf4, 128, 0);
         if (!e) e = layout_groups(c, b, lc_fwd);
         if (!e) e = launch_config(c, b.max_tasks, &lc_fwd, lc_fwd.variant, lc_fwd.block, lc_fwd.stages);
         if (!e) e = launch_config(c, b.max_tasks, &lc_prod, prod_variant, 128, 0);

@@ -224,3 +224,26 @@ def test_gradient_allreduce_through_nccl(ctx):
     assert O.rel_l2(gv.cpu().numpy(), ref.grad_vp) <= 1e-6
     assert O.rel_l2(gr.cpu().numpy(), ref.grad_rho) <= 1e-6
     assert abs(mis - ref.misfit) <= 1e-9 * ref.misfit
+
+
+def test_products_variants_give_the_same_gradient(ctx):
+    """The product-writing recompute with plain loads (3) and with the next
+    column prefetched (19, the default) share the update arithmetic: one
+    shot's gradient is the same bit for bit."""
+    from seis2d_b200 import Shot
+    vp, rho = _model(41)
+    src, rec = _geom(310.0)
+    nt = O.derive(O.Params(NX, NZ, NB, D, D, T, DT, DDT, F))["real_nt"]
+    adj = np.random.default_rng(43).standard_normal((rec.shape[0], nt)).astype(np.float32)
+    m = ctx.model(vp, rho, D, D, NB)
+    try:
+        ctx.set_option("grad_segment", 37)
+        out = {}
+        for pv in (3, 19):
+            ctx.set_option("products_variant", pv)
+            out[pv] = ctx.gradient([Shot(m, src, rec)], _wave(), adj)
+    finally:
+        ctx.set_option("products_variant", 19)
+        ctx.set_option("grad_segment", 0)
+    np.testing.assert_array_equal(out[3].grad_vp, out[19].grad_vp)
+    np.testing.assert_array_equal(out[3].grad_rho, out[19].grad_rho)
