@@ -109,7 +109,9 @@ __device__ __forceinline__ float4 &adj_ring(float4 *ring, int field, int col, in
     return ring[(field * kAdjRing + ((col + 2 * S2D_GX) & (kAdjRing - 1))) * 32 + lane];
 }
 
-template <bool FAST>
+// XF: every column the task touches (xa-3 .. xb+2) lies in the shot's
+// x-interior: literal column coefficients, no coefficient loads.
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                              int kt, int lane, float4 *ring) {
     const int nnx = S.nnx;
@@ -147,12 +149,13 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
 
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 tbp = zero;                                      // tbx at Q-1
+    const float kx = S.kx_in;
 
     for (int L = xa - 3; L <= xb + 2; ++L) {
         {
             const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
             const float4 m = ld4(mvxi + colL), b = ld4(bxp + colL);
-            const float lx = __ldg(S.xcoef + (L + S2D_GX)).w;
+            const float lx = XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
             adj_ring(ring, 0, L, lane) = m;
             adj_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
                                                      (lx * b.w) * m.w);
@@ -163,8 +166,8 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const bool in_seg = Q >= xa && Q < xb;
         const bool upd = in_seg && ln.owner;       // this lane writes column Q
         const bool img = Q >= 0 && Q < xb;         // buoyancy terms at Q (xa-1 feeds column xa)
-        const float4 xq = __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx at Q
-        const bool colm = xq.x == 1.0f;
+        const float4 xq = XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx
+        const bool colm = XF || xq.x == 1.0f;
         const bool pz_live = !(FAST && colm);  // some cell of the column keeps mpz
         const float4 mpx = ld4(mpxi + colQ), mvz = ld4(mvzi + colQ);
         const float4 mpz = pz_live ? ld4(mpzi + colQ) : zero;
@@ -188,7 +191,8 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         float4 q = hzt(ln, h, __shfl_up_sync(kFull, h.z, 1), __shfl_up_sync(kFull, h.w, 1),
                        __shfl_down_sync(kFull, h.x, 1));
         {
-            const float p0a = xc0p(Q - 1, nnx), p0b = xc0p(Q, nnx), p1a = xc1p(Q - 2, nnx), p1b = xc1p(Q + 1, nnx);
+            const float p0a = XF ? kA0 : xc0p(Q - 1, nnx), p0b = XF ? kA0 : xc0p(Q, nnx);
+            const float p1a = XF ? kA1 : xc1p(Q - 2, nnx), p1b = XF ? kA1 : xc1p(Q + 1, nnx);
             const float4 mg0 = adj_ring(ring, 1, L - 3, lane), mg1 = adj_ring(ring, 1, L - 2, lane);
             const float4 mg2 = adj_ring(ring, 1, L - 1, lane), mg3 = adj_ring(ring, 1, L, lane);
             q.x += p0a * mg1.x - p0b * mg2.x + p1a * mg0.x - p1b * mg3.x;
@@ -263,8 +267,9 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         // ---- x-velocity adjoint at W = L - 3 ----
         const int W = L - 3;
         const ptrdiff_t colW = (ptrdiff_t)W * (ptrdiff_t)ld;
-        const float dbx = __ldg(S.xcoef + (W + S2D_GX)).z;
-        const float m0a = xc0m(W, nnx), m0b = xc0m(W + 1, nnx), m1a = xc1m(W - 1, nnx), m1b = xc1m(W + 2, nnx);
+        const float dbx = XF ? 1.0f : __ldg(S.xcoef + (W + S2D_GX)).z;
+        const float m0a = XF ? kA0 : xc0m(W, nnx), m0b = XF ? kA0 : xc0m(W + 1, nnx);
+        const float m1a = XF ? kA1 : xc1m(W - 1, nnx), m1b = XF ? kA1 : xc1m(W + 2, nnx);
         const float4 mv0 = adj_ring(ring, 0, W, lane);
         const float4 ma0 = adj_ring(ring, 2, W - 1, lane), ma1 = adj_ring(ring, 2, W, lane);
         const float4 ma2 = adj_ring(ring, 2, W + 1, lane), ma3 = adj_ring(ring, 2, W + 2, lane);
@@ -294,11 +299,15 @@ __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__re
         const ShotDev &S = task_of(a, t, strip, xa, seg_len);
         if (!task_in_bounds(a, S, strip, xa, seg_len, kt, true, 2)) continue;
         const int c = strip * S2D_STRIP_OUT - 4;
-        // the z-transposes read the coefficient pairs of rows c-2 .. c+129
-        if (rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1))
-            adjoint_task<true>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else
-            adjoint_task<false>(a, S, strip, xa, seg_len, kt, lane, ring);
+        const int xb = min(S.nnx, xa + seg_len);
+        // the z-transposes read the coefficient pairs of rows c-2 .. c+129,
+        // the x-gathers those of columns xa-3 .. xb+2
+        const bool zf = rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1);
+        const bool xf = xa - 3 >= S.xfast_lo && xb + 2 < S.xfast_hi;
+        if (zf && xf) adjoint_task<true, true>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (zf) adjoint_task<true, false>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (xf) adjoint_task<false, true>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else adjoint_task<false, false>(a, S, strip, xa, seg_len, kt, lane, ring);
     }
 }
 
