@@ -169,6 +169,7 @@ struct Ctx {
     int opt_prod_variant = kVariantLdgPfProducts;  // s2d_gradient's product-writing forward (4th order)
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
+    DevBuf bar_d;             // grid-barrier counter of the persistent step kernel
     // Launch-argument block read by every step launch, and the graphs of step
     // launches captured against it (by step count and launch configuration);
     // kept for the context's lifetime, so later runs replay them.
@@ -469,6 +470,24 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
     args.fault_iter = c->opt_fault_iter;
     args.task_order = c->opt_order;
     StepArgs *args_d = c->args_d.as<StepArgs>();
+    if (lc.variant == kVariantPersist) {
+        // chunks of graph_chunk steps, one cooperative launch each (not
+        // captured: the launch itself covers the chunk)
+        const int chunk = std::max(1, c->opt_graph_chunk);
+        for (int done = 0; done < nsteps; done += chunk) {
+            const int n = std::min(chunk, nsteps - done);
+            args.kt_base = kt_begin + done;
+            args.par0 = b.cur;
+            int e = launch_set_args(args, args_d, c->stream);
+            if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+            CK(cudaMemsetAsync(c->bar_d.p, 0, sizeof(unsigned), c->stream));
+            e = launch_persist(args_d, n, c->bar_d.as<unsigned>(), lc.grid, c->stream);
+            if (e) return fail(c, S2D_ERR_CUDA, "persistent step launch: %s", cudaGetErrorString((cudaError_t)e));
+            *launches += 2;
+            b.cur ^= n & 1;
+        }
+        return S2D_OK;
+    }
     const int spl = steps_per_launch(lc.variant);
     const int nl = nsteps / spl, rem = nsteps - nl * spl;
     const int chunk = use_graph ? std::max(1, c->opt_graph_chunk) : std::max(nl, 1);
@@ -800,6 +819,7 @@ int check_device_error(Ctx *c) {
 constexpr int kTuneCandidates[][3] = {
     {kVariantLdg128, 128, 0}, {kVariantLdgPf4, 128, 0}, {kVariantLdgPf, 128, 0},      {kVariantBulk128, 128, 3},
     {kVariantTs2, 128, 0},    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
+    {kVariantPersist, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
@@ -811,7 +831,7 @@ constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
 // FD steps the trials take (a two-step candidate advances two per launch).
 constexpr int tune_steps(const int (*cand)[3], int n) {
     int steps = 0;
-    for (int i = 0; i < n; ++i) steps += (kTuneWarm + kTuneTimed) * (cand[i][0] == kVariantTs2 ? 2 : 1);
+    for (int i = 0; i < n; ++i) steps += (kTuneWarm + kTuneTimed) * steps_per_launch(cand[i][0]);
     return steps;
 }
 constexpr int kTuneSteps = tune_steps(kTuneCandidates, kNumTuneCandidates);
@@ -940,7 +960,7 @@ int s2d_set_option(void *ctx, const char *key, long value) {
         if (value != kVariantBulk && value != kVariantLdg && value != kVariantBulk128 && value != kVariantLdg128 &&
             value != kVariantTs2 && value != kVariantTma && value != kVariantAsync && value != kVariantLdgU4 &&
             value != kVariantLdgPf && value != kVariantLdgPf4 && value != kVariantLdgPfU4 &&
-            value != kVariantLdgPfU3)
+            value != kVariantLdgPfU3 && value != kVariantPersist)
             return fail(c, S2D_ERR_ARG, "unknown step kernel variant %ld", value);
         c->opt_variant = (int)value;
         c->opt_autotune = 0;
@@ -1016,6 +1036,7 @@ int s2d_create(void **ctx, int device) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = c->dev_err.alloc(sizeof(int));
+    if (e == cudaSuccess) e = c->bar_d.alloc(sizeof(unsigned));
     if (e == cudaSuccess) e = c->args_d.alloc(sizeof(StepArgs));
     if (e == cudaSuccess) e = cudaMemset(c->dev_err.p, 0, sizeof(int));
     if (e != cudaSuccess) {

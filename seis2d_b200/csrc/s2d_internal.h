@@ -149,7 +149,8 @@ enum StepVariant { kVariantBulk = 0, kVariantLdg = 1, kVariantBulk128 = 2,
                    kVariantLdgPf4 = 16 /* the same compiled for 4 blocks per SM */,
                    kVariantLdgPfU4 = 17 /* prefetch into two buffers in turn, unrolled by 4, 4 blocks per SM */,
                    kVariantLdgPfU3 = 18 /* the same compiled for 3 blocks per SM */,
-                   kVariantLdgPfProducts = 19 /* kVariantLdgPf + S2D_STEP_PRODUCTS, gradient runs */ };
+                   kVariantLdgPfProducts = 19 /* kVariantLdgPf + S2D_STEP_PRODUCTS, gradient runs */,
+                   kVariantPersist = 20 /* prefetching plain loads, many steps per cooperative launch */ };
 
 // Per-warp ring of the async variant: kAsyncStages iterations of kAsyncSlots
 // 128-row column slices (vx; px, pz, kappa, vz; bx, bz).
@@ -177,7 +178,12 @@ constexpr int kTmaMapBytes = 128;  // sizeof(CUtensorMap)
 S2D_HD inline int tma_blocks(int nshots, int nstrips) { return (nshots * nstrips + kTmaWarps - 1) / kTmaWarps; }
 
 // FD steps one launch of a variant advances.
-inline int steps_per_launch(int variant) { return variant == kVariantTs2 ? 2 : 1; }
+// (The persistent kernel runs any number of steps per launch; the autotuner's
+// trial launches of it run 4.)
+constexpr int kPersistTrialSteps = 4;
+constexpr int steps_per_launch(int variant) {
+    return variant == kVariantTs2 ? 2 : variant == kVariantPersist ? kPersistTrialSteps : 1;
+}
 // Variants whose strips are S2D_TS_OUT rows (and whose tasks stream 12 or 13 halo columns).
 inline bool ts_layout(int variant) {
     return variant == kVariantTs2 || variant == kVariantTs1 || variant == kVariantO8 || variant == kVariantO8r ||
@@ -192,7 +198,7 @@ inline bool async_variant(int variant) { return variant == kVariantAsync || vari
 inline bool plain_loads(int variant) {
     return variant == kVariantLdg || variant == kVariantLdgProducts || variant == kVariantLdg128 || variant == kVariantLdgU4 ||
            variant == kVariantLdgPf || variant == kVariantLdgPf4 || variant == kVariantLdgPfU4 ||
-           variant == kVariantLdgPfU3 || variant == kVariantLdgPfProducts ||
+           variant == kVariantLdgPfU3 || variant == kVariantLdgPfProducts || variant == kVariantPersist ||
            variant == kVariantO8 || variant == kVariantO8r || variant == kVariantO8Products;
 }
 
@@ -218,6 +224,11 @@ inline size_t bulk_smem_bytes(int warps_per_block, int stages) {
 int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int block, size_t smem,
                 void *stream);
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream);
+// Persistent step kernel: `nsteps` FD steps from args->kt_base in one
+// cooperative launch of `grid` blocks of 128 threads (all co-resident), with
+// a grid barrier on the zeroed counter `bar` between steps.
+int launch_persist(const StepArgs *args_dev, int nsteps, unsigned *bar, int grid, void *stream);
+int persist_occupancy(int *blocks_per_sm);
 // Adjoint FD step (step kt = args.kt_base - kt_off) and the gradient finalisation.
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream);
 // Adjoint FD step of the 8th-order scheme: two cell-parallel passes over

@@ -207,16 +207,25 @@ struct LdgTask {
 struct ColIn {
     float4 vx, px, pz, k, vz, bx, bz;
 };
-template <bool PROD, bool FAST, bool XF>
+// State loads: the read-only path, or (CG) loads cached in L2 only, for a
+// kernel that reads in one step what another block wrote in the previous
+// step of the same launch.
+template <bool CG>
+__device__ __forceinline__ float4 ld4s(const float *p) {
+    if (CG) return __ldcg(reinterpret_cast<const float4 *>(p));
+    return __ldg(reinterpret_cast<const float4 *>(p));
+}
+
+template <bool PROD, bool FAST, bool XF, bool CG = false>
 __device__ __forceinline__ void ldg_load(const LdgTask<PROD, FAST> &k, const ShotDev &S, int L, ColIn &in) {
     const ptrdiff_t colL = (ptrdiff_t)L * k.ld, colP = colL - k.ld, colV = colL - 3 * k.ld;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-    in.vx = ld4(k.vxi + colL);
-    in.px = ld4(k.pxi + colP);
+    in.vx = ld4s<CG>(k.vxi + colL);
+    in.px = ld4s<CG>(k.pxi + colP);
     const bool pz_live = !(FAST && (XF || __ldg(S.xcoef + (L - 1 + S2D_GX)).x == 1.0f));
-    in.pz = pz_live ? ld4(k.pzi + colP) : zero;
+    in.pz = pz_live ? ld4s<CG>(k.pzi + colP) : zero;
     in.k = ld4(k.kap + colP);
-    in.vz = ld4(k.vzi + colP);
+    in.vz = ld4s<CG>(k.vzi + colP);
     in.bx = ld4(k.bxp + colV);
     in.bz = ld4(k.bzp + colV);
 }
@@ -322,7 +331,7 @@ __device__ __forceinline__ void ldg_column(const LdgTask<PROD, FAST> &k, const S
 // names (no moves); otherwise one column per iteration.  PF: the loads of
 // column L+1 are issued before column L is computed (two columns of loads in
 // flight per warp).
-template <bool PROD, bool FAST, bool XF, bool U4, bool PF = false>
+template <bool PROD, bool FAST, bool XF, bool U4, bool PF = false, bool CG = false>
 __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                          int kt, int par, bool rec_step, int slot, int lane) {
     LdgTask<PROD, FAST> k;
@@ -359,9 +368,9 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     float4 vA = zero, vB, vC, vD;
     float4 pA = zero, pB = zero, pC = zero, pD = zero;
     float4 zA = zero, zB = zero, zC = zero, zD = zero;
-    vB = ld4(k.vxi + (ptrdiff_t)(xa - 3) * k.ld);
-    vC = ld4(k.vxi + (ptrdiff_t)(xa - 2) * k.ld);
-    vD = ld4(k.vxi + (ptrdiff_t)(xa - 1) * k.ld);
+    vB = ld4s<CG>(k.vxi + (ptrdiff_t)(xa - 3) * k.ld);
+    vC = ld4s<CG>(k.vxi + (ptrdiff_t)(xa - 2) * k.ld);
+    vD = ld4s<CG>(k.vxi + (ptrdiff_t)(xa - 1) * k.ld);
     const int Lend = k.xb + 2;
     int L = xa;
     if (PF && U4) {
@@ -395,10 +404,10 @@ __device__ __forceinline__ void ldg_task(const StepArgs &a, const ShotDev &S, in
     }
     if (PF) {
         ColIn cur, nxt;
-        ldg_load<PROD, FAST, XF>(k, S, L, nxt);
+        ldg_load<PROD, FAST, XF, CG>(k, S, L, nxt);
         for (; L <= Lend; ++L) {
             cur = nxt;
-            if (L < Lend) ldg_load<PROD, FAST, XF>(k, S, L + 1, nxt);
+            if (L < Lend) ldg_load<PROD, FAST, XF, CG>(k, S, L + 1, nxt);
             ldg_column_in<PROD, FAST, XF>(k, S, L, cur, vA, vB, vC, vD, pA, pB, pC, pD, zA, zC);
             float4 t = vA;
             vA = vB; vB = vC; vC = vD; vD = t;
@@ -454,6 +463,79 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__r
         else if (zf) ldg_task<PROD, true, false, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
         else if (xf) ldg_task<PROD, false, true, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
         else ldg_task<PROD, false, false, U4, PF>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+    }
+}
+
+// ---------------------------------------------------------- persistent variant
+//
+// One launch advances up to `nsteps` FD steps: every warp runs its tasks of
+// a step (the prefetching plain-load loop), then the grid meets at a barrier
+// before the next step, so a run of small grids (one shot, one round of
+// tasks per step) pays one launch per chunk of steps instead of one per
+// step.  The grid is exactly the co-resident blocks (a cooperative launch).
+// State written in step k is read by other blocks in step k+1 of the same
+// launch, so state loads take the L2-only path (ld.global.cg) and each block
+// fences its stores before it arrives.  The barrier is a counter that every
+// block increments once per step; a block waits (bounded: spin_limit polls)
+// for (k+1) x gridDim.x arrivals.  A wait that runs out records
+// S2D_DEV_ERR_WAIT and the block leaves; the call then returns
+// S2D_ERR_TIMEOUT.  Test knob fault_iter: block 0 does not arrive after step
+// fault_iter, so every wait of that step runs out.
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) step_kernel_persist(const StepArgs *__restrict__ A, int nsteps,
+                                                                  unsigned *bar) {
+    __shared__ int s_ok;
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int s = 0; s < nsteps; ++s) {
+        const int kt = a.kt_base + s;
+        if (kt >= a.fd_nt) return;
+        const int par = a.par0 ^ (s & 1);
+        const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
+        const int slot = (kt + 1) / a.dt_factor - 1;
+        for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+            int strip, xa, seg_len;
+            const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+            if (!task_in_bounds(a, S, strip, xa, seg_len, kt, false, 1)) continue;
+            const int c = strip * S2D_STRIP_OUT - 4;
+            const int xb = min(S.nnx, xa + seg_len);
+            const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+            const bool xf = xa - 1 >= S.xfast_lo && xb + 1 < S.xfast_hi;
+            if (zf && xf)
+                ldg_task<false, true, true, false, true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+            else if (zf)
+                ldg_task<false, true, false, false, true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+            else if (xf)
+                ldg_task<false, false, true, false, true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+            else
+                ldg_task<false, false, false, false, true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot,
+                                                                 lane);
+        }
+        if (s + 1 == nsteps) break;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (!(s == a.fault_iter && blockIdx.x == 0)) atomicAdd(bar, 1u);
+            const unsigned target = (unsigned)(s + 1) * gridDim.x;
+            bool ok = false;
+            for (int i = 0; i < a.spin_limit && !ok; ++i) {
+                ok = ld_acquire_gpu(bar) >= target;
+                if (!ok) __nanosleep(64);
+            }
+            if (!ok) atomicOr(a.err, S2D_DEV_ERR_WAIT);
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return;
     }
 }
 
@@ -1713,6 +1795,16 @@ int launch_step(int variant, const StepArgs *args_dev, int kt_off, int grid, int
     return (int)cudaGetLastError();
 }
 
+int launch_persist(const StepArgs *args_dev, int nsteps, unsigned *bar, int grid, void *stream) {
+    void *args[] = {(void *)&args_dev, (void *)&nsteps, (void *)&bar};
+    return (int)cudaLaunchCooperativeKernel((const void *)step_kernel_persist<4>, dim3(grid), dim3(128), args, 0,
+                                            (cudaStream_t)stream);
+}
+
+int persist_occupancy(int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel_persist<4>, 128, 0);
+}
+
 int launch_set_args(const StepArgs &v, StepArgs *args_dev, void *stream) {
     set_args_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(v, args_dev);
     return (int)cudaGetLastError();
@@ -1747,6 +1839,7 @@ const void *kernel_of(int variant) {
     if (variant == kVariantLdgPfU4) return (const void *)step_kernel_ldg<false, 4, true, true>;
     if (variant == kVariantLdgPfU3) return (const void *)step_kernel_ldg<false, 3, true, true>;
     if (variant == kVariantLdgPfProducts) return (const void *)step_kernel_ldg<true, 3, false, true>;
+    if (variant == kVariantPersist) return (const void *)step_kernel_persist<4>;
     if (variant == kVariantAsyncProducts) return (const void *)step_kernel_async<true, 3>;
     return (const void *)step_kernel_ldg<false, 1>;
 }

@@ -40,7 +40,7 @@ def _wave(c):
     return Wave(c["T"], c["dt"], c["ddt"], c["f"])
 
 
-VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5, "tma": 11, "async": 12, "ldgu4": 14, "ldgpf": 15, "ldgpf4": 16, "ldgpfu4": 17, "ldgpfu3": 18}
+VARIANTS = {"bulk": 0, "ldg": 1, "bulk128": 2, "ldg128": 4, "twostep": 5, "tma": 11, "async": 12, "ldgu4": 14, "ldgpf": 15, "ldgpf4": 16, "ldgpfu4": 17, "ldgpfu3": 18, "persist": 20}
 
 
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
@@ -206,12 +206,13 @@ def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
     np.testing.assert_array_equal(got, base)
 
 
-@pytest.mark.parametrize("variant", [0, 11])
+@pytest.mark.parametrize("variant", [0, 11, 20])
 def test_bounded_wait_reports_timeout_and_context_survives(ctx, variant):
-    """A pipeline barrier whose bytes never arrive (the per-warp bulk-copy
-    pipeline, and the TMA kernel's producer/consumer ring): every wait is
-    bounded, the kernel records the error and returns, the call reports
-    S2D_ERR_TIMEOUT and the next call on the same context is correct."""
+    """A wait that never completes (the per-warp bulk-copy pipeline's stage,
+    the TMA kernel's producer/consumer ring, the persistent kernel's grid
+    barrier with one block not arriving): every wait is bounded, the kernel
+    records the error and returns, the call reports S2D_ERR_TIMEOUT and the
+    next call on the same context is correct."""
     from seis2d_b200 import Shot
     from seis2d_b200._lib import Seis2dError, S2D_ERR_TIMEOUT
     z, c, vp, rho = _golden("edges_explicit_nb32")
