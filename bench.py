@@ -247,21 +247,22 @@ def surface_shots(nx, d, nshots, nrec=None):
     return src, rec
 
 
-def gradient_leg(ctx, nshots=32, T=3.0):
+def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     """FWI gradient on the 1201 x 401 models of fwi_models (nb 50, 10 Hz,
-    dt 1 ms, T seconds): the forward of `nshots` shots, then one warm-up
-    gradient and one timed gradient of the same shots, timed with CUDA events."""
+    dt 1 ms, T seconds; 4th- or 8th-order operator): the forward of `nshots`
+    shots, then one warm-up gradient and one timed gradient of the same shots,
+    timed with CUDA events."""
     import torch
     from seis2d_b200 import Shot, Wave, derive_steps
     true, start, rho = fwi_models()
     wave = Wave(T, 0.001, 0.001, 10.0)
     st = derive_steps(wave)
     src, rec = surface_shots(1201, 10.0, nshots)
-    mt = ctx.model(true, rho, 10.0, 10.0, 50)
+    mt = ctx.model(true, rho, 10.0, 10.0, 50, fd_order=fd_order)
     dobs = torch.zeros(nshots * rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
     ctx.forward([Shot(mt, s_, rec) for s_ in src], wave, out=dobs)
     mt.release()
-    ms = ctx.model(start, rho, 10.0, 10.0, 50)
+    ms = ctx.model(start, rho, 10.0, 10.0, 50, fd_order=fd_order)
     shots = [Shot(ms, s_, rec) for s_ in src]
     fbuf = torch.zeros_like(dobs)
     ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 96 steps) outside the timing
@@ -276,7 +277,7 @@ def gradient_leg(ctx, nshots=32, T=3.0):
     tg, g = _timed(lambda: ctx.gradient(shots, wave, dobs, misfit=True, grad_vp=gvp, grad_rho=grho))
     clocks = clk.stop()
     res = {"workload": f"FWI gradient, 1201x401 (seeded gradient + two +-300 m/s anomalies; start = gradient), "
-                       f"rho 2000, nb 50, {nshots} shots x 1201 receivers, nt {st['fd_nt']}",
+                       f"rho 2000, nb 50, {nshots} shots x 1201 receivers, nt {st['fd_nt']}, FD order {fd_order}",
            "gradient_s_per_shot": tg / nshots, "forward_s_per_shot": tf / nshots,
            "gradient_over_forward": tg / tf, "misfit": g.misfit,
            "checkpoint_interval": int(g.stats.grad_segment),
@@ -384,6 +385,12 @@ def extra_legs(device):
         # checkpoint every 100 steps, as the configuration states
         ctx.set_option("grad_segment", 100)
         out["c5_gradient"] = gradient_leg(ctx, 32, 3.0)
+        # the same with the 8th-order operator (its adjoint is the two-pass
+        # cell-parallel form); a failed extra leg must not cost the main line
+        try:
+            out["c5_gradient_order8"] = gradient_leg(ctx, 32, 3.0, fd_order=8)
+        except Exception as exc:
+            out["c5_gradient_order8"] = {"error": str(exc)}
         ctx.set_option("grad_segment", 0)
     return out
 
