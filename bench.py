@@ -265,7 +265,7 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     ms = ctx.model(start, rho, 10.0, 10.0, 50, fd_order=fd_order)
     shots = [Shot(ms, s_, rec) for s_ in src]
     fbuf = torch.zeros_like(dobs)
-    ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 96 steps) outside the timing
+    ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 64 steps) outside the timing
     tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
     gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
     grho = torch.zeros_like(gvp)
@@ -302,7 +302,7 @@ def extra_legs(device):
         st = derive_steps(wave)
         buf = torch.zeros(rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
         shots = [Shot(m, src[0], rec)]
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 96 steps)
+        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 64 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         l1 = ctx.last_stats
         cells = m.padded_cells * st["fd_nt"]
@@ -344,7 +344,7 @@ def extra_legs(device):
             cells_step += 16 * mm.padded_cells
             total_rec += 16 * rec.shape[0]
         buf = torch.zeros(total_rec * st["real_nt"], dtype=torch.float32, device="cuda")
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 96 steps)
+        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 64 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak

@@ -144,9 +144,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 96 steps
- *                 spends 48 of them on 8 candidate configurations (variants
- *                 4, 16, 15, 2, 5, 11, 12, 20), one untimed and three timed launches
+ *                 shape (models, grids, shot counts) with at least 64 steps
+ *                 spends 32 of them on 7 candidate configurations (variants
+ *                 4, 16, 15, 2, 5, 11, 12), one untimed and three timed launches
  *                 each, in rounds (the results do not change: every candidate
  *                 computes the same bits), times them with events and keeps the
  *                 fastest per FD step for that shape in the context; runs that
@@ -168,8 +168,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 17 and 18 the prefetch with the loop unrolled by 4 at 4 and
  *                 3 blocks per SM, 20 variant 16's loop in a persistent
  *                 cooperative launch that advances "graph_chunk" steps with a
- *                 bounded grid barrier between steps; s2d_gradient always runs
- *                 one step per launch.
+ *                 bounded grid barrier between steps (an option only: slower
+ *                 than per-step launches on the grids measured);
+ *                 s2d_gradient always runs one step per launch.
  *                 For batches of S2D_MODEL_ORDER8 models: 7 register windows
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in
  *                 shared memory at 4 (each setting applies to its own order)

@@ -819,7 +819,6 @@ int check_device_error(Ctx *c) {
 constexpr int kTuneCandidates[][3] = {
     {kVariantLdg128, 128, 0}, {kVariantLdgPf4, 128, 0}, {kVariantLdgPf, 128, 0},      {kVariantBulk128, 128, 3},
     {kVariantTs2, 128, 0},    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
-    {kVariantPersist, 128, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
