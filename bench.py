@@ -522,7 +522,8 @@ def main():
                 ctx.set_option("variant", args.variant)
             if args.products_variant:
                 ctx.set_option("products_variant", args.products_variant)
-            print(json.dumps({"leg": "c5_gradient", **gradient_leg(ctx, args.shots or 32, args.grad_time)}))
+            leg = "c5_gradient" if args.fd_order == 4 else "c5_gradient_order8"
+            print(json.dumps({"leg": leg, **gradient_leg(ctx, args.shots or 32, args.grad_time, args.fd_order)}))
         return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
