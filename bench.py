@@ -508,6 +508,8 @@ def main():
                     help="gradient: only the FWI gradient leg (--shots shots, --grad-time seconds)")
     ap.add_argument("--grad-time", type=float, default=3.0, help="record length of the gradient leg (s)")
     ap.add_argument("--grad-segment", type=int, default=0, help="checkpoint interval of the gradient leg (0: auto)")
+    ap.add_argument("--adjoint-blocks", type=int, default=0,
+                    help="gradient leg: s2d_set_option 'adjoint_blocks' (0: library default)")
     ap.add_argument("--products-variant", type=int, default=0,
                     help="gradient leg: s2d_set_option 'products_variant' (0: library default)")
     ap.add_argument("--fd-order", type=int, default=4, choices=[4, 8],
@@ -522,6 +524,8 @@ def main():
                 ctx.set_option("variant", args.variant)
             if args.products_variant:
                 ctx.set_option("products_variant", args.products_variant)
+            if args.adjoint_blocks:
+                ctx.set_option("adjoint_blocks", args.adjoint_blocks)
             leg = "c5_gradient" if args.fd_order == 4 else "c5_gradient_order8"
             print(json.dumps({"leg": leg, **gradient_leg(ctx, args.shots or 32, args.grad_time, args.fd_order)}))
         return 0

@@ -190,7 +190,8 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 derivatives: 3 plain loads, 19 plain loads with the next
  *                 column prefetched (default)
  *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 (default) or 4
- *                 blocks of 128 threads per SM
+ *                 blocks of 128 threads per SM, or 12: 2 blocks per SM with
+ *                 the next column's loads issued before a column is computed
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
  *                 longest that fits in free device memory (default)
  *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of

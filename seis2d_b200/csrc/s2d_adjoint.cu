@@ -109,9 +109,20 @@ __device__ __forceinline__ float4 &adj_ring(float4 *ring, int field, int col, in
     return ring[(field * kAdjRing + ((col + 2 * S2D_GX) & (kAdjRing - 1))) * 32 + lane];
 }
 
+// The loads of one column L of the adjoint loop (prefetching form): mvx'
+// and bx at L; at Q = L-1 the column coefficients, mpx, mvz, mpz, bz, kappa
+// and the step's products (first two slots where the lane updates Q, last two
+// where Q is imaged).
+struct AdjIn {
+    float4 m, b, xq, mpx, mvz, mpz, bz, kk, pa, pc, pg, ph;
+    float lx;
+};
+
 // XF: every column the task touches (xa-3 .. xb+2) lies in the shot's
-// x-interior: literal column coefficients, no coefficient loads.
-template <bool FAST, bool XF = false>
+// x-interior: literal column coefficients, no coefficient loads.  PF: the
+// loads of column L+1 are issued before column L is computed (two columns
+// in flight per warp); otherwise each value is loaded where it is used.
+template <bool FAST, bool XF = false, bool PF = false>
 __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                              int kt, int lane, float4 *ring) {
     const int nnx = S.nnx;
@@ -150,12 +161,40 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 tbp = zero;                                      // tbx at Q-1
     const float kx = S.kx_in;
+    auto fetch = [&](int L, AdjIn &in) {
+        const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
+        in.m = ld4(mvxi + colL);
+        in.b = ld4(bxp + colL);
+        in.lx = XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
+        if (L < xa) return;
+        const int Q = L - 1;
+        const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
+        in.xq = XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));
+        const bool pz_live = !(FAST && (XF || in.xq.x == 1.0f));
+        const bool upd = Q >= xa && Q < xb && ln.owner;
+        const bool img = Q >= 0 && Q < xb;
+        in.mpx = ld4(mpxi + colQ);
+        in.mvz = ld4(mvzi + colQ);
+        in.mpz = pz_live ? ld4(mpzi + colQ) : zero;
+        in.bz = ld4(bzp + colQ);
+        in.kk = ld4(kap + colQ);
+        in.pa = upd ? ld4(pr + colQ) : zero;
+        in.pc = upd && pz_live ? ld4(pr + F + colQ) : zero;
+        in.pg = img ? ld4(pr + 2 * F + colQ) : zero;
+        in.ph = img ? ld4(pr + 3 * F + colQ) : zero;
+    };
+    AdjIn cur, nxt;
+    if (PF) fetch(xa - 3, nxt);
 
     for (int L = xa - 3; L <= xb + 2; ++L) {
+        if (PF) {
+            cur = nxt;
+            if (L < xb + 2) fetch(L + 1, nxt);
+        }
         {
             const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
-            const float4 m = ld4(mvxi + colL), b = ld4(bxp + colL);
-            const float lx = XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
+            const float4 m = PF ? cur.m : ld4(mvxi + colL), b = PF ? cur.b : ld4(bxp + colL);
+            const float lx = PF ? cur.lx : XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
             adj_ring(ring, 0, L, lane) = m;
             adj_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
                                                      (lx * b.w) * m.w);
@@ -166,20 +205,27 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const bool in_seg = Q >= xa && Q < xb;
         const bool upd = in_seg && ln.owner;       // this lane writes column Q
         const bool img = Q >= 0 && Q < xb;         // buoyancy terms at Q (xa-1 feeds column xa)
-        const float4 xq = XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));  // Dax, Kx, Dbx, Lx
-        const bool colm = XF || xq.x == 1.0f;
+        const float4 xq = PF ? cur.xq : XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));
+        const bool colm = XF || xq.x == 1.0f;  // xq: Dax, Kx, Dbx, Lx at Q
         const bool pz_live = !(FAST && colm);  // some cell of the column keeps mpz
-        const float4 mpx = ld4(mpxi + colQ), mvz = ld4(mvzi + colQ);
-        const float4 mpz = pz_live ? ld4(mpzi + colQ) : zero;
-        const float4 bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
+        const float4 mpx = PF ? cur.mpx : ld4(mpxi + colQ), mvz = PF ? cur.mvz : ld4(mvzi + colQ);
+        const float4 mpz = PF ? cur.mpz : pz_live ? ld4(mpzi + colQ) : zero;
+        const float4 bz = PF ? cur.bz : ld4(bzp + colQ), kk = PF ? cur.kk : ld4(kap + colQ);
         float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tb = zero;
-        if (upd) {
-            pa = ld4(pr + colQ);
-            if (pz_live) pc = ld4(pr + F + colQ);
-        }
-        if (img) {
-            pg = ld4(pr + 2 * F + colQ);
-            ph = ld4(pr + 3 * F + colQ);
+        if (PF) {
+            pa = cur.pa;
+            pc = cur.pc;
+            pg = cur.pg;
+            ph = cur.ph;
+        } else {
+            if (upd) {
+                pa = ld4(pr + colQ);
+                if (pz_live) pc = ld4(pr + F + colQ);
+            }
+            if (img) {
+                pg = ld4(pr + 2 * F + colQ);
+                ph = ld4(pr + 3 * F + colQ);
+            }
         }
         const float4 r0 = zrow(ln, 0), r1 = zrow(ln, 1), r2 = zrow(ln, 2), r3 = zrow(ln, 3);
         // merged cells (both pressure dampings 1) carry one pressure adjoint
@@ -284,7 +330,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
 
 // MINB blocks of 4 warps per SM: 2 leaves the compiler its registers, 3 caps
 // them at 168 (12 warps per SM), 4 at 128 (16 warps per SM, some spills).
-template <int MINB>
+template <int MINB, bool PF = false>
 __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
     extern __shared__ __align__(128) unsigned char smem[];
     float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kAdjWarpBytes);
@@ -304,10 +350,10 @@ __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__re
         // the x-gathers those of columns xa-3 .. xb+2
         const bool zf = rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1);
         const bool xf = xa - 3 >= S.xfast_lo && xb + 2 < S.xfast_hi;
-        if (zf && xf) adjoint_task<true, true>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else if (zf) adjoint_task<true, false>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else if (xf) adjoint_task<false, true>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else adjoint_task<false, false>(a, S, strip, xa, seg_len, kt, lane, ring);
+        if (zf && xf) adjoint_task<true, true, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (zf) adjoint_task<true, false, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (xf) adjoint_task<false, true, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else adjoint_task<false, false, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
     }
 }
 
@@ -515,22 +561,25 @@ int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int 
     return (int)cudaGetLastError();
 }
 
+namespace {
+// minb 2, 3, 4: blocks per SM the kernel is built for; 12: 2 blocks per SM
+// with the next column's loads prefetched
+using AdjKernel = void (*)(const StepArgs *, int);
+AdjKernel adjoint_kernel_of(int minb) {
+    if (minb == 12) return adjoint_kernel<2, true>;
+    return minb >= 4 ? adjoint_kernel<4> : minb == 3 ? adjoint_kernel<3> : adjoint_kernel<2>;
+}
+}  // namespace
+
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream) {
     const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
-    if (minb >= 4)
-        adjoint_kernel<4><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
-    else if (minb == 3)
-        adjoint_kernel<3><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
-    else
-        adjoint_kernel<2><<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
+    adjoint_kernel_of(minb)<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
     const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        blocks_per_sm, minb >= 4 ? adjoint_kernel<4> : minb == 3 ? adjoint_kernel<3> : adjoint_kernel<2>, block,
-        smem);
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint_kernel_of(minb), block, smem);
 }
 
 int launch_gradient_finalize(float *const *gk, float *const *gb, int nshots, int nacc, const int *src_cells,

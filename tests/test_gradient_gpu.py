@@ -247,3 +247,25 @@ def test_products_variants_give_the_same_gradient(ctx):
         ctx.set_option("grad_segment", 0)
     np.testing.assert_array_equal(out[3].grad_vp, out[19].grad_vp)
     np.testing.assert_array_equal(out[3].grad_rho, out[19].grad_rho)
+
+
+def test_adjoint_forms_give_the_same_gradient(ctx):
+    """The adjoint kernel's builds (3 blocks per SM, the default; 2; 2 with
+    the next column prefetched) share its arithmetic: one shot's gradient is
+    the same bit for bit."""
+    from seis2d_b200 import Shot
+    vp, rho = _model(47)
+    src, rec = _geom(290.0)
+    nt = O.derive(O.Params(NX, NZ, NB, D, D, T, DT, DDT, F))["real_nt"]
+    adj = np.random.default_rng(53).standard_normal((rec.shape[0], nt)).astype(np.float32)
+    m = ctx.model(vp, rho, D, D, NB)
+    out = {}
+    try:
+        for ab in (3, 2, 12):
+            ctx.set_option("adjoint_blocks", ab)
+            out[ab] = ctx.gradient([Shot(m, src, rec)], _wave(), adj)
+    finally:
+        ctx.set_option("adjoint_blocks", 3)
+    for ab in (2, 12):
+        np.testing.assert_array_equal(out[ab].grad_vp, out[3].grad_vp)
+        np.testing.assert_array_equal(out[ab].grad_rho, out[3].grad_rho)
