@@ -1222,8 +1222,16 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         t1 = std::max(t0, std::min(t1, rs.real_nt));
         if (t1 > t0) {
             const size_t rows = b.seis_elems / rs.real_nt;
-            CK(cudaMemcpy2DAsync(seis_out + t0, sizeof(float) * rs.real_nt, b.seis_d + t0, sizeof(float) * rs.real_nt,
-                                 sizeof(float) * (t1 - t0), rows, cudaMemcpyDeviceToHost, c->stream));
+            if (t1 - t0 == rs.real_nt) {
+                // whole traces: one contiguous copy (a copy of one row per
+                // trace would take the copy engine row by row)
+                CK(cudaMemcpyAsync(seis_out, b.seis_d, sizeof(float) * b.seis_elems, cudaMemcpyDeviceToHost,
+                                   c->stream));
+            } else {
+                CK(cudaMemcpy2DAsync(seis_out + t0, sizeof(float) * rs.real_nt, b.seis_d + t0,
+                                     sizeof(float) * rs.real_nt, sizeof(float) * (t1 - t0), rows,
+                                     cudaMemcpyDeviceToHost, c->stream));
+            }
         }
         CK(cudaStreamSynchronize(c->stream));
     } else if (flags & S2D_SYNC) {
