@@ -944,7 +944,8 @@ __device__ __forceinline__ float4 zdp8(const Lane<FAST> &ln, int i) {
 
 // New p at column P from vx at P-4 .. P+3 (w), old px, pz, kappa and vz at P;
 // the step's first two products (as p_cell forms them) in dxv, dzv.
-template <bool FAST>
+// XF: column P lies in the 8th-order x-interior (8-tap pair, dampings 1).
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev &S, int P, const float4 &xc,
                                             bool colm, const float4 (&w)[8], const float4 &px, const float4 &pz,
                                             const float4 &kk, const float4 &vz, float4 &pxn, float4 &pzn,
@@ -958,7 +959,7 @@ __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev 
     const float dz1 = dif8(zdm8(ln, 1), vz.y - vz.x, vz.z - u3, vz.w - u2, d0 - u1);
     const float dz2 = dif8(zdm8(ln, 2), vz.z - vz.y, vz.w - vz.x, d0 - u3, d1 - u2);
     const float dz3 = dif8(zdm8(ln, 3), vz.w - vz.z, d0 - vz.y, d1 - vz.x, d2 - u3);
-    const float4 cx = dm8(P, S.nnx);
+    const float4 cx = XF ? make_float4(kC81, kC82, kC83, kC84) : dm8(P, S.nnx);
     const float dx0 = dif8(cx, w[4].x - w[3].x, w[5].x - w[2].x, w[6].x - w[1].x, w[7].x - w[0].x);
     const float dx1 = dif8(cx, w[4].y - w[3].y, w[5].y - w[2].y, w[6].y - w[1].y, w[7].y - w[0].y);
     const float dx2 = dif8(cx, w[4].z - w[3].z, w[5].z - w[2].z, w[6].z - w[1].z, w[7].z - w[0].z);
@@ -983,12 +984,13 @@ __device__ __forceinline__ float4 p_update8(const Lane<FAST> &ln, const ShotDev 
 
 // Velocities at column V from new p at V-3 .. V+4 (pw), old vx, vz and bx, bz
 // at V; D+x p and D+z p in dxp, dzp.
-template <bool FAST>
+// XF: column V lies in the 8th-order x-interior: no coefficient load.
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S, int V, const float4 (&pw)[8],
                                           const float4 &vx, const float4 &vz, const float4 &bx, const float4 &bz,
                                           float4 &vxn, float4 &vzn, float4 &dxp, float4 &dzp) {
-    const float4 xc = __ldg(S.xcoef + (V + S2D_GX));
-    const float4 cx = dp8(V, S.nnx);
+    const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (V + S2D_GX));
+    const float4 cx = XF ? make_float4(kC81, kC82, kC83, kC84) : dp8(V, S.nnx);
     const float ex0 = dif8(cx, pw[4].x - pw[3].x, pw[5].x - pw[2].x, pw[6].x - pw[1].x, pw[7].x - pw[0].x);
     const float ex1 = dif8(cx, pw[4].y - pw[3].y, pw[5].y - pw[2].y, pw[6].y - pw[1].y, pw[7].y - pw[0].y);
     const float ex2 = dif8(cx, pw[4].z - pw[3].z, pw[5].z - pw[2].z, pw[6].z - pw[1].z, pw[7].z - pw[0].z);
@@ -1022,7 +1024,9 @@ __device__ __forceinline__ void v_update8(const Lane<FAST> &ln, const ShotDev &S
 // One (shot, strip, segment) task of the 8th-order step.  Columns read:
 // vx at xa-7 .. xb+6, px, pz, kappa, vz at xa-3 .. xb+3, bx, bz at xa .. xb-1
 // (inside the 8 ghost columns on each side).
-template <bool FAST, bool PROD>
+// XF: every column the task updates or differentiates lies in the 8th-order
+// x-interior (literal coefficients, no coefficient loads).
+template <bool FAST, bool PROD, bool XF = false>
 __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len, int kt,
                                         int par, bool rec_step, int slot, int lane) {
     const int xb = min(S.nnx, xa + seg_len);
@@ -1030,8 +1034,10 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
     const int c = strip * S2D_TS_OUT - 8;
     Lane<FAST> ln;
     lane_setup(ln, S, c, lane, kt);
-    ln.owner = lane >= 2 && lane <= 29;
-    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    ln.owner = lane >= 2 && lane <= 29 && ln.z0 >= 0 && ln.z0 < S.nnz;
+    // receivers only where the strip's rows hold some
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD) &&
+                     c + S2D_STRIP_ROWS > S.rec_zlo && c <= S.rec_zhi;
     const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const int fs = S.fstride;
     float *const sb = S.st[0][0] + off;
@@ -1065,12 +1071,13 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
         for (int i = 0; i < 7; ++i) w[i] = w[i + 1];
         w[7] = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
         const float4 vz = ld4(vzi + colP);
-        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
-        const bool colm = xc.x == 1.0f;
+        const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = XF || xc.x == 1.0f;
         const bool pz_live = !(FAST && colm);
         float4 pxn, pzn, dxv, dzv;
-        const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
-                                    ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
+        const float4 pn = p_update8<FAST, XF>(ln, S, P, xc, colm, w, ld4(pxi + colP),
+                                              pz_live ? ld4(pzi + colP) : zero, ld4(kap + colP), vz, pxn, pzn,
+                                              dxv, dzv);
         const bool in_seg = P >= xa && P < xb;
         if (in_seg && ln.owner) {
             st4(pxo + colP, pxn);
@@ -1091,7 +1098,7 @@ __device__ __forceinline__ void o8_task(const StepArgs &a, const ShotDev &S, int
             const int V = L - 7;
             const ptrdiff_t colV = (ptrdiff_t)V * (ptrdiff_t)ld;
             float4 vxn, vzn, dxp, dzp;
-            v_update8(ln, S, V, pw, w[0], zq[0], ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
+            v_update8<FAST, XF>(ln, S, V, pw, w[0], zq[0], ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
             if (ln.owner) {
                 st4(vxo + colV, vxn);
                 st4(vzo + colV, vzn);
@@ -1218,10 +1225,15 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__re
         if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
         const int c = strip * S2D_TS_OUT - 8;
         // literal coefficients: every row of the strip 8th-order and undamped in z
-        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
-            o8_task<true, PROD>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
-        else
-            o8_task<false, PROD>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5;
+        // pressure on columns xa-3 .. xb+3 (8-tap D-: columns [4, nnx-4]),
+        // velocities on xa .. xb-1 (D+: [3, nnx-5]), all undamped in x
+        const int xb = min(S.nnx, xa + seg_len);
+        const bool xf = xa - 3 >= max(S.xfast_lo, 4) && xb + 3 < min(S.xfast_hi, S.nnx - 3);
+        if (zf && xf) o8_task<true, PROD, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (zf) o8_task<true, PROD, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else if (xf) o8_task<false, PROD, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
+        else o8_task<false, PROD, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane);
     }
 }
 
