@@ -186,6 +186,10 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 (same results, a check of the fast path)
  *   "graph_chunk" FD steps per captured CUDA graph, replayed as often as a
  *                 run needs (default 64)
+ *   "adjoint8_form" s2d_gradient of 8th-order models: 0 (default) one
+ *                 streaming pass per step (8-column shared-memory rings for the
+ *                 x-gathers, shuffles for the z-gathers), 1 two cell-parallel
+ *                 passes with the gathers read from memory
  *   "products_variant" s2d_gradient's forward recompute that keeps the step
  *                 derivatives: 3 plain loads, 19 plain loads with the next
  *                 column prefetched (default)

@@ -552,7 +552,266 @@ __global__ void __launch_bounds__(128) adjoint8_velocity(const StepArgs *__restr
     atomicAdd(S.grad[1] + id, 0.5f * ((tbx + tbxm) + (tbz + tbzm)));
 }
 
+// ---------------------------------------------------------------- 8th order, streaming
+//
+// The adjoint step of the 8th-order scheme as one streaming pass (the
+// algebra of adjoint8_pressure / adjoint8_velocity, the same products in the
+// same order per cell): a warp owns a 128-row strip read from 112k - 8 and
+// writes its middle 112 rows (lanes 2..29, the 8th-order forward's layout),
+// streaming along x.  At loop column L it loads mvx' and bx; at Q = L-3 it
+// forms the pressure adjoint (x-gather of Lx bx mvx' over Q-4 .. Q+3, z-gather
+// of Lz bz mvz' over the rows z-4 .. z+3 by shuffles from the neighbouring
+// lanes), the z-velocity adjoint (z-gather of Kz kappa mPZ) and the imaging
+// terms; at W = L-7 the x-velocity adjoint (x-gather of Kx kappa mPX over
+// W-3 .. W+4).  The x-gathers read 8-column per-warp shared-memory rings of
+// mvx', Lx bx mvx' and Kx kappa mPX; each lane reads back only what it wrote.
+constexpr int kAdj8Ring = 8, kAdj8Fields = 3;
+constexpr int kAdj8WarpBytes = kAdj8Ring * kAdj8Fields * S2D_STRIP_ROWS * 4;
+__device__ __forceinline__ float4 &adj8_ring(float4 *ring, int field, int col, int lane) {
+    return ring[(field * kAdj8Ring + ((col + 2 * S2D_GX) & (kAdj8Ring - 1))) * 32 + lane];
+}
+__device__ __forceinline__ float c8(const float4 &c, int k) { return comp(c, k); }
+
+// FAST: every row the task touches is in the 8th-order z-interior (literal
+// coefficients, no z-damping); XF: likewise every column.
+template <bool FAST, bool XF>
+__device__ __forceinline__ void adjoint8s_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
+                                               int kt, int lane, float4 *ring) {
+    const int nnx = S.nnx, nnz = S.nnz;
+    const size_t ld = (size_t)S.ld;
+    const int xb = min(nnx, xa + seg_len);
+    const int c = strip * S2D_TS_OUT - 8;
+    const int z0 = c + S2D_ZPT * lane;
+    const bool ghost = z0 < 0 || z0 >= nnz;
+    const bool owner = lane >= 2 && lane <= 29 && !ghost;
+    const int zl = ghost ? -S2D_GZ : z0;
+    const int pin = (kt + 1) & 1, pout = kt & 1;
+    const size_t off = (size_t)(zl + S2D_GZ) + (size_t)S2D_GX * ld;
+    const size_t F = (size_t)(nnx + 2 * S2D_GX) * ld;
+    const float *__restrict__ mpxi = S.st[pin][0] + off;
+    const float *__restrict__ mpzi = S.st[pin][1] + off;
+    const float *__restrict__ mvxi = S.st[pin][2] + off;
+    const float *__restrict__ mvzi = S.st[pin][3] + off;
+    float *__restrict__ mpxo = S.st[pout][0] + off;
+    float *__restrict__ mpzo = S.st[pout][1] + off;
+    float *__restrict__ mvxo = S.st[pout][2] + off;
+    float *__restrict__ mvzo = S.st[pout][3] + off;
+    const float *__restrict__ kap = S.kappa + off;
+    const float *__restrict__ bxp = S.bx + off;
+    const float *__restrict__ bzp = S.bz + off;
+    const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
+    float *__restrict__ gk = S.grad[0] + off;
+    float *__restrict__ gb = S.grad[1] + off;
+    const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
+                     (kt + 1) / a.dt_factor - 1 < S.real_nt;
+    const int slot = (kt + 1) / a.dt_factor - 1;
+    const float kx = S.kx_in, kz = S.kz_in;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lit = make_float4(kC81, kC82, kC83, kC84);
+    // coefficient k of the forward D+ / D- row j (x: columns, z: rows)
+    auto cpx = [&](int j, int k) { return XF ? comp(lit, k) : c8(dp8(j, nnx), k); };
+    auto cmx = [&](int j, int k) { return XF ? comp(lit, k) : c8(dm8(j, nnx), k); };
+    auto cpz = [&](int j, int k) { return FAST ? comp(lit, k) : c8(dp8(j, nnz), k); };
+    auto cmz = [&](int j, int k) { return FAST ? comp(lit, k) : c8(dm8(j, nnz), k); };
+    // z-row coefficients (Daz, Kz, Dbz, Lz) of the lane's row z0 + i
+    auto zr = [&](int i) { return FAST ? make_float4(1.0f, kz, 1.0f, kz) : __ldg(S.zcoef + (z0 + i + S2D_GZ)); };
+    float4 tbp = zero;  // tbx at Q-1
+    for (int L = xa - 7; L <= xb + 6; ++L) {
+        {
+            const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
+            const float4 m = ld4(mvxi + colL), b = ld4(bxp + colL);
+            const float lx = XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
+            adj8_ring(ring, 0, L, lane) = m;
+            adj8_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
+                                                      (lx * b.w) * m.w);
+        }
+        const int Q = L - 3;
+        if (Q < xa - 3) continue;
+        const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
+        const bool upd = owner && Q >= xa && Q < xb;
+        const bool img = Q >= xa - 1 && Q < xb && Q >= 0;
+        const float4 xq = XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));
+        const bool colm = XF || xq.x == 1.0f;
+        const bool pz_live = !(FAST && colm);
+        const float4 mvz = ld4(mvzi + colQ), bz = ld4(bzp + colQ), kk = ld4(kap + colQ);
+        const float4 mpx = ld4(mpxi + colQ);
+        const float4 mpz = pz_live ? ld4(mpzi + colQ) : zero;
+        const float4 r0 = zr(0), r1 = zr(1), r2 = zr(2), r3 = zr(3);
+        const bool m0 = colm && r0.x == 1.0f, m1 = colm && r1.x == 1.0f;
+        const bool m2 = colm && r2.x == 1.0f, m3 = colm && r3.x == 1.0f;
+        // ---- pressure adjoint at Q ----
+        float qv[4];
+        {
+            // x-gather of g = Lx bx mvx' (columns Q-4 .. Q+3 in ring 1)
+            float4 acc = zero;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int j0 = Q - 1 - k, j1 = Q + k;
+                const float c0 = cpx(j0, k), c1 = cpx(j1, k);
+                const float4 g0 = adj8_ring(ring, 1, j0, lane), g1 = adj8_ring(ring, 1, j1, lane);
+                acc.x += c0 * g0.x; acc.x -= c1 * g1.x;
+                acc.y += c0 * g0.y; acc.y -= c1 * g1.y;
+                acc.z += c0 * g0.z; acc.z -= c1 * g1.z;
+                acc.w += c0 * g0.w; acc.w -= c1 * g1.w;
+            }
+            // z-gather of h = Lz bz mvz' over rows z-4 .. z+3: rows z0-4 .. z0+6
+            const float4 h = make_float4((r0.w * bz.x) * mvz.x, (r1.w * bz.y) * mvz.y, (r2.w * bz.z) * mvz.z,
+                                         (r3.w * bz.w) * mvz.w);
+            float hh[11];
+            hh[0] = __shfl_up_sync(kFull, h.x, 1);
+            hh[1] = __shfl_up_sync(kFull, h.y, 1);
+            hh[2] = __shfl_up_sync(kFull, h.z, 1);
+            hh[3] = __shfl_up_sync(kFull, h.w, 1);
+            hh[4] = h.x; hh[5] = h.y; hh[6] = h.z; hh[7] = h.w;
+            hh[8] = __shfl_down_sync(kFull, h.x, 1);
+            hh[9] = __shfl_down_sync(kFull, h.y, 1);
+            hh[10] = __shfl_down_sync(kFull, h.z, 1);
+            qv[0] = acc.x; qv[1] = acc.y; qv[2] = acc.z; qv[3] = acc.w;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int z = z0 + i;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    qv[i] += cpz(z - 1 - k, k) * hh[4 + i - 1 - k];
+                    qv[i] -= cpz(z + k, k) * hh[4 + i + k];
+                }
+            }
+        }
+        // transpose of the receiver sampling (cpumodelling.cpp:356-360)
+        if (inj && Q >= 0 && Q < nnx) {
+            const int j1 = __ldg(S.rec_ptr + Q + 1);
+            for (int j = __ldg(S.rec_ptr + Q); j < j1; ++j) {
+                const int d = __ldg(S.rec_z + j) - z0;
+                if (d >= 0 && d < 4) qv[d] += __ldg(S.seis + (size_t)__ldg(S.rec_id + j) * S.real_nt + slot);
+            }
+        }
+        const float4 mPX = make_float4(mpx.x + qv[0], mpx.y + qv[1], mpx.z + qv[2], mpx.w + qv[3]);
+        const float4 mPZ = make_float4(m0 ? mPX.x : mpz.x + qv[0], m1 ? mPX.y : mpz.y + qv[1],
+                                       m2 ? mPX.z : mpz.z + qv[2], m3 ? mPX.w : mpz.w + qv[3]);
+        if (upd) {
+            st4(mpxo + colQ, make_float4(xq.x * mPX.x, xq.x * mPX.y, xq.x * mPX.z, xq.x * mPX.w));
+            if (pz_live)
+                st4(mpzo + colQ, make_float4(m0 ? 0.0f : r0.x * mPZ.x, m1 ? 0.0f : r1.x * mPZ.y,
+                                             m2 ? 0.0f : r2.x * mPZ.z, m3 ? 0.0f : r3.x * mPZ.w));
+            const float4 pa = ld4(pr + colQ);
+            const float4 pc = pz_live ? ld4(pr + F + colQ) : zero;
+            float4 tk;
+            tk.x = m0 ? pa.x * mPX.x : (xq.y * pa.x) * mPX.x + (r0.y * pc.x) * mPZ.x;
+            tk.y = m1 ? pa.y * mPX.y : (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
+            tk.z = m2 ? pa.z * mPX.z : (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
+            tk.w = m3 ? pa.w * mPX.w : (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
+            atomicAdd(reinterpret_cast<float4 *>(gk + colQ), tk);
+            if (Q == S.src_x && S.src_z - z0 >= 0 && S.src_z - z0 < 4) S.srcadj[kt] = comp(mPX, S.src_z - z0);
+        }
+        adj8_ring(ring, 2, Q, lane) = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y,
+                                                  (xq.y * kk.z) * mPX.z, (xq.y * kk.w) * mPX.w);
+        // ---- z-velocity adjoint at Q: z-gather of sb = Kz kappa mPZ over rows z-3 .. z+4 ----
+        {
+            const float4 sb = make_float4((r0.y * kk.x) * mPZ.x, (r1.y * kk.y) * mPZ.y, (r2.y * kk.z) * mPZ.z,
+                                          (r3.y * kk.w) * mPZ.w);
+            float ss[11];  // rows z0-3 .. z0+7
+            ss[0] = __shfl_up_sync(kFull, sb.y, 1);
+            ss[1] = __shfl_up_sync(kFull, sb.z, 1);
+            ss[2] = __shfl_up_sync(kFull, sb.w, 1);
+            ss[3] = sb.x; ss[4] = sb.y; ss[5] = sb.z; ss[6] = sb.w;
+            ss[7] = __shfl_down_sync(kFull, sb.x, 1);
+            ss[8] = __shfl_down_sync(kFull, sb.y, 1);
+            ss[9] = __shfl_down_sync(kFull, sb.z, 1);
+            ss[10] = __shfl_down_sync(kFull, sb.w, 1);
+            float gz[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int z = z0 + i;
+                gz[i] = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    gz[i] += cmz(z - k, k) * ss[3 + i - k];
+                    gz[i] -= cmz(z + 1 + k, k) * ss[3 + i + 1 + k];
+                }
+            }
+            if (upd)
+                st4(mvzo + colQ, make_float4(r0.z * mvz.x + gz[0], r1.z * mvz.y + gz[1], r2.z * mvz.z + gz[2],
+                                             r3.z * mvz.w + gz[3]));
+        }
+        // ---- buoyancy imaging at Q ----
+        if (img) {
+            const float4 pg = ld4(pr + 2 * F + colQ);
+            const float4 mv2 = adj8_ring(ring, 0, Q, lane);
+            const float4 tbx = make_float4((xq.w * pg.x) * mv2.x, (xq.w * pg.y) * mv2.y, (xq.w * pg.z) * mv2.z,
+                                           (xq.w * pg.w) * mv2.w);
+            const float4 ph = ld4(pr + 3 * F + colQ);
+            const float4 tbz = make_float4((r0.w * ph.x) * mvz.x, (r1.w * ph.y) * mvz.y, (r2.w * ph.z) * mvz.z,
+                                           (r3.w * ph.w) * mvz.w);
+            const float up = __shfl_up_sync(kFull, tbz.w, 1);  // img is the same for the whole warp
+            if (upd) {
+                const float4 px = Q >= 1 ? tbp : zero;
+                float4 tb;
+                tb.x = 0.5f * ((tbx.x + px.x) + (tbz.x + (z0 >= 1 ? up : 0.0f)));
+                tb.y = 0.5f * ((tbx.y + px.y) + (tbz.y + tbz.x));
+                tb.z = 0.5f * ((tbx.z + px.z) + (tbz.z + tbz.y));
+                tb.w = 0.5f * ((tbx.w + px.w) + (tbz.w + tbz.z));
+                atomicAdd(reinterpret_cast<float4 *>(gb + colQ), tb);
+            }
+            tbp = tbx;
+        }
+        // ---- x-velocity adjoint at W = L - 7: x-gather of Kx kappa mPX over W-3 .. W+4 ----
+        const int W = L - 7;
+        if (W < xa || W >= xb || !owner) continue;
+        const ptrdiff_t colW = (ptrdiff_t)W * (ptrdiff_t)ld;
+        const float dbx = XF ? 1.0f : __ldg(S.xcoef + (W + S2D_GX)).z;
+        const float4 mv0 = adj8_ring(ring, 0, W, lane);
+        float4 gx = zero;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float c0 = cmx(W - k, k), c1 = cmx(W + 1 + k, k);
+            const float4 s0 = adj8_ring(ring, 2, W - k, lane), s1 = adj8_ring(ring, 2, W + 1 + k, lane);
+            gx.x += c0 * s0.x; gx.x -= c1 * s1.x;
+            gx.y += c0 * s0.y; gx.y -= c1 * s1.y;
+            gx.z += c0 * s0.z; gx.z -= c1 * s1.z;
+            gx.w += c0 * s0.w; gx.w -= c1 * s1.w;
+        }
+        st4(mvxo + colW, make_float4(dbx * mv0.x + gx.x, dbx * mv0.y + gx.y, dbx * mv0.z + gx.z, dbx * mv0.w + gx.w));
+    }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) adjoint8s_kernel(const StepArgs *__restrict__ A, int kt_off) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kAdj8WarpBytes);
+    const StepArgs a = *A;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const int kt = a.kt_base - kt_off;
+    if (kt < 0 || kt >= a.fd_nt) return;
+    for (int t = gwarp; t < a.total_tasks; t += nwarp) {
+        int strip, xa, seg_len;
+        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const int c = strip * S2D_TS_OUT - 8;
+        const int xb = min(S.nnx, xa + seg_len);
+        // rows c-4 .. c+131 take part (gathers reach 4 rows past the strip)
+        const bool zf = rows_fast(S, c - 4, c + S2D_STRIP_ROWS + 3) && c - 4 >= 4 &&
+                        c + S2D_STRIP_ROWS + 3 <= S.nnz - 5;
+        // columns xa-7 .. xb+6 take part
+        const bool xf = xa - 7 >= max(S.xfast_lo, 4) && xb + 6 < min(S.xfast_hi, S.nnx - 4);
+        if (zf && xf) adjoint8s_task<true, true>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (zf) adjoint8s_task<true, false>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else if (xf) adjoint8s_task<false, true>(a, S, strip, xa, seg_len, kt, lane, ring);
+        else adjoint8s_task<false, false>(a, S, strip, xa, seg_len, kt, lane, ring);
+    }
+}
+
 }  // namespace
+
+int launch_adjoint8s(const StepArgs *args_dev, int kt_off, int grid, void *stream) {
+    adjoint8s_kernel<3><<<grid, 128, 4 * kAdj8WarpBytes, (cudaStream_t)stream>>>(args_dev, kt_off);
+    return (int)cudaGetLastError();
+}
+
+int adjoint8s_occupancy(int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint8s_kernel<3>, 128,
+                                                             4 * kAdj8WarpBytes);
+}
 
 int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int nshots, void *stream) {
     const dim3 blk(128), grd((nnz + 127) / 128, nnx, nshots);

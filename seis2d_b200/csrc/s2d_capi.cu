@@ -166,6 +166,7 @@ struct Ctx {
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
     int opt_adj_minb = 3;     // adjoint kernel compiled for 2, 3 or 4 blocks per SM
+    int opt_adj8_form = 0;    // 8th-order adjoint: 0 streaming pass, 1 two cell-parallel passes
     int opt_prod_variant = kVariantLdgPfProducts;  // s2d_gradient's product-writing forward (4th order)
     int last_segment = 0;     // interval the last gradient call used
     DevBuf dev_err;           // device error word of the step kernels
@@ -981,6 +982,9 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "spin_limit") {
         if (value < 1) return fail(c, S2D_ERR_ARG, "spin_limit must be >= 1");
         c->opt_spin_limit = (int)std::min<long>(value, 1L << 30);
+    } else if (k == "adjoint8_form") {
+        if (value != 0 && value != 1) return fail(c, S2D_ERR_ARG, "adjoint8_form must be 0 or 1");
+        c->opt_adj8_form = (int)value;
     } else if (k == "products_variant") {
         if (value != kVariantLdgProducts && value != kVariantLdgPfProducts)
             return fail(c, S2D_ERR_ARG, "products_variant must be %d or %d", kVariantLdgProducts, kVariantLdgPfProducts);
@@ -1300,6 +1304,20 @@ int run_adjoint8(Ctx *c, StepArgs args, int kt_top, int n, int nnx, int nnz, int
     args.kt_base = kt_top;
     int e = launch_set_args(args, args_d, c->stream);
     if (e) return fail(c, S2D_ERR_CUDA, "set_args launch: %s", cudaGetErrorString((cudaError_t)e));
+    if (c->opt_adj8_form == 0) {
+        // one streaming pass per step over the warp tasks of the current
+        // (112-row) layout, the grid exactly its resident blocks
+        int bps = 0;
+        if (adjoint8s_occupancy(&bps) || bps < 1) bps = 1;
+        const int grid = (int)std::max<long>(
+            1, std::min<long>((long)c->sm_count * bps, ((long)args.total_tasks * 32 + 127) / 128));
+        *launches += 1 + n;
+        for (int k = 0; k < n; ++k) {
+            e = launch_adjoint8s(args_d, k, grid, c->stream);
+            if (e) return fail(c, S2D_ERR_CUDA, "adjoint launch: %s", cudaGetErrorString((cudaError_t)e));
+        }
+        return S2D_OK;
+    }
     *launches += 1 + 2 * n;
     for (int k = 0; k < n; ++k) {
         e = launch_adjoint8(args_d, k, nnx, nnz, nshots, c->stream);
@@ -1415,8 +1433,9 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         adj[s].grad[1] = acc_pair + F;
         gk[s] = adj[s].grad[0];
         gb[s] = adj[s].grad[1];
-        // 8th-order adjoint: two scratch fields for its velocity gathers (ghosts stay 0)
-        if (b.order8) {
+        // 8th-order cell-parallel adjoint: two scratch fields for its velocity
+        // gathers (ghosts stay 0); the streaming form keeps them in shared memory
+        if (b.order8 && c->opt_adj8_form == 1) {
             int e = grad_alloc(c, g, 2 * fb, &p);
             if (e) return e;
             CK(cudaMemsetAsync(p, 0, 2 * fb, c->stream));
@@ -1528,7 +1547,8 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     int agrid = 1;
     auto backward_layout = [&]() -> int {
         if (b.order8) {
-            // the 8th-order adjoint runs cell-parallel: the products kernel keeps its own layout
+            // the 8th-order products kernel and the streaming adjoint share the
+            // 112-row layout (the cell-parallel adjoint needs none)
             int e = layout_groups(c, b, lc_prod);
             if (!e) e = launch_config(c, b.max_tasks, &lc_prod, prod_variant, 128, 0);
             fa.total_tasks = batch_tasks(b);

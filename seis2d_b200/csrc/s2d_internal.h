@@ -234,6 +234,10 @@ int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, in
 // Adjoint FD step of the 8th-order scheme: two cell-parallel passes over
 // `nshots` shots of one nnx x nnz grid.
 int launch_adjoint8(const StepArgs *args_dev, int kt_off, int nnx, int nnz, int nshots, void *stream);
+// Adjoint FD step of the 8th-order scheme as one streaming pass (warp tasks on
+// the 112-row strips of the batch's current layout), 4 warps per block.
+int launch_adjoint8s(const StepArgs *args_dev, int kt_off, int grid, void *stream);
+int adjoint8s_occupancy(int *blocks_per_sm);
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm);
 // Add each shot's source term to its accumulator gk[s] (the entries may all
 // be the one shared pair), sum the nacc accumulator pairs gk[0..nacc),
