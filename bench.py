@@ -247,6 +247,17 @@ def surface_shots(nx, d, nshots, nrec=None):
     return src, rec
 
 
+def phase_split(stats, t_forward_s):
+    """The gradient call's device time by phase (the library's CUDA events),
+    each as a multiple of the forward's time: the forward sweep, the
+    recomputes with products, the adjoint steps and the rest (set-up, adjoint
+    source, finalisation)."""
+    tf = t_forward_s * 1e3
+    ph = {"sweep": stats.sweep_ms, "recompute": stats.recompute_ms, "adjoint": stats.adjoint_ms}
+    ph["other"] = stats.loop_ms - sum(ph.values())
+    return {k: round(v / tf, 3) for k, v in ph.items()}
+
+
 def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     """FWI gradient on the 1201 x 401 models of fwi_models (nb 50, 10 Hz,
     dt 1 ms, T seconds; 4th- or 8th-order operator): the forward of `nshots`
@@ -281,6 +292,7 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
            "gradient_s_per_shot": tg / nshots, "forward_s_per_shot": tf / nshots,
            "gradient_over_forward": tg / tf, "misfit": g.misfit,
            "checkpoint_interval": int(g.stats.grad_segment),
+           "phases_over_forward": phase_split(g.stats, tf),
            "forward_gcells_per_s": ms.padded_cells * nshots * st["fd_nt"] / tf / 1e9,
            "clocks_during_gradient": clocks}
     ms.release()

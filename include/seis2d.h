@@ -44,7 +44,7 @@ extern "C" {
 #define S2D_API
 #endif
 
-#define S2D_ABI_VERSION 2
+#define S2D_ABI_VERSION 3
 
 /* status codes */
 #define S2D_OK 0
@@ -124,6 +124,13 @@ typedef struct {
                                 where both pressure dampings are 1 (the cell
                                 carries p alone); a pass is one FD step, or
                                 two with the two-step variant                 */
+    double sweep_ms;         /* s2d_gradient: CUDA-event time of the forward
+                                sweep (checkpoint saves included)              */
+    double recompute_ms;     /* s2d_gradient: the recomputes that keep the
+                                step products (checkpoint restores included)  */
+    double adjoint_ms;       /* s2d_gradient: the adjoint steps; loop_ms minus
+                                the three is set-up, adjoint source and
+                                finalisation                                   */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */

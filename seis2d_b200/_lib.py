@@ -23,7 +23,7 @@ S2D_ERR_STABILITY = -8
 S2D_ERR_TIMEOUT = -9
 S2D_ERR_NODEV = -10
 
-ABI_VERSION = 2  # S2D_ABI_VERSION of include/seis2d.h
+ABI_VERSION = 3  # S2D_ABI_VERSION of include/seis2d.h
 
 S2D_SEIS_DEVICE = 0x1
 S2D_PLAIN = 0x2
@@ -71,7 +71,8 @@ class Stats(C.Structure):
     _fields_ = [("loop_ms", C.c_double), ("cell_updates", C.c_double), ("gcells_per_s", C.c_double),
                 ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int),
                 ("variant", C.c_int), ("block", C.c_int), ("stages", C.c_int), ("seg_len", C.c_int),
-                ("autotuned", C.c_int), ("alg_bytes", C.c_double)]
+                ("autotuned", C.c_int), ("alg_bytes", C.c_double), ("sweep_ms", C.c_double),
+                ("recompute_ms", C.c_double), ("adjoint_ms", C.c_double)]
 
 
 # Every symbol include/seis2d.h declares, with its ctypes signature.

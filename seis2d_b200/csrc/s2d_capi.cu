@@ -185,6 +185,8 @@ struct Ctx {
     }
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // event pairs bracketing the phases of s2d_gradient (grown on demand)
+    std::vector<cudaEvent_t> phase_ev;
     std::string err = "no error";
     std::map<int, std::unique_ptr<Model>> models;
     int next_model = 1;
@@ -1062,6 +1064,7 @@ void s2d_destroy(void *ctx) {
     c->models.clear();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (cudaEvent_t e : c->phase_ev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1266,6 +1269,7 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;
         stats->grad_segment = 0;
+        stats->sweep_ms = stats->recompute_ms = stats->adjoint_ms = 0;
         stats->variant = lc.variant;
         stats->block = lc.block;
         stats->stages = lc.stages;
@@ -1284,7 +1288,23 @@ namespace {
 
 struct GradRun {
     std::vector<std::unique_ptr<DevBuf>> bufs;
+    // phase boundaries: (phase, index into Ctx::phase_ev); the time from one
+    // mark to the next counts for the first mark's phase
+    std::vector<std::pair<int, int>> marks;
 };
+enum { kPhaseOther = 0, kPhaseSweep = 1, kPhaseRecompute = 2, kPhaseAdjoint = 3 };
+
+int phase_mark(Ctx *c, GradRun &g, int phase) {
+    const int i = (int)g.marks.size();
+    if (i == (int)c->phase_ev.size()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        c->phase_ev.push_back(e);
+    }
+    CK(cudaEventRecord(c->phase_ev[i], c->stream));
+    g.marks.emplace_back(phase, i);
+    return S2D_OK;
+}
 
 int grad_alloc(Ctx *c, GradRun &g, size_t bytes, void **out) {
     cudaError_t e;
@@ -1531,6 +1551,10 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     fa.dt_factor = rs.dt_factor;
     fa.fd_nt = rs.fd_nt;
     bool graph_used = false;
+    {
+        int e = phase_mark(c, g, kPhaseSweep);
+        if (e) return e;
+    }
     // ---- forward sweep, saving the state at each segment start ----
     auto save_ckpt = [&](int j) -> int {
         const int par = (j * C) & 1;
@@ -1583,6 +1607,10 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         }
     }
     // ---- adjoint source ----
+    {
+        int e = phase_mark(c, g, kPhaseOther);
+        if (e) return e;
+    }
     DevBuf sumsq;
     CK(sumsq.alloc(sizeof(double)));
     CK(cudaMemsetAsync(sumsq.p, 0, sizeof(double), c->stream));
@@ -1605,6 +1633,8 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     for (int j = nseg - 1; j >= 0; --j) {
         const int k0 = j * C, n = std::min(C, rs.fd_nt - k0);
         if (j < nseg - 1) {
+            int e = phase_mark(c, g, kPhaseRecompute);
+            if (e) return e;
             const int par = k0 & 1;
             for (int s = 0; s < nshots; ++s)
                 for (int f = 0; f < 4; ++f)
@@ -1614,16 +1644,22 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
             a.flags = S2D_STEP_PRODUCTS | S2D_STEP_NO_RECORD;
             a.prod_kt0 = k0;
             b.cur = k0 & 1;
-            int e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
+            e = run_loop(c, b, lc_prod, a, k0, n, use_graph, &launches, &graph_used);
             if (e) return e;
         }
         StepArgs a = aa;
         a.prod_kt0 = k0;
-        int e = b.order8 ? run_adjoint8(c, a, k0 + n - 1, n, m.nnx, m.nnz, nshots, &launches)
+        int e = phase_mark(c, g, kPhaseAdjoint);
+        if (e) return e;
+        e = b.order8 ? run_adjoint8(c, a, k0 + n - 1, n, m.nnx, m.nnz, nshots, &launches)
                          : run_adjoint(c, b, g, a, k0 + n - 1, n, agrid, use_graph, &launches);
         if (e) return e;
     }
     // ---- source term, chain rule, fold ----
+    {
+        int e = phase_mark(c, g, kPhaseOther);
+        if (e) return e;
+    }
     std::vector<double> wv;
     int inject_last;
     if (wavelet) {
@@ -1718,6 +1754,16 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         stats->kernel_launches = launches;
         stats->graph_used = graph_used ? 1 : 0;
         stats->grad_segment = C;
+        double ph[4] = {0, 0, 0, 0};
+        for (size_t i = 0; i < g.marks.size(); ++i) {
+            cudaEvent_t end = i + 1 < g.marks.size() ? c->phase_ev[g.marks[i + 1].second] : c->ev1;
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, c->phase_ev[g.marks[i].second], end));
+            ph[g.marks[i].first] += t;
+        }
+        stats->sweep_ms = ph[kPhaseSweep];
+        stats->recompute_ms = ph[kPhaseRecompute];
+        stats->adjoint_ms = ph[kPhaseAdjoint];
     }
     c->last_segment = C;
     return S2D_OK;

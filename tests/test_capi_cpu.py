@@ -26,7 +26,7 @@ def _declared_symbols():
 def test_library_builds_and_loads():
     B.build()
     assert os.path.exists(L.LIB_PATH)
-    assert L.lib().s2d_abi_version() == 2
+    assert L.lib().s2d_abi_version() == 3
 
 
 def test_every_declared_symbol_is_exported():
