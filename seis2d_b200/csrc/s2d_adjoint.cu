@@ -118,13 +118,23 @@ struct AdjIn {
     float lx;
 };
 
+// Asynchronous form: the eleven column inputs of AdjIn (mvx', bx at L;
+// mpx, mvz, mpz, bz, kappa and the four product slots at Q = L-1) as 16-byte
+// cp.async copies into a per-warp ring of AS columns, issued AS-1 columns
+// ahead, so the loads in flight hold no registers.  Each lane reads back only
+// what it copied; inputs a column does not use are zero-filled copies that
+// read nothing.
+constexpr int kAdjAsyncSlots = 11;
+constexpr int kAdjAsyncStageBytes = kAdjAsyncSlots * S2D_STRIP_ROWS * 4;
+
 // XF: every column the task touches (xa-3 .. xb+2) lies in the shot's
 // x-interior: literal column coefficients, no coefficient loads.  PF: the
 // loads of column L+1 are issued before column L is computed (two columns
-// in flight per warp); otherwise each value is loaded where it is used.
-template <bool FAST, bool XF = false, bool PF = false>
+// in flight per warp); AS > 0: asynchronous copies AS-1 columns ahead into
+// `aring`; otherwise each value is loaded where it is used.
+template <bool FAST, bool XF = false, bool PF = false, int AS = 0>
 __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
-                                             int kt, int lane, float4 *ring) {
+                                             int kt, int lane, float4 *ring, float4 *aring = nullptr) {
     const int nnx = S.nnx;
     const size_t ld = (size_t)S.ld;
     const int xb = min(nnx, xa + seg_len);
@@ -153,8 +163,11 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
     float *__restrict__ gk = S.grad[0] + off;
     float *__restrict__ gb = S.grad[1] + off;
+    // receiver adjoint source on recording steps, in strips whose rows hold
+    // receivers (the lookup is three dependent loads per column)
     const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
-                     (kt + 1) / a.dt_factor - 1 < S.real_nt;
+                     (kt + 1) / a.dt_factor - 1 < S.real_nt && c + S2D_STRIP_ROWS > S.rec_zlo &&
+                     c <= S.rec_zhi;
     const int slot = (kt + 1) / a.dt_factor - 1;
     const bool row0 = FAST || z0 >= 1;  // the lane's first row has a row above it in the grid
 
@@ -185,15 +198,55 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     };
     AdjIn cur, nxt;
     if (PF) fetch(xa - 3, nxt);
+    // asynchronous form: iteration i is column L = xa-3+i
+    const int n_it = xb - xa + 6;
+    auto issue = [&](int i) {
+        float4 *st = aring + (i % (AS > 0 ? AS : 1)) * kAdjAsyncSlots * 32 + lane;
+        const int L = xa - 3 + i;
+        const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
+        cp_async16(st, mvxi + colL, true);
+        cp_async16(st + 32, bxp + colL, true);
+        if (L < xa) return;
+        const int Q = L - 1;
+        const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
+        const bool pz_live = !(FAST && (XF || __ldg(S.xcoef + (Q + S2D_GX)).x == 1.0f));
+        const bool upd = Q >= xa && Q < xb && ln.owner;
+        const bool img = Q >= 0 && Q < xb;
+        cp_async16(st + 2 * 32, mpxi + colQ, true);
+        cp_async16(st + 3 * 32, mvzi + colQ, true);
+        cp_async16(st + 4 * 32, mpzi + colQ, pz_live);
+        cp_async16(st + 5 * 32, bzp + colQ, true);
+        cp_async16(st + 6 * 32, kap + colQ, true);
+        cp_async16(st + 7 * 32, pr + colQ, upd);
+        cp_async16(st + 8 * 32, pr + F + colQ, upd && pz_live);
+        cp_async16(st + 9 * 32, pr + 2 * F + colQ, img);
+        cp_async16(st + 10 * 32, pr + 3 * F + colQ, img);
+    };
+    if constexpr (AS > 0) {
+#pragma unroll
+        for (int i = 0; i < AS - 1; ++i) {
+            if (i < n_it) issue(i);
+            cp_async_commit();
+        }
+    }
+    const float4 *as = aring;  // this column's ring slots (asynchronous form)
 
     for (int L = xa - 3; L <= xb + 2; ++L) {
         if (PF) {
             cur = nxt;
             if (L < xb + 2) fetch(L + 1, nxt);
         }
+        if constexpr (AS > 0) {
+            const int i = L - (xa - 3);
+            if (i + AS - 1 < n_it) issue(i + AS - 1);
+            cp_async_commit();
+            cp_async_wait<AS - 1>();  // column L's copies have landed
+            as = aring + (i % AS) * kAdjAsyncSlots * 32 + lane;
+        }
         {
             const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
-            const float4 m = PF ? cur.m : ld4(mvxi + colL), b = PF ? cur.b : ld4(bxp + colL);
+            const float4 m = PF ? cur.m : AS ? as[0] : ld4(mvxi + colL);
+            const float4 b = PF ? cur.b : AS ? as[32] : ld4(bxp + colL);
             const float lx = PF ? cur.lx : XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
             adj_ring(ring, 0, L, lane) = m;
             adj_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
@@ -208,15 +261,22 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const float4 xq = PF ? cur.xq : XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));
         const bool colm = XF || xq.x == 1.0f;  // xq: Dax, Kx, Dbx, Lx at Q
         const bool pz_live = !(FAST && colm);  // some cell of the column keeps mpz
-        const float4 mpx = PF ? cur.mpx : ld4(mpxi + colQ), mvz = PF ? cur.mvz : ld4(mvzi + colQ);
-        const float4 mpz = PF ? cur.mpz : pz_live ? ld4(mpzi + colQ) : zero;
-        const float4 bz = PF ? cur.bz : ld4(bzp + colQ), kk = PF ? cur.kk : ld4(kap + colQ);
+        const float4 mpx = PF ? cur.mpx : AS ? as[2 * 32] : ld4(mpxi + colQ);
+        const float4 mvz = PF ? cur.mvz : AS ? as[3 * 32] : ld4(mvzi + colQ);
+        const float4 mpz = PF ? cur.mpz : AS ? as[4 * 32] : pz_live ? ld4(mpzi + colQ) : zero;
+        const float4 bz = PF ? cur.bz : AS ? as[5 * 32] : ld4(bzp + colQ);
+        const float4 kk = PF ? cur.kk : AS ? as[6 * 32] : ld4(kap + colQ);
         float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tb = zero;
         if (PF) {
             pa = cur.pa;
             pc = cur.pc;
             pg = cur.pg;
             ph = cur.ph;
+        } else if (AS) {
+            pa = as[7 * 32];
+            pc = as[8 * 32];
+            pg = as[9 * 32];
+            ph = as[10 * 32];
         } else {
             if (upd) {
                 pa = ld4(pr + colQ);
@@ -276,7 +336,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             tk.y += m1 ? pa.y * mPX.y : (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
             tk.z += m2 ? pa.z * mPX.z : (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
             tk.w += m3 ? pa.w * mPX.w : (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
-            atomicAdd(reinterpret_cast<float4 *>(gk + colQ), tk);
+            red_add4(gk + colQ, tk);
             if (Q == S.src_x && ln.sdz >= 0 && ln.sdz < 4) S.srcadj[kt] = comp(mPX, ln.sdz);
         }
         adj_ring(ring, 2, Q, lane) = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y, (xq.y * kk.z) * mPX.z,
@@ -305,7 +365,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
                 tb.y += 0.5f * ((tbx.y + px.y) + (tbz.y + tbz.x));
                 tb.z += 0.5f * ((tbx.z + px.z) + (tbz.z + tbz.y));
                 tb.w += 0.5f * ((tbx.w + px.w) + (tbz.w + tbz.z));
-                atomicAdd(reinterpret_cast<float4 *>(gb + colQ), tb);
+                red_add4(gb + colQ, tb);
             }
             tbp = tbx;
         }
@@ -326,14 +386,19 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         ovx.w = dbx * mv0.w + (m0a * ma1.w - m0b * ma2.w + m1a * ma0.w - m1b * ma3.w);
         if (ln.owner) st4(mvxo + colW, ovx);
     }
+    if constexpr (AS > 0) cp_async_wait<0>();
 }
 
 // MINB blocks of 4 warps per SM: 2 leaves the compiler its registers, 3 caps
 // them at 168 (12 warps per SM), 4 at 128 (16 warps per SM, some spills).
-template <int MINB, bool PF = false>
+// AS > 0: the asynchronous form with an AS-column copy ring per warp after
+// its delay lines.
+template <int MINB, bool PF = false, int AS = 0>
 __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kAdjWarpBytes);
+    constexpr int kWarpBytes = kAdjWarpBytes + AS * kAdjAsyncStageBytes;
+    float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kWarpBytes);
+    float4 *aring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kWarpBytes + kAdjWarpBytes);
     const StepArgs a = *A;
     const int lane = threadIdx.x & 31;
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -350,10 +415,10 @@ __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__re
         // the x-gathers those of columns xa-3 .. xb+2
         const bool zf = rows_fast(S, c - 2, c + S2D_STRIP_ROWS + 1);
         const bool xf = xa - 3 >= S.xfast_lo && xb + 2 < S.xfast_hi;
-        if (zf && xf) adjoint_task<true, true, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else if (zf) adjoint_task<true, false, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else if (xf) adjoint_task<false, true, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
-        else adjoint_task<false, false, PF>(a, S, strip, xa, seg_len, kt, lane, ring);
+        if (zf && xf) adjoint_task<true, true, PF, AS>(a, S, strip, xa, seg_len, kt, lane, ring, aring);
+        else if (zf) adjoint_task<true, false, PF, AS>(a, S, strip, xa, seg_len, kt, lane, ring, aring);
+        else if (xf) adjoint_task<false, true, PF, AS>(a, S, strip, xa, seg_len, kt, lane, ring, aring);
+        else adjoint_task<false, false, PF, AS>(a, S, strip, xa, seg_len, kt, lane, ring, aring);
     }
 }
 
@@ -602,8 +667,11 @@ __device__ __forceinline__ void adjoint8s_task(const StepArgs &a, const ShotDev 
     const float *__restrict__ pr = S.prod + (size_t)(kt - a.prod_kt0) * 4 * F + off;
     float *__restrict__ gk = S.grad[0] + off;
     float *__restrict__ gb = S.grad[1] + off;
+    // receiver adjoint source on recording steps, in strips whose rows hold
+    // receivers (the lookup is three dependent loads per column)
     const bool inj = !(a.flags & S2D_STEP_NO_RECORD) && ((kt + 1) % a.dt_factor) == 0 &&
-                     (kt + 1) / a.dt_factor - 1 < S.real_nt;
+                     (kt + 1) / a.dt_factor - 1 < S.real_nt && c + S2D_STRIP_ROWS > S.rec_zlo &&
+                     c <= S.rec_zhi;
     const int slot = (kt + 1) / a.dt_factor - 1;
     const float kx = S.kx_in, kz = S.kz_in;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -700,7 +768,7 @@ __device__ __forceinline__ void adjoint8s_task(const StepArgs &a, const ShotDev 
             tk.y = m1 ? pa.y * mPX.y : (xq.y * pa.y) * mPX.y + (r1.y * pc.y) * mPZ.y;
             tk.z = m2 ? pa.z * mPX.z : (xq.y * pa.z) * mPX.z + (r2.y * pc.z) * mPZ.z;
             tk.w = m3 ? pa.w * mPX.w : (xq.y * pa.w) * mPX.w + (r3.y * pc.w) * mPZ.w;
-            atomicAdd(reinterpret_cast<float4 *>(gk + colQ), tk);
+            red_add4(gk + colQ, tk);
             if (Q == S.src_x && S.src_z - z0 >= 0 && S.src_z - z0 < 4) S.srcadj[kt] = comp(mPX, S.src_z - z0);
         }
         adj8_ring(ring, 2, Q, lane) = make_float4((xq.y * kk.x) * mPX.x, (xq.y * kk.y) * mPX.y,
@@ -750,7 +818,7 @@ __device__ __forceinline__ void adjoint8s_task(const StepArgs &a, const ShotDev 
                 tb.y = 0.5f * ((tbx.y + px.y) + (tbz.y + tbz.x));
                 tb.z = 0.5f * ((tbx.z + px.z) + (tbz.z + tbz.y));
                 tb.w = 0.5f * ((tbx.w + px.w) + (tbz.w + tbz.z));
-                atomicAdd(reinterpret_cast<float4 *>(gb + colQ), tb);
+                red_add4(gb + colQ, tb);
             }
             tbp = tbx;
         }
@@ -824,20 +892,33 @@ namespace {
 // minb 2, 3, 4: blocks per SM the kernel is built for; 12: 2 blocks per SM
 // with the next column's loads prefetched
 using AdjKernel = void (*)(const StepArgs *, int);
+// Kernel of an `adjoint_blocks` code: 2, 3, 4 blocks per SM; 12: 2 with the
+// register prefetch; 13: 3 with a 2-column copy ring; 14: 2 with a 3-column ring.
 AdjKernel adjoint_kernel_of(int minb) {
     if (minb == 12) return adjoint_kernel<2, true>;
+    if (minb == 13) return adjoint_kernel<3, false, 2>;
+    if (minb == 14) return adjoint_kernel<2, false, 3>;
     return minb >= 4 ? adjoint_kernel<4> : minb == 3 ? adjoint_kernel<3> : adjoint_kernel<2>;
+}
+size_t adjoint_warp_bytes(int minb) {
+    const int as = minb == 13 ? 2 : minb == 14 ? 3 : 0;
+    return (size_t)kAdjWarpBytes + (size_t)as * kAdjAsyncStageBytes;
 }
 }  // namespace
 
 int launch_adjoint(const StepArgs *args_dev, int kt_off, int grid, int block, int minb, void *stream) {
-    const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
+    const size_t smem = (size_t)(block / 32) * adjoint_warp_bytes(minb);
     adjoint_kernel_of(minb)<<<grid, block, smem, (cudaStream_t)stream>>>(args_dev, kt_off);
     return (int)cudaGetLastError();
 }
 
+// Also raises the kernel's dynamic shared-memory limit (the copy-ring forms
+// take more than 48 KB per block); called before the adjoint's launches.
 int adjoint_kernel_occupancy(int block, int minb, int *blocks_per_sm) {
-    const size_t smem = (size_t)(block / 32) * kAdjWarpBytes;
+    const size_t smem = (size_t)(block / 32) * adjoint_warp_bytes(minb);
+    cudaError_t e = cudaFuncSetAttribute(adjoint_kernel_of(minb), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return (int)e;
     return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint_kernel_of(minb), block, smem);
 }
 

@@ -992,8 +992,10 @@ int s2d_set_option(void *ctx, const char *key, long value) {
             return fail(c, S2D_ERR_ARG, "products_variant must be %d or %d", kVariantLdgProducts, kVariantLdgPfProducts);
         c->opt_prod_variant = (int)value;
     } else if (k == "adjoint_blocks") {
-        if ((value < 2 || value > 4) && value != 12)
-            return fail(c, S2D_ERR_ARG, "adjoint_blocks must be 2, 3, 4 or 12 (2 with the next column prefetched)");
+        if ((value < 2 || value > 4) && (value < 12 || value > 14))
+            return fail(c, S2D_ERR_ARG,
+                        "adjoint_blocks must be 2, 3, 4, 12 (2 with the next column prefetched), 13 or 14 (3 or 2 "
+                        "with asynchronous copies 1 or 2 columns ahead)");
         c->opt_adj_minb = (int)value;
     } else if (k == "fast_rows") {
         c->opt_fast_rows = value ? 1 : 0;

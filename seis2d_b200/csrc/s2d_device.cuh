@@ -12,6 +12,27 @@ static constexpr unsigned kFull = 0xffffffffu;
 
 static __device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 static __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+// p[0..3] += v as one vector reduction in L2 (red: no value comes back, so
+// the warp does not wait for it; p 16-byte aligned).
+static __device__ __forceinline__ void red_add4(float *p, float4 v) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+static __device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only); read =
+// false copies nothing and zero-fills the 16 bytes.
+static __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool read) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(read ? 16 : 0)
+                 : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+static __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Coefficients (c0, c1) of a0*(f[i]-f[i-1]) + a1*(f[i+1]-f[i-2]) per row of
 // the backward operators: 4th order on rows [2, n-2], plain difference on

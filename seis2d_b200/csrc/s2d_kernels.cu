@@ -541,9 +541,6 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_persist(const StepArgs 
 
 // --------------------------------------------------------------- bulk variant
 
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
@@ -1316,16 +1313,6 @@ __global__ void set_args_kernel(StepArgs v, StepArgs *dst) { *dst = v; }
 // own copy groups is the whole synchronisation.  A ghost lane's copies are
 // zero-fills that read nothing.  The arithmetic is ldg_task's: the same bits.
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool read) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
-                 "r"(read ? 16 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 template <bool PROD, bool FAST, bool XF>
 __device__ __forceinline__ void async_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
