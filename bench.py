@@ -159,6 +159,16 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver and NVML initialisation, a few hundred
+        # ms) can hold up the CUDA calls of this process: let it write its
+        # first sample before the timed region begins
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            with open(self.path) as f:
+                if f.readline().endswith("\n"):
+                    break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -293,6 +303,7 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
            "gradient_over_forward": tg / tf, "misfit": g.misfit,
            "checkpoint_interval": int(g.stats.grad_segment),
            "phases_over_forward": phase_split(g.stats, tf),
+           "call_over_loop": round(tg * 1e3 / g.stats.loop_ms, 3),
            "forward_gcells_per_s": ms.padded_cells * nshots * st["fd_nt"] / tf / 1e9,
            "clocks_during_gradient": clocks}
     ms.release()
@@ -361,6 +372,7 @@ def extra_legs(device):
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         l4 = ctx.last_stats
+        ctx.forward(shots, wave, kt_count=60, out=buf, plain=True)  # warm-up of the plain launch sequence
         tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
         prate = cells_step * 60 / tp / 1e9
         out["c4"] = {"workload": "48 shots on 601x301 / 1201x601 / 2401x801 layered models (16 each), nb 50, "

@@ -204,8 +204,9 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 blocks of 128 threads per SM, or 12: 2 blocks per SM with
  *                 the next column's loads issued before a column is computed,
  *                 or 13 / 14: 3 / 2 blocks per SM with the column inputs
- *                 copied into shared memory (cp.async) 1 / 2 columns ahead;
- *                 every form computes the same bits
+ *                 copied into shared memory (cp.async) 1 / 2 columns ahead,
+ *                 or 15: 3 blocks per SM with the per-shot inputs copied
+ *                 2 columns ahead; every form computes the same bits
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
  *                 longest that fits in free device memory (default)
  *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of

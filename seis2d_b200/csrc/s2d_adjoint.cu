@@ -124,8 +124,11 @@ struct AdjIn {
 // ahead, so the loads in flight hold no registers.  Each lane reads back only
 // what it copied; inputs a column does not use are zero-filled copies that
 // read nothing.
-constexpr int kAdjAsyncSlots = 11;
-constexpr int kAdjAsyncStageBytes = kAdjAsyncSlots * S2D_STRIP_ROWS * 4;
+// With 3 or more columns in the ring the materials (bx, bz, kappa: shared by
+// the shots, L2-resident) are loaded where they are used instead, and the ring
+// holds the eight per-shot inputs, so three columns fit three blocks per SM.
+__host__ __device__ constexpr int adj_async_slots(int as) { return as == 0 ? 0 : as < 3 ? 11 : 8; }
+__host__ __device__ constexpr int adj_async_stage_bytes(int as) { return adj_async_slots(as) * S2D_STRIP_ROWS * 4; }
 
 // XF: every column the task touches (xa-3 .. xb+2) lies in the shot's
 // x-interior: literal column coefficients, no coefficient loads.  PF: the
@@ -198,29 +201,36 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
     };
     AdjIn cur, nxt;
     if (PF) fetch(xa - 3, nxt);
-    // asynchronous form: iteration i is column L = xa-3+i
+    // asynchronous form: iteration i is column L = xa-3+i; ring slots
+    // (times 32 float4) of its inputs
+    constexpr bool kMatRing = AS < 3;
+    constexpr int kSlots = adj_async_slots(AS);
+    constexpr int sM = 0, sB = 1, sPX = kMatRing ? 2 : 1, sVZ = sPX + 1, sPZ = sPX + 2, sBZ = 5, sKK = 6;
+    constexpr int sPA = kMatRing ? 7 : 4, sPC = sPA + 1, sPG = sPA + 2, sPH = sPA + 3;
     const int n_it = xb - xa + 6;
     auto issue = [&](int i) {
-        float4 *st = aring + (i % (AS > 0 ? AS : 1)) * kAdjAsyncSlots * 32 + lane;
+        float4 *st = aring + (i % (AS > 0 ? AS : 1)) * kSlots * 32 + lane;
         const int L = xa - 3 + i;
         const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
-        cp_async16(st, mvxi + colL, true);
-        cp_async16(st + 32, bxp + colL, true);
+        cp_async16(st + sM * 32, mvxi + colL, true);
+        if (kMatRing) cp_async16(st + sB * 32, bxp + colL, true);
         if (L < xa) return;
         const int Q = L - 1;
         const ptrdiff_t colQ = (ptrdiff_t)Q * (ptrdiff_t)ld;
         const bool pz_live = !(FAST && (XF || __ldg(S.xcoef + (Q + S2D_GX)).x == 1.0f));
         const bool upd = Q >= xa && Q < xb && ln.owner;
         const bool img = Q >= 0 && Q < xb;
-        cp_async16(st + 2 * 32, mpxi + colQ, true);
-        cp_async16(st + 3 * 32, mvzi + colQ, true);
-        cp_async16(st + 4 * 32, mpzi + colQ, pz_live);
-        cp_async16(st + 5 * 32, bzp + colQ, true);
-        cp_async16(st + 6 * 32, kap + colQ, true);
-        cp_async16(st + 7 * 32, pr + colQ, upd);
-        cp_async16(st + 8 * 32, pr + F + colQ, upd && pz_live);
-        cp_async16(st + 9 * 32, pr + 2 * F + colQ, img);
-        cp_async16(st + 10 * 32, pr + 3 * F + colQ, img);
+        cp_async16(st + sPX * 32, mpxi + colQ, true);
+        cp_async16(st + sVZ * 32, mvzi + colQ, true);
+        cp_async16(st + sPZ * 32, mpzi + colQ, pz_live);
+        if (kMatRing) {
+            cp_async16(st + sBZ * 32, bzp + colQ, true);
+            cp_async16(st + sKK * 32, kap + colQ, true);
+        }
+        cp_async16(st + sPA * 32, pr + colQ, upd);
+        cp_async16(st + sPC * 32, pr + F + colQ, upd && pz_live);
+        cp_async16(st + sPG * 32, pr + 2 * F + colQ, img);
+        cp_async16(st + sPH * 32, pr + 3 * F + colQ, img);
     };
     if constexpr (AS > 0) {
 #pragma unroll
@@ -241,12 +251,12 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             if (i + AS - 1 < n_it) issue(i + AS - 1);
             cp_async_commit();
             cp_async_wait<AS - 1>();  // column L's copies have landed
-            as = aring + (i % AS) * kAdjAsyncSlots * 32 + lane;
+            as = aring + (i % AS) * kSlots * 32 + lane;
         }
         {
             const ptrdiff_t colL = (ptrdiff_t)L * (ptrdiff_t)ld;
-            const float4 m = PF ? cur.m : AS ? as[0] : ld4(mvxi + colL);
-            const float4 b = PF ? cur.b : AS ? as[32] : ld4(bxp + colL);
+            const float4 m = PF ? cur.m : AS ? as[sM * 32] : ld4(mvxi + colL);
+            const float4 b = PF ? cur.b : AS && kMatRing ? as[sB * 32] : ld4(bxp + colL);
             const float lx = PF ? cur.lx : XF ? kx : __ldg(S.xcoef + (L + S2D_GX)).w;
             adj_ring(ring, 0, L, lane) = m;
             adj_ring(ring, 1, L, lane) = make_float4((lx * b.x) * m.x, (lx * b.y) * m.y, (lx * b.z) * m.z,
@@ -261,11 +271,11 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
         const float4 xq = PF ? cur.xq : XF ? make_float4(1.0f, kx, 1.0f, kx) : __ldg(S.xcoef + (Q + S2D_GX));
         const bool colm = XF || xq.x == 1.0f;  // xq: Dax, Kx, Dbx, Lx at Q
         const bool pz_live = !(FAST && colm);  // some cell of the column keeps mpz
-        const float4 mpx = PF ? cur.mpx : AS ? as[2 * 32] : ld4(mpxi + colQ);
-        const float4 mvz = PF ? cur.mvz : AS ? as[3 * 32] : ld4(mvzi + colQ);
-        const float4 mpz = PF ? cur.mpz : AS ? as[4 * 32] : pz_live ? ld4(mpzi + colQ) : zero;
-        const float4 bz = PF ? cur.bz : AS ? as[5 * 32] : ld4(bzp + colQ);
-        const float4 kk = PF ? cur.kk : AS ? as[6 * 32] : ld4(kap + colQ);
+        const float4 mpx = PF ? cur.mpx : AS ? as[sPX * 32] : ld4(mpxi + colQ);
+        const float4 mvz = PF ? cur.mvz : AS ? as[sVZ * 32] : ld4(mvzi + colQ);
+        const float4 mpz = PF ? cur.mpz : AS ? as[sPZ * 32] : pz_live ? ld4(mpzi + colQ) : zero;
+        const float4 bz = PF ? cur.bz : AS && kMatRing ? as[sBZ * 32] : ld4(bzp + colQ);
+        const float4 kk = PF ? cur.kk : AS && kMatRing ? as[sKK * 32] : ld4(kap + colQ);
         float4 pa = zero, pc = zero, pg = zero, ph = zero, tk = zero, tb = zero;
         if (PF) {
             pa = cur.pa;
@@ -273,10 +283,10 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
             pg = cur.pg;
             ph = cur.ph;
         } else if (AS) {
-            pa = as[7 * 32];
-            pc = as[8 * 32];
-            pg = as[9 * 32];
-            ph = as[10 * 32];
+            pa = as[sPA * 32];
+            pc = as[sPC * 32];
+            pg = as[sPG * 32];
+            ph = as[sPH * 32];
         } else {
             if (upd) {
                 pa = ld4(pr + colQ);
@@ -396,7 +406,7 @@ __device__ __forceinline__ void adjoint_task(const StepArgs &a, const ShotDev &S
 template <int MINB, bool PF = false, int AS = 0>
 __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__restrict__ A, int kt_off) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int kWarpBytes = kAdjWarpBytes + AS * kAdjAsyncStageBytes;
+    constexpr int kWarpBytes = kAdjWarpBytes + AS * adj_async_stage_bytes(AS);
     float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kWarpBytes);
     float4 *aring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kWarpBytes + kAdjWarpBytes);
     const StepArgs a = *A;
@@ -405,10 +415,14 @@ __global__ void __launch_bounds__(128, MINB) adjoint_kernel(const StepArgs *__re
     const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
     const int kt = a.kt_base - kt_off;
     if (kt < 0 || kt >= a.fd_nt) return;
+    // the task's shot record in this warp's shared-memory slot
+    __shared__ ShotDev shot_rec[4];
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
-        if (!task_in_bounds(a, S, strip, xa, seg_len, kt, true, 2)) continue;
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        if (!task_in_bounds(a, G, strip, xa, seg_len, kt, true, 2)) continue;
+        warp_copy_shot(S, G, lane);
         const int c = strip * S2D_STRIP_OUT - 4;
         const int xb = min(S.nnx, xa + seg_len);
         // the z-transposes read the coefficient pairs of rows c-2 .. c+129,
@@ -852,9 +866,12 @@ __global__ void __launch_bounds__(128, MINB) adjoint8s_kernel(const StepArgs *__
     const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
     const int kt = a.kt_base - kt_off;
     if (kt < 0 || kt >= a.fd_nt) return;
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        warp_copy_shot(S, G, lane);
         const int c = strip * S2D_TS_OUT - 8;
         const int xb = min(S.nnx, xa + seg_len);
         // rows c-4 .. c+131 take part (gathers reach 4 rows past the strip)
@@ -876,7 +893,13 @@ int launch_adjoint8s(const StepArgs *args_dev, int kt_off, int grid, void *strea
     return (int)cudaGetLastError();
 }
 
+// Also raises the kernel's dynamic shared-memory limit (its 48 KB of rings
+// and the static shot records exceed the default); called before the
+// launches.
 int adjoint8s_occupancy(int *blocks_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(adjoint8s_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         4 * kAdj8WarpBytes);
+    if (e != cudaSuccess) return (int)e;
     return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, adjoint8s_kernel<3>, 128,
                                                              4 * kAdj8WarpBytes);
 }
@@ -893,16 +916,18 @@ namespace {
 // with the next column's loads prefetched
 using AdjKernel = void (*)(const StepArgs *, int);
 // Kernel of an `adjoint_blocks` code: 2, 3, 4 blocks per SM; 12: 2 with the
-// register prefetch; 13: 3 with a 2-column copy ring; 14: 2 with a 3-column ring.
+// register prefetch; 13: 3 with a 2-column copy ring; 14: 2 with a 3-column
+// ring; 15: 3 with a 3-column ring of the per-shot inputs.
 AdjKernel adjoint_kernel_of(int minb) {
     if (minb == 12) return adjoint_kernel<2, true>;
     if (minb == 13) return adjoint_kernel<3, false, 2>;
     if (minb == 14) return adjoint_kernel<2, false, 3>;
+    if (minb == 15) return adjoint_kernel<3, false, 3>;
     return minb >= 4 ? adjoint_kernel<4> : minb == 3 ? adjoint_kernel<3> : adjoint_kernel<2>;
 }
 size_t adjoint_warp_bytes(int minb) {
-    const int as = minb == 13 ? 2 : minb == 14 ? 3 : 0;
-    return (size_t)kAdjWarpBytes + (size_t)as * kAdjAsyncStageBytes;
+    const int as = minb == 13 ? 2 : minb == 14 || minb == 15 ? 3 : 0;
+    return (size_t)kAdjWarpBytes + (size_t)as * adj_async_stage_bytes(as);
 }
 }  // namespace
 

@@ -18,6 +18,17 @@ static __device__ __forceinline__ void red_add4(float *p, float4 v) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
                  : "memory");
 }
+// Copies a shot record into this warp's shared-memory slot (every lane
+// takes part; nothing may read the slot meanwhile).  Loops that re-read the
+// record's pointers and constants then read shared memory, not L1, where the
+// streamed columns evict them.
+static __device__ __forceinline__ void warp_copy_shot(ShotDev &dst, const ShotDev &src, int lane) {
+    static_assert(sizeof(ShotDev) % 8 == 0, "shot record copied in 8-byte words");
+    __syncwarp();
+    for (int i = lane; i < (int)(sizeof(ShotDev) / 8); i += 32)
+        reinterpret_cast<unsigned long long *>(&dst)[i] = reinterpret_cast<const unsigned long long *>(&src)[i];
+    __syncwarp();
+}
 static __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }

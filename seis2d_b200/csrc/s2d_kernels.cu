@@ -450,10 +450,13 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_ldg(const StepArgs *__r
     const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
-        if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        if (!task_in_bounds(a, G, strip, xa, seg_len, kt, PROD, 1)) continue;
+        warp_copy_shot(S, G, lane);
         const int c = strip * S2D_STRIP_OUT - 4;
         const int xb = min(S.nnx, xa + seg_len);
         const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
@@ -895,9 +898,12 @@ __global__ void __launch_bounds__(128, 4) step_kernel_ts(const StepArgs *__restr
     if (kt + (TWO ? 1 : 0) >= a.fd_nt) return;
     const int par = a.par0 ^ (kt_off & 1);
     float4 *ring = reinterpret_cast<float4 *>(smem + (size_t)(threadIdx.x >> 5) * kTsWarpBytes);
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        warp_copy_shot(S, G, lane);
         const int c = strip * S2D_TS_OUT - 8;
         if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1))
             ts_task<true, TWO>(a, S, strip, xa, seg_len, kt, par, lane, ring);
@@ -1216,9 +1222,12 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_o8(const StepArgs *__re
     const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        warp_copy_shot(S, G, lane);
         if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
         const int c = strip * S2D_TS_OUT - 8;
         // literal coefficients: every row of the strip 8th-order and undamped in z
@@ -1248,9 +1257,12 @@ __global__ void __launch_bounds__(128, 4) step_kernel_o8s(const StepArgs *__rest
     const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        warp_copy_shot(S, G, lane);
         if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
         const int c = strip * S2D_TS_OUT - 8;
         if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
@@ -1434,9 +1446,12 @@ __global__ void __launch_bounds__(128, MINB) step_kernel_async(const StepArgs *_
     const int par = a.par0 ^ (kt_off & 1);
     const bool rec_step = ((kt + 1) % a.dt_factor) == 0;
     const int slot = (kt + 1) / a.dt_factor - 1;
+    __shared__ ShotDev shot_rec[4];  // the task's shot record, one slot per warp
+    ShotDev &S = shot_rec[(threadIdx.x >> 5) & 3];
     for (int t = gwarp; t < a.total_tasks; t += nwarp) {
         int strip, xa, seg_len;
-        const ShotDev &S = task_of(a, t, strip, xa, seg_len);
+        const ShotDev &G = task_of(a, t, strip, xa, seg_len);
+        warp_copy_shot(S, G, lane);
         if (!task_in_bounds(a, S, strip, xa, seg_len, kt, PROD, 1)) continue;
         const int c = strip * S2D_STRIP_OUT - 4;
         const int xb = min(S.nnx, xa + seg_len);

@@ -262,11 +262,11 @@ def test_adjoint_forms_give_the_same_gradient(ctx):
     m = ctx.model(vp, rho, D, D, NB)
     out = {}
     try:
-        for ab in (3, 2, 12, 13, 14):
+        for ab in (3, 2, 12, 13, 14, 15):
             ctx.set_option("adjoint_blocks", ab)
             out[ab] = ctx.gradient([Shot(m, src, rec)], _wave(), adj)
     finally:
         ctx.set_option("adjoint_blocks", 3)
-    for ab in (2, 12, 13, 14):
+    for ab in (2, 12, 13, 14, 15):
         np.testing.assert_array_equal(out[ab].grad_vp, out[3].grad_vp)
         np.testing.assert_array_equal(out[ab].grad_rho, out[3].grad_rho)
