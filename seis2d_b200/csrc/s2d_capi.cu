@@ -223,7 +223,7 @@ int fail(Ctx *c, int code, const char *fmt, ...) {
 // ceil(tasks / resident warps) rounds of the longest task.  Pick the L with
 // the fewest round-columns (longer segments on ties).
 int choose_seg_len(int nnx, long tasks_per_seg, long resident_warps, int halo) {
-    static const int cand[] = {1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16, 12, 8};
+    static const int cand[] = {1024, 768, 512, 384, 256, 192, 128, 96, 64, 48, 32, 24, 16, 12, 8, 6, 4};
     int best = 8;
     double best_cost = 1e300;
     for (int L : cand) {

@@ -206,6 +206,27 @@ def test_launch_shapes_agree(ctx, stages, block, seg_len, order):
     np.testing.assert_array_equal(got, base)
 
 
+@pytest.mark.parametrize("seg_len", [4, 6])
+@pytest.mark.parametrize("variant", [16, 15, 4, 5, 11, 12])
+def test_short_segments_agree(ctx, variant, seg_len):
+    """Segments of 4 and 6 columns (the layout picks them for small single
+    grids: more tasks, fewer columns per task) give the same bits in every
+    kernel family."""
+    from seis2d_b200 import Shot
+    z, c, vp, rho = _golden("layers_endonright_near_nb32")
+    m = ctx.model(vp, rho, c["dx"], c["dz"], c["nb"])
+    shot = [Shot(m, tuple(z["src"]), z["rec"])]
+    base = ctx.forward(shot, _wave(c))[0]
+    try:
+        ctx.set_option("variant", variant)
+        ctx.set_option("seg_len", seg_len)
+        got = ctx.forward(shot, _wave(c))[0]
+    finally:
+        ctx.set_option("seg_len", 0)
+        ctx.set_option("autotune", 1)
+    np.testing.assert_array_equal(got, base)
+
+
 @pytest.mark.parametrize("variant", [0, 11, 20])
 def test_bounded_wait_reports_timeout_and_context_survives(ctx, variant):
     """A wait that never completes (the per-warp bulk-copy pipeline's stage,
