@@ -66,6 +66,10 @@ def lib():
             C.POINTER(_Params), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float, C.c_float, C.c_int,
             C.POINTER(C.c_float), C.POINTER(C.c_float), dp, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp]
         L.orc_gradient.restype = C.c_int
+        L.orc_gradient_seg.argtypes = L.orc_gradient.argtypes + [C.c_int]
+        L.orc_gradient_seg.restype = C.c_int
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_threads.restype = None
         _lib = L
     return _lib
 
@@ -143,11 +147,18 @@ def forward(p: Params, vp: np.ndarray, rho: np.ndarray, src: Sequence[float],
     return seis
 
 
+def set_threads(n: int) -> None:
+    """Threads of the FP64 gradient's loops (same bits for every count)."""
+    lib().orc_set_threads(int(n))
+
+
 def gradient(p: Params, vp: np.ndarray, rho: np.ndarray, src, rec_x, rec_z, adj: Optional[np.ndarray],
-             wavelet: Optional[np.ndarray] = None):
+             wavelet: Optional[np.ndarray] = None, segment: int = 0):
     """FP64 discrete adjoint of the FP64 forward.  Returns a dict with
     grad_vp, grad_rho ([nx][nz]), grad_kappa, grad_bx, grad_bz ([nnx][nnz]),
-    src_adj ([fd_nt]) and seis64 ([nrec][real_nt])."""
+    src_adj ([fd_nt]) and seis64 ([nrec][real_nt]).  ``segment``: checkpoint
+    interval in FD steps (0: every step's products kept); ``adj=None`` runs
+    the forward alone (seis64; the gradients are zero)."""
     vp = np.ascontiguousarray(vp, np.float32)
     rho = np.ascontiguousarray(rho, np.float32)
     gx = np.ascontiguousarray(rec_x, np.float32)
@@ -166,10 +177,10 @@ def gradient(p: Params, vp: np.ndarray, rho: np.ndarray, src, rec_x, rec_z, adj:
     if adj is not None:
         a = np.ascontiguousarray(adj, np.float64)
         assert a.shape == (gx.size, d["real_nt"])
-    rc = lib().orc_gradient(C.byref(p.c()), _fp(vp), _fp(rho), float(src[0]), float(src[1]), gx.size, _fp(gx),
-                            _fp(gz), wp, nw, dpp(a) if a is not None else None,
-                            *(dpp(out[k]) for k in ("grad_vp", "grad_rho", "grad_kappa", "grad_bx", "grad_bz",
-                                                    "src_adj", "seis64")))
+    rc = lib().orc_gradient_seg(C.byref(p.c()), _fp(vp), _fp(rho), float(src[0]), float(src[1]), gx.size,
+                                _fp(gx), _fp(gz), wp, nw, dpp(a) if a is not None else None,
+                                *(dpp(out[k]) for k in ("grad_vp", "grad_rho", "grad_kappa", "grad_bx", "grad_bz",
+                                                        "src_adj", "seis64")), int(segment))
     if rc != 0:
         raise ValueError(f"orc_gradient failed with status {rc}")
     return out

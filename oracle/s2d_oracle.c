@@ -20,6 +20,15 @@
 
 #define ORC_PI 3.141592654 /* CM:9, CK:7 */
 
+/* Threads of the gradient's loops (orc_set_threads).  ORC_PAR_FOR splits a
+ * loop over cells whose updates are independent, or over row blocks of a
+ * scatter whose additions into each cell keep their serial order: the same
+ * bits for every thread count.  One thread runs the loops serially. */
+static int g_threads = 1;
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+#define ORC_PAR_FOR _Pragma("omp parallel for if (g_threads > 1) num_threads(g_threads) schedule(static)")
+#define ORC_ROWS 64 /* rows per block of the x-direction scatters */
+
 /* 4th-order staggered coefficients, CK:9-10.  The reference's macro
  * "-1.0f/24.0f" is a float quotient, so a1 carries float rounding. */
 static const float ORC_A0 = 1.125f;
@@ -610,15 +619,18 @@ bad_pos:
 
 /* out += Gx^T mu, Gx = D-x of CK:201-229 */
 static void gxT_add(const double *mu, double *out, int nnz, int nnx) {
-    for (int i2 = 2; i2 < nnx - 1; i2++)
-        for (int i1 = 0; i1 < nnz; i1++) {
-            size_t id = (size_t)i1 + (size_t)i2 * nnz;
-            double m = mu[id];
-            out[id] += ORC_A0 * m;
-            out[id - nnz] -= ORC_A0 * m;
-            out[id + nnz] += ORC_A1 * m;
-            out[id - 2 * nnz] -= ORC_A1 * m;
-        }
+    const int nblk = (nnz + ORC_ROWS - 1) / ORC_ROWS;
+    ORC_PAR_FOR
+    for (int b = 0; b < nblk; b++)
+        for (int i2 = 2; i2 < nnx - 1; i2++)
+            for (int i1 = b * ORC_ROWS; i1 < nnz && i1 < (b + 1) * ORC_ROWS; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                double m = mu[id];
+                out[id] += ORC_A0 * m;
+                out[id - nnz] -= ORC_A0 * m;
+                out[id + nnz] += ORC_A1 * m;
+                out[id - 2 * nnz] -= ORC_A1 * m;
+            }
     for (int i1 = 0; i1 < nnz; i1++) {
         size_t id = (size_t)i1 + (size_t)1 * nnz;
         out[id] += mu[id];
@@ -630,6 +642,7 @@ static void gxT_add(const double *mu, double *out, int nnz, int nnx) {
 }
 /* out += Gz^T mu, Gz = D-z of CK:231-258 */
 static void gzT_add(const double *mu, double *out, int nnz, int nnx) {
+    ORC_PAR_FOR
     for (int i2 = 0; i2 < nnx; i2++)
         for (int i1 = 2; i1 < nnz - 1; i1++) {
             size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -650,15 +663,18 @@ static void gzT_add(const double *mu, double *out, int nnz, int nnx) {
 }
 /* out += Hx^T mu, Hx = D+x of CK:260-287 */
 static void hxT_add(const double *mu, double *out, int nnz, int nnx) {
-    for (int i2 = 1; i2 < nnx - 2; i2++)
-        for (int i1 = 0; i1 < nnz; i1++) {
-            size_t id = (size_t)i1 + (size_t)i2 * nnz;
-            double m = mu[id];
-            out[id + nnz] += ORC_A0 * m;
-            out[id] -= ORC_A0 * m;
-            out[id + 2 * nnz] += ORC_A1 * m;
-            out[id - nnz] -= ORC_A1 * m;
-        }
+    const int nblk = (nnz + ORC_ROWS - 1) / ORC_ROWS;
+    ORC_PAR_FOR
+    for (int b = 0; b < nblk; b++)
+        for (int i2 = 1; i2 < nnx - 2; i2++)
+            for (int i1 = b * ORC_ROWS; i1 < nnz && i1 < (b + 1) * ORC_ROWS; i1++) {
+                size_t id = (size_t)i1 + (size_t)i2 * nnz;
+                double m = mu[id];
+                out[id + nnz] += ORC_A0 * m;
+                out[id] -= ORC_A0 * m;
+                out[id + 2 * nnz] += ORC_A1 * m;
+                out[id - nnz] -= ORC_A1 * m;
+            }
     for (int i1 = 0; i1 < nnz; i1++) {
         size_t id = (size_t)i1;
         out[id + nnz] += mu[id];
@@ -670,6 +686,7 @@ static void hxT_add(const double *mu, double *out, int nnz, int nnx) {
 }
 /* out += Hz^T mu, Hz = D+z of CK:289-316 */
 static void hzT_add(const double *mu, double *out, int nnz, int nnx) {
+    ORC_PAR_FOR
     for (int i2 = 0; i2 < nnx; i2++)
         for (int i1 = 1; i1 < nnz - 2; i1++) {
             size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -694,6 +711,7 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
     size_t N = (size_t)nnz * nnx;
     memset(d, 0, N * sizeof(double));
     if (which == 0) { /* Gx */
+        ORC_PAR_FOR
         for (int i2 = 2; i2 < nnx - 1; i2++)
             for (int i1 = 0; i1 < nnz; i1++) {
                 size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -706,6 +724,7 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
             d[id] = f[id] - f[id - nnz];
         }
     } else if (which == 1) { /* Gz */
+        ORC_PAR_FOR
         for (int i2 = 0; i2 < nnx; i2++)
             for (int i1 = 2; i1 < nnz - 1; i1++) {
                 size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -718,6 +737,7 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
             d[id] = f[id] - f[id - 1];
         }
     } else if (which == 2) { /* Hx */
+        ORC_PAR_FOR
         for (int i2 = 1; i2 < nnx - 2; i2++)
             for (int i1 = 0; i1 < nnz; i1++) {
                 size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -730,6 +750,7 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
             d[id] = f[id + nnz] - f[id];
         }
     } else { /* Hz */
+        ORC_PAR_FOR
         for (int i2 = 0; i2 < nnx; i2++)
             for (int i1 = 1; i1 < nnz - 2; i1++) {
                 size_t id = (size_t)i1 + (size_t)i2 * nnz;
@@ -749,6 +770,7 @@ static void op_apply(int which, const double *f, double *d, int nnz, int nnx) {
  * edges): d = D f, and out += D^T mu as the scatter of each forward row. */
 static void op8_apply(int which, const double *f, double *d, int nnz, int nnx) {
 #define F8(ix, iz) ((ix) < 0 || (ix) >= nnx || (iz) < 0 || (iz) >= nnz ? 0.0 : f[(size_t)(iz) + (size_t)(ix) * nnz])
+    ORC_PAR_FOR
     for (int ix = 0; ix < nnx; ix++)
         for (int iz = 0; iz < nnz; iz++) {
             float c[4];
@@ -776,8 +798,15 @@ static void op8T_add(int which, const double *mu, double *out, int nnz, int nnx)
         if ((ix) >= 0 && (ix) < nnx && (iz) >= 0 && (iz) < nnz)                  \
             out[(size_t)(iz) + (size_t)(ix) * nnz] += (v);                       \
     } while (0)
-    for (int ix = 0; ix < nnx; ix++)
-        for (int iz = 0; iz < nnz; iz++) {
+    /* x-direction rows scatter across columns: row blocks in parallel, the
+     * columns of a block in order; z-direction rows stay in their column:
+     * columns in parallel */
+    const int xdir = which == 0 || which == 2;
+    const int nblk = xdir ? (nnz + ORC_ROWS - 1) / ORC_ROWS : 1;
+    ORC_PAR_FOR
+    for (int t = 0; t < (xdir ? nblk : nnx); t++)
+    for (int ix = xdir ? 0 : t; ix < (xdir ? nnx : t + 1); ix++)
+        for (int iz = xdir ? t * ORC_ROWS : 0; iz < (xdir ? ((t + 1) * ORC_ROWS < nnz ? (t + 1) * ORC_ROWS : nnz) : nnz); iz++) {
             const double m = mu[(size_t)iz + (size_t)ix * nnz];
             float c[4];
             for (int k = 0; k < 4; k++) {
@@ -803,12 +832,70 @@ static void op8T_add(int which, const double *mu, double *out, int nnz, int nnx)
 #undef ADD8
 }
 
+/* One forward step of the gradient's FP64 scheme (the stages of f64_step,
+ * written with the step's products a, c, g, h kept in the given arrays). */
+typedef struct {
+    int nnz, nnx, o8, isrc, nts, nw;
+    size_t N;
+    const float *damp2a, *damp1a, *damp2b, *damp1b;
+    const double *kw1, *kw2, *bw1, *bw2, *kappa, *w;
+    float fd_dt, dxdz;
+    double *px, *pz, *vx, *vz, *p;
+} gfwd;
+
+static void gfwd_step(const gfwd *s, int kt, double *a, double *c, double *g, double *h) {
+    const int nnz = s->nnz, nnx = s->nnx;
+    double *px = s->px, *pz = s->pz, *vx = s->vx, *vz = s->vz, *p = s->p;
+    if (s->o8) {
+        op8_apply(0, vx, a, nnz, nnx);
+        op8_apply(1, vz, c, nnz, nnx);
+    } else {
+        op_apply(0, vx, a, nnz, nnx);
+        op_apply(1, vz, c, nnz, nnx);
+    }
+    ORC_PAR_FOR
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            px[id] = s->damp2a[ix] * px[id] + s->kw2[id] * a[id];
+            pz[id] = s->damp1a[iz] * pz[id] + s->kw1[id] * c[id];
+        }
+    if (kt <= s->nts)
+        px[s->isrc] = px[s->isrc] + s->fd_dt * (kt < s->nw ? s->w[kt] : 0.0) * s->kappa[s->isrc] / (s->dxdz);
+    ORC_PAR_FOR
+    for (size_t id = 0; id < s->N; id++) p[id] = px[id] + pz[id];
+    if (s->o8) {
+        op8_apply(2, p, g, nnz, nnx);
+        op8_apply(3, p, h, nnz, nnx);
+    } else {
+        op_apply(2, p, g, nnz, nnx);
+        op_apply(3, p, h, nnz, nnx);
+    }
+    ORC_PAR_FOR
+    for (int ix = 0; ix < nnx; ix++)
+        for (int iz = 0; iz < nnz; iz++) {
+            size_t id = (size_t)iz + (size_t)ix * nnz;
+            vx[id] = s->damp2b[ix] * vx[id] + s->bw2[id] * g[id];
+            vz[id] = s->damp1b[iz] * vz[id] + s->bw1[id] * h[id];
+        }
+}
+
 int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                  float sx, float sz, int nrec, const float *gx, const float *gz,
                  const double *wavelet, int nwav, const double *adj,
                  double *grad_vp, double *grad_rho,
                  double *grad_kappa, double *grad_bx, double *grad_bz,
                  double *src_adj, double *seis64) {
+    return orc_gradient_seg(prm, vp, rho, sx, sz, nrec, gx, gz, wavelet, nwav, adj, grad_vp, grad_rho, grad_kappa,
+                            grad_bx, grad_bz, src_adj, seis64, 0);
+}
+
+int orc_gradient_seg(const orc_params *prm, const float *vp, const float *rho,
+                     float sx, float sz, int nrec, const float *gx, const float *gz,
+                     const double *wavelet, int nwav, const double *adj,
+                     double *grad_vp, double *grad_rho,
+                     double *grad_kappa, double *grad_bx, double *grad_bz,
+                     double *src_adj, double *seis64, int segment) {
     if (!prm || !vp || !rho || nrec < 0 || (nrec > 0 && (!gx || !gz))) return -1;
     if (prm->fd_order != 0 && prm->fd_order != 4 && prm->fd_order != 8) return -1;
     const int o8 = prm->fd_order == 8;
@@ -847,45 +934,38 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
             bw1[id] = d.dtdz * bz[id] * damp1b1[iz];
         }
     const float dxdz = prm->dx * prm->dz;
-    /* forward, storing a, c, g, h of every step */
-    double *A = malloc(N * 8 * (size_t)nt), *Cc = malloc(N * 8 * (size_t)nt);
-    double *Gg = malloc(N * 8 * (size_t)nt), *Hh = malloc(N * 8 * (size_t)nt);
+    /* checkpointing: segments of `seg` steps; the products a, c, g, h of one
+     * segment at a time (every step's when there is one segment) and the
+     * state at each segment start; a forward alone keeps neither */
+    const int seg = segment <= 0 || segment >= nt ? nt : segment;
+    const int nseg = (nt + seg - 1) / seg;
+    const size_t keep = adj ? (size_t)seg : 1;
+    double *A = malloc(N * 8 * keep), *Cc = malloc(N * 8 * keep);
+    double *Gg = malloc(N * 8 * keep), *Hh = malloc(N * 8 * keep);
+    double *ck = adj && nseg > 1 ? malloc(N * 8 * 4 * (size_t)nseg) : NULL;
     double *px = calloc(N, 8), *pz = calloc(N, 8), *vx = calloc(N, 8), *vz = calloc(N, 8), *p = calloc(N, 8);
-    if (!A || !Cc || !Gg || !Hh) return -4;
-    for (int kt = 0; kt < nt; kt++) {
-        double *a = A + N * kt, *c = Cc + N * kt, *g = Gg + N * kt, *h = Hh + N * kt;
-        if (o8) {
-            op8_apply(0, vx, a, nnz, nnx);
-            op8_apply(1, vz, c, nnz, nnx);
-        } else {
-            op_apply(0, vx, a, nnz, nnx);
-            op_apply(1, vz, c, nnz, nnx);
+    if (!A || !Cc || !Gg || !Hh || (adj && nseg > 1 && !ck)) return -4;
+    gfwd fs = {nnz, nnx, o8, isrc, d.nts, nw, N, damp2a, damp1a, damp2b, damp1b, kw1, kw2, bw1, bw2, kappa, w,
+               prm->fd_dt, dxdz, px, pz, vx, vz, p};
+    /* forward sweep: the state at each segment start, the traces, and the
+     * last segment's products */
+    for (int j = 0; j < nseg; j++) {
+        const int k0 = j * seg, k1 = k0 + seg < nt ? k0 + seg : nt;
+        if (ck) {
+            double *st = ck + N * 4 * (size_t)j;
+            memcpy(st, px, N * 8);
+            memcpy(st + N, pz, N * 8);
+            memcpy(st + 2 * N, vx, N * 8);
+            memcpy(st + 3 * N, vz, N * 8);
         }
-        for (int ix = 0; ix < nnx; ix++)
-            for (int iz = 0; iz < nnz; iz++) {
-                size_t id = (size_t)iz + (size_t)ix * nnz;
-                px[id] = damp2a[ix] * px[id] + kw2[id] * a[id];
-                pz[id] = damp1a[iz] * pz[id] + kw1[id] * c[id];
+        for (int kt = k0; kt < k1; kt++) {
+            const size_t sl = adj && j == nseg - 1 ? (size_t)(kt - k0) : 0;
+            gfwd_step(&fs, kt, A + N * sl, Cc + N * sl, Gg + N * sl, Hh + N * sl);
+            if (seis64 && (kt + 1) % d.dt_factor == 0) {
+                int it = (kt + 1) / d.dt_factor - 1;
+                if (it < d.real_nt)
+                    for (int r = 0; r < nrec; r++) seis64[(size_t)r * d.real_nt + it] = p[gcell[r]];
             }
-        if (kt <= d.nts) px[isrc] = px[isrc] + prm->fd_dt * (kt < nw ? w[kt] : 0.0) * kappa[isrc] / (dxdz);
-        for (size_t id = 0; id < N; id++) p[id] = px[id] + pz[id];
-        if (o8) {
-            op8_apply(2, p, g, nnz, nnx);
-            op8_apply(3, p, h, nnz, nnx);
-        } else {
-            op_apply(2, p, g, nnz, nnx);
-            op_apply(3, p, h, nnz, nnx);
-        }
-        for (int ix = 0; ix < nnx; ix++)
-            for (int iz = 0; iz < nnz; iz++) {
-                size_t id = (size_t)iz + (size_t)ix * nnz;
-                vx[id] = damp2b[ix] * vx[id] + bw2[id] * g[id];
-                vz[id] = damp1b[iz] * vz[id] + bw1[id] * h[id];
-            }
-        if (seis64 && (kt + 1) % d.dt_factor == 0) {
-            int it = (kt + 1) / d.dt_factor - 1;
-            if (it < d.real_nt)
-                for (int r = 0; r < nrec; r++) seis64[(size_t)r * d.real_nt + it] = p[gcell[r]];
         }
     }
     /* adjoint, backwards in time */
@@ -894,9 +974,26 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
     double *ma = malloc(N * 8), *mc = malloc(N * 8), *nvx = malloc(N * 8), *nvz = malloc(N * 8);
     double *gk = calloc(N, 8), *gbx = calloc(N, 8), *gbz = calloc(N, 8);
     double gk_src = 0.0;
-    for (int kt = nt - 1; kt >= 0; kt--) {
-        double *a = A + N * kt, *c = Cc + N * kt, *g = Gg + N * kt, *h = Hh + N * kt;
+    if (!adj && src_adj) memset(src_adj, 0, (size_t)nt * sizeof(double));
+    for (int j = nseg - 1; j >= 0 && adj; j--) {
+        const int k0 = j * seg, k1 = k0 + seg < nt ? k0 + seg : nt;
+        if (j < nseg - 1) {
+            /* recompute the segment's products from its checkpoint */
+            const double *st = ck + N * 4 * (size_t)j;
+            memcpy(px, st, N * 8);
+            memcpy(pz, st + N, N * 8);
+            memcpy(vx, st + 2 * N, N * 8);
+            memcpy(vz, st + 3 * N, N * 8);
+            for (int kt = k0; kt < k1; kt++) {
+                const size_t sl = (size_t)(kt - k0);
+                gfwd_step(&fs, kt, A + N * sl, Cc + N * sl, Gg + N * sl, Hh + N * sl);
+            }
+        }
+    for (int kt = k1 - 1; kt >= k0; kt--) {
+        double *a = A + N * (size_t)(kt - k0), *c = Cc + N * (size_t)(kt - k0);
+        double *g = Gg + N * (size_t)(kt - k0), *h = Hh + N * (size_t)(kt - k0);
         /* vx' = damp2b vx + bw2 g ; vz' = damp1b vz + bw1 h */
+        ORC_PAR_FOR
         for (int ix = 0; ix < nnx; ix++)
             for (int iz = 0; iz < nnz; iz++) {
                 size_t id = (size_t)iz + (size_t)ix * nnz;
@@ -922,6 +1019,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
                 for (int r = 0; r < nrec; r++) q[gcell[r]] += adj[(size_t)r * d.real_nt + it];
         }
         /* p' = px' + pz' */
+        ORC_PAR_FOR
         for (size_t id = 0; id < N; id++) {
             mPX[id] = mpx[id] + q[id];
             mPZ[id] = mpz[id] + q[id];
@@ -930,6 +1028,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
         if (src_adj) src_adj[kt] = mPX[isrc];
         if (kt <= d.nts) gk_src += mPX[isrc] * (prm->fd_dt * (kt < nw ? w[kt] : 0.0) / (dxdz));
         /* px' = damp2a px + kw2 a ; pz' = damp1a pz + kw1 c */
+        ORC_PAR_FOR
         for (int ix = 0; ix < nnx; ix++)
             for (int iz = 0; iz < nnz; iz++) {
                 size_t id = (size_t)iz + (size_t)ix * nnz;
@@ -949,6 +1048,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
         }
         memcpy(mvx, nvx, N * 8);
         memcpy(mvz, nvz, N * 8);
+    }
     }
     gk[isrc] += gk_src;
     /* with a free surface kappa is held at 0 on rows 0..nb: not a function of
@@ -993,7 +1093,7 @@ int orc_gradient(const orc_params *prm, const float *vp, const float *rho,
             if (grad_rho) grad_rho[m] += v * v * gk[id] + (r > 0 ? -gb[id] / (r * r) : 0.0);
         }
     free(gb);
-    free(A); free(Cc); free(Gg); free(Hh); free(px); free(pz); free(vx); free(vz); free(p);
+    free(A); free(Cc); free(Gg); free(Hh); free(ck); free(px); free(pz); free(vx); free(vz); free(p);
     free(mpx); free(mpz); free(mvx); free(mvz); free(mg); free(mh); free(q); free(mPX); free(mPZ);
     free(ma); free(mc); free(nvx); free(nvz); free(gk); free(gbx); free(gbz);
     free(kw1); free(kw2); free(bw1); free(bw2); free(gcell); free(w);

@@ -102,6 +102,28 @@ int orc_gradient(const orc_params *p, const float *vp, const float *rho,
                  double *grad_kappa, double *grad_bx, double *grad_bz,
                  double *src_adj, double *seis64);
 
+/*
+ * orc_gradient with checkpointing: the forward keeps its state every
+ * `segment` steps and each segment's step products are recomputed from its
+ * checkpoint on the way back (segment <= 0 or >= fd_nt: one segment, every
+ * product of the run kept).  Bit-identical to orc_gradient for every segment
+ * length.  adj == NULL runs the forward alone (seis64) and keeps nothing.
+ */
+int orc_gradient_seg(const orc_params *p, const float *vp, const float *rho,
+                     float sx, float sz, int nrec, const float *gx, const float *gz,
+                     const double *wavelet, int nwav, const double *adj,
+                     double *grad_vp, double *grad_rho,
+                     double *grad_kappa, double *grad_bx, double *grad_bz,
+                     double *src_adj, double *seis64, int segment);
+
+/*
+ * Threads of orc_gradient / orc_gradient_seg (OpenMP, default 1).  Each
+ * parallel loop splits cells whose updates do not depend on one another and
+ * keeps the order of the additions into every cell, so the results are the
+ * same bits for every thread count.
+ */
+void orc_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif
