@@ -286,7 +286,7 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     ms = ctx.model(start, rho, 10.0, 10.0, 50, fd_order=fd_order)
     shots = [Shot(ms, s_, rec) for s_ in src]
     fbuf = torch.zeros_like(dobs)
-    ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 64 steps) outside the timing
+    ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 80 steps) outside the timing
     tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
     gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
     grho = torch.zeros_like(gvp)
@@ -325,14 +325,14 @@ def extra_legs(device):
         st = derive_steps(wave)
         buf = torch.zeros(rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
         shots = [Shot(m, src[0], rec)]
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 64 steps)
+        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 80 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         l1 = ctx.last_stats
         cells = m.padded_cells * st["fd_nt"]
         out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
                      "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": ctx.last_stats.alg_bytes / t / 1e9 / peak,
                      "note": "whole job ~37 MB of state: L2-resident",
-                     "launch": {"variant": l1.variant, "seg_len": l1.seg_len}}
+                     "launch": {"variant": l1.variant, "seg_len": l1.seg_len, "task_order": l1.task_order}}
         m.release()
         # c3: salt 3201x1201, d 7.62, nb 50, 20 Hz, dt 0.6 ms, nt 10000, 1 shot; 1000 of the 10000 steps
         vp, rho = salt_model()
@@ -351,7 +351,7 @@ def extra_legs(device):
         l3 = ctx.last_stats
         out["c3"] = {"workload": "3201x1201 salt (seeded), d 7.62, nb 50, 1 shot, 1000 of 10000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (m.padded_cells * st["fd_nt"]),
-                     "roofline_frac": frac, "launch": {"variant": l3.variant, "seg_len": l3.seg_len}}
+                     "roofline_frac": frac, "launch": {"variant": l3.variant, "seg_len": l3.seg_len, "task_order": l3.task_order}}
         m.release()
         # c4: 48 shots on three layered models of uneven size, one launch sequence; 300 of 3000 steps
         wave = Wave(2.3996, 0.0008, 0.0008, 15.0)
@@ -367,7 +367,7 @@ def extra_legs(device):
             cells_step += 16 * mm.padded_cells
             total_rec += 16 * rec.shape[0]
         buf = torch.zeros(total_rec * st["real_nt"], dtype=torch.float32, device="cuda")
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 64 steps)
+        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 80 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
@@ -379,7 +379,7 @@ def extra_legs(device):
                                  "one launch per step for all; 300 of 3000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (cells_step / 48 * st["fd_nt"]),
                      "plain_gcells_per_s": prate, "roofline_frac": frac,
-                     "launch": {"variant": l4.variant, "seg_len": l4.seg_len}}
+                     "launch": {"variant": l4.variant, "seg_len": l4.seg_len, "task_order": l4.task_order}}
         for mm in models:
             mm.release()
         # the 8th-order operator ("Order of FD Operator" : "8") on the 5000x5000
@@ -400,7 +400,7 @@ def extra_legs(device):
             out["c2_order8"] = {"workload": "5000x5000 two-layer, nb 60, 8th-order operator, 16 shots x 5000 "
                                             "receivers; 200 of 4000 steps",
                                 "gcells_per_s": rate, "roofline_frac": l8.alg_bytes / t / 1e9 / peak,
-                                "launch": {"variant": l8.variant, "seg_len": l8.seg_len}}
+                                "launch": {"variant": l8.variant, "seg_len": l8.seg_len, "task_order": l8.task_order}}
             m.release()
             del buf
         except Exception as exc:  # a failed extra leg must not cost the main line
@@ -606,7 +606,7 @@ def main():
         st = ctx.last_stats
         if tune is None or st.autotuned:
             tune = {"variant": st.variant, "block": st.block, "stages": st.stages, "seg_len": st.seg_len,
-                    "autotuned_in_warmup": bool(st.autotuned)}
+                    "task_order": st.task_order, "autotuned_in_warmup": bool(st.autotuned)}
     barrier()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()

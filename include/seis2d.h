@@ -131,6 +131,7 @@ typedef struct {
     double adjoint_ms;       /* s2d_gradient: the adjoint steps; loop_ms minus
                                 the three is set-up, adjoint source and
                                 finalisation                                   */
+    int task_order;          /* task order of the time loop ("task_order")    */
 } s2d_stats;
 
 /* ---- library / context ------------------------------------------------ */
@@ -151,13 +152,15 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 64 steps
- *                 spends 32 of them on 7 candidate configurations (variants
- *                 4, 16, 15, 2, 5, 11, 12), one untimed and three timed launches
- *                 each, in rounds (the results do not change: every candidate
- *                 computes the same bits), times them with events and keeps the
- *                 fastest per FD step for that shape in the context; runs that
- *                 do not tune (shorter calls, S2D_PLAIN) use variant 16.
+ *                 shape (models, grids, shot counts) with at least 80 steps
+ *                 spends 40 of them on 9 candidate configurations (variants
+ *                 4, 16, 15, 2, 5, 11, 12 in task order 1, and 16 and 15 in
+ *                 task order 0, unless "task_order" was set), one untimed and
+ *                 three timed launches each, in rounds (the results do not
+ *                 change: every candidate computes the same bits), times them
+ *                 with events and keeps the fastest per FD step for that shape
+ *                 in the context; runs that do not tune (shorter calls,
+ *                 S2D_PLAIN) use variant 16.
  *                 0: use "variant", "block" and "stages".
  *                 Setting any of those three turns autotuning off.
  *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline
@@ -182,8 +185,10 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *                 at 3 blocks per SM (default), 8 the same at 2, 9 windows in
  *                 shared memory at 4 (each setting applies to its own order)
  *   "block"       threads per block: 32, 64, 96 or 128 (default 128)
- *   "task_order"  0: consecutive warps take the shots of one tile;
- *                 1: consecutive warps take adjacent strips of one shot (default)
+ *   "task_order"  0: consecutive warps take the shots of one tile (the four
+ *                 warps of a block share its kappa, bx, bz through L1);
+ *                 1: consecutive warps take adjacent strips of one shot (the
+ *                 default); setting it keeps the autotuner off this choice
  *   "stages"      bulk-copy ring depth per warp, 2..16 (default 3)
  *   "seg_len"     columns per x-segment of a warp task, 0 = automatic
  *   "spin_limit"  polls of a pipeline barrier before the wait gives up and the

@@ -72,7 +72,7 @@ class Stats(C.Structure):
                 ("kernel_launches", C.c_int), ("graph_used", C.c_int), ("grad_segment", C.c_int),
                 ("variant", C.c_int), ("block", C.c_int), ("stages", C.c_int), ("seg_len", C.c_int),
                 ("autotuned", C.c_int), ("alg_bytes", C.c_double), ("sweep_ms", C.c_double),
-                ("recompute_ms", C.c_double), ("adjoint_ms", C.c_double)]
+                ("recompute_ms", C.c_double), ("adjoint_ms", C.c_double), ("task_order", C.c_int)]
 
 
 # Every symbol include/seis2d.h declares, with its ctypes signature.

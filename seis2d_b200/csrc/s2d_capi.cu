@@ -146,6 +146,7 @@ struct LaunchCfg {
     int stages = 3;       // bulk-copy ring depth per warp (bulk-copy variants)
     size_t smem = 0;
     int grid = 0;
+    int order = -1;       // task order (StepArgs::task_order); -1: the context's option
 };
 
 struct Ctx {
@@ -162,6 +163,7 @@ struct Ctx {
     int opt_spin_limit = 1 << 20;
     int opt_fault_iter = -1;  // test knob, see s2d_set_option
     int opt_order = 1;        // task order (StepArgs::task_order)
+    bool order_fixed = false; // task_order set by the caller: the autotuner keeps it
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
@@ -178,7 +180,7 @@ struct Ctx {
     std::map<std::vector<long>, cudaGraphExec_t> graphs;
     std::map<std::vector<long>, cudaGraphExec_t> adj_graphs;  // by (step count, grid)
     // autotuner results: batch shape -> (variant, block, stages)
-    std::map<std::vector<long>, std::array<int, 3>> tuned;
+    std::map<std::vector<long>, std::array<int, 4>> tuned;  // variant, block, stages, task order
     ~Ctx() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
         for (auto &kv : adj_graphs) cudaGraphExecDestroy(kv.second);
@@ -326,7 +328,9 @@ int base_config(Ctx *c, const Batch &b, LaunchCfg *out, bool *tuned = nullptr) {
     auto it = c->tuned.find(tune_key(c, b));
     if (it != c->tuned.end()) {
         if (tuned) *tuned = true;
-        return launch_config(c, b.max_tasks, out, it->second[0], it->second[1], it->second[2]);
+        int e = launch_config(c, b.max_tasks, out, it->second[0], it->second[1], it->second[2]);
+        out->order = c->order_fixed ? -1 : it->second[3];
+        return e;
     }
     const LaunchCfg d;
     return launch_config(c, b.max_tasks, out, b.order8 ? kVariantO8 : d.variant, d.block, b.order8 ? 0 : d.stages);
@@ -474,7 +478,7 @@ int run_loop(Ctx *c, Batch &b, const LaunchCfg &lc, StepArgs args, int kt_begin,
     args.err = c->dev_err.as<int>();
     args.spin_limit = c->opt_spin_limit;
     args.fault_iter = c->opt_fault_iter;
-    args.task_order = c->opt_order;
+    args.task_order = lc.order >= 0 ? lc.order : c->opt_order;
     StepArgs *args_d = c->args_d.as<StepArgs>();
     if (lc.variant == kVariantPersist) {
         // chunks of graph_chunk steps, one cooperative launch each (not
@@ -825,20 +829,25 @@ int check_device_error(Ctx *c) {
 
 }  // namespace
 
-// Candidate launch configurations of the autotuner: (variant, block, stages).
-constexpr int kTuneCandidates[][3] = {
-    {kVariantLdg128, 128, 0}, {kVariantLdgPf4, 128, 0}, {kVariantLdgPf, 128, 0},      {kVariantBulk128, 128, 3},
-    {kVariantTs2, 128, 0},    {kVariantTma, kTmaThreads, 0}, {kVariantAsync, 128, 0},
+// Candidate launch configurations of the autotuner: (variant, block, stages,
+// task order).  Task order 1 runs adjacent strips of one shot on the warps
+// of a block; order 0 gives a block's warps the same strip and segment of
+// consecutive shots, which then share the segment's kappa, bx, bz through
+// the SM's L1 (the tasks of one launch are the same either way).
+constexpr int kTuneCandidates[][4] = {
+    {kVariantLdg128, 128, 0, 1}, {kVariantLdgPf4, 128, 0, 1}, {kVariantLdgPf, 128, 0, 1},
+    {kVariantBulk128, 128, 3, 1}, {kVariantTs2, 128, 0, 1},    {kVariantTma, kTmaThreads, 0, 1},
+    {kVariantAsync, 128, 0, 1},   {kVariantLdgPf4, 128, 0, 0}, {kVariantLdgPf, 128, 0, 0},
 };
 constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]));
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
 // SM (168 registers) and at 2 (224 registers, no spills), and the
 // shared-memory-window kernel at 4 (128 registers).
-constexpr int kTuneCandidatesO8[][3] = {{kVariantO8, 128, 0}, {kVariantO8r, 128, 0}, {kVariantO8s, 128, 0}};
+constexpr int kTuneCandidatesO8[][4] = {{kVariantO8, 128, 0, 1}, {kVariantO8r, 128, 0, 1}, {kVariantO8s, 128, 0, 1}};
 constexpr int kNumTuneCandidatesO8 = (int)(sizeof(kTuneCandidatesO8) / sizeof(kTuneCandidatesO8[0]));
 constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
 // FD steps the trials take (a two-step candidate advances two per launch).
-constexpr int tune_steps(const int (*cand)[3], int n) {
+constexpr int tune_steps(const int (*cand)[4], int n) {
     int steps = 0;
     for (int i = 0; i < n; ++i) steps += (kTuneWarm + kTuneTimed) * steps_per_launch(cand[i][0]);
     return steps;
@@ -868,7 +877,7 @@ int plain_tasks(const Batch &b, int s) {
 // candidate with the lowest median time per FD step is cached for the batch's
 // shape and returned, its segment layout in place.
 int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best) {
-    const int (*const cands)[3] = b.order8 ? kTuneCandidatesO8 : kTuneCandidates;
+    const int (*const cands)[4] = b.order8 ? kTuneCandidatesO8 : kTuneCandidates;
     const int ncand = b.order8 ? kNumTuneCandidatesO8 : kNumTuneCandidates;
     std::vector<cudaEvent_t> ev(2 * kTuneTimed * ncand, nullptr);
     for (auto &e : ev) {
@@ -888,6 +897,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
         const int *k = cands[i];
         if (launch_config(c, 1L << 40, &full[i], k[0], k[1], k[2]) == S2D_OK) {
             ok[i] = true;
+            full[i].order = c->order_fixed ? -1 : k[3];
         } else {
             if (i == 0) {
                 release();
@@ -912,6 +922,7 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
                 release();
                 return e;
             }
+            lc.order = full[i].order;
             cfg[i] = lc;
             a.total_tasks = batch_tasks(b);
             const int spl = steps_per_launch(lc.variant);
@@ -944,9 +955,10 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
     release();
     CK(ce);
     const int *k = cands[pick];
-    c->tuned[tune_key(c, b)] = {k[0], k[1], k[2]};
+    c->tuned[tune_key(c, b)] = {k[0], k[1], k[2], full[pick].order};
     int e = layout_groups(c, b, cfg[pick]);
     if (!e) e = launch_config(c, b.max_tasks, best, k[0], k[1], k[2]);
+    best->order = full[pick].order;
     return e;
 }
 
@@ -1017,6 +1029,7 @@ int s2d_set_option(void *ctx, const char *key, long value) {
     } else if (k == "task_order") {
         if (value != 0 && value != 1) return fail(c, S2D_ERR_ARG, "task_order must be 0 or 1");
         c->opt_order = (int)value;
+        c->order_fixed = true;
     } else if (k == "inject_wait_fault") {
         c->opt_fault_iter = value < 0 ? -1 : (int)value;
     } else {
@@ -1187,9 +1200,11 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     LaunchCfg lc;
     {
         int e = base_config(c, b, &lc, &tuned);
+        const int order = lc.order;
         if (!e) e = layout_groups(c, b, lc);
         if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
         if (e) return e;
+        lc.order = order;
     }
     CK(cudaEventRecord(c->ev0, c->stream));
     StepArgs a{};
@@ -1281,6 +1296,7 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
         stats->graph_used = graph_used ? 1 : 0;
         stats->grad_segment = 0;
         stats->sweep_ms = stats->recompute_ms = stats->adjoint_ms = 0;
+        stats->task_order = lc.order >= 0 ? lc.order : c->opt_order;
         stats->variant = lc.variant;
         stats->block = lc.block;
         stats->stages = lc.stages;
@@ -1543,6 +1559,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     const int prod_variant = b.order8 ? kVariantO8Products : c->opt_prod_variant;
     {
         int e = base_config(c, b, &lc_fwd);
+        const int order = lc_fwd.order;
         // the gradient keeps every step's state (checkpoints at kt parity):
         // one step per launch
         if (!e && steps_per_launch(lc_fwd.variant) != 1)
@@ -1551,6 +1568,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
         if (!e) e = launch_config(c, b.max_tasks, &lc_fwd, lc_fwd.variant, lc_fwd.block, lc_fwd.stages);
         if (!e) e = launch_config(c, b.max_tasks, &lc_prod, prod_variant, 128, 0);
         if (e) return e;
+        lc_fwd.order = steps_per_launch(lc_fwd.variant) == 1 ? order : -1;
     }
     StepArgs fa{};
     fa.shots = b.shots_d.as<ShotDev>();
@@ -1772,6 +1790,7 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
             CK(cudaEventElapsedTime(&t, c->phase_ev[g.marks[i].second], end));
             ph[g.marks[i].first] += t;
         }
+        stats->task_order = lc_fwd.order >= 0 ? lc_fwd.order : c->opt_order;
         stats->sweep_ms = ph[kPhaseSweep];
         stats->recompute_ms = ph[kPhaseRecompute];
         stats->adjoint_ms = ph[kPhaseAdjoint];

@@ -336,9 +336,9 @@ def test_variants_compute_the_same_bits(ctx):
 
 
 def test_autotuner_tunes_once_per_shape_and_keeps_the_bits():
-    """A fresh context tunes on the first run of a batch shape (28 of its
-    steps), reuses the result for the next run of that shape, and the traces
-    equal those of a fixed configuration."""
+    """A fresh context tunes on the first run of a batch shape (40 of its
+    steps, variant and task order), reuses the result for the next run of
+    that shape, and the traces equal those of a fixed configuration."""
     from seis2d_b200 import Context
     c = Context(0)
     try:
@@ -353,8 +353,9 @@ def test_autotuner_tunes_once_per_shape_and_keeps_the_bits():
     finally:
         c.close()
     assert s1.autotuned == 1 and s2.autotuned == 0 and s3.autotuned == 0
-    assert (s1.variant, s1.block, s1.stages) == (s2.variant, s2.block, s2.stages)
+    assert (s1.variant, s1.block, s1.stages, s1.task_order) == (s2.variant, s2.block, s2.stages, s2.task_order)
     assert s1.variant in (2, 4, 5, 11, 12, 15, 16) and s3.variant == 1
+    assert s1.task_order in (0, 1) and (s1.task_order == 1 or s1.variant in (15, 16))
     for a, b, f in zip(first, again, fixed):
         np.testing.assert_array_equal(a, f)
         np.testing.assert_array_equal(b, f)
