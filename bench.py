@@ -528,6 +528,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the c1/c3/c4/c5 legs")
     ap.add_argument("--variant", type=int, default=-1,
                     help="force a step-kernel variant (s2d_set_option 'variant'); default: autotuned")
+    ap.add_argument("--task-order", type=int, default=-1, choices=[-1, 0, 1],
+                    help="force the task order (s2d_set_option 'task_order'); default: autotuned")
     ap.add_argument("--leg", default="main", choices=["main", "gradient"],
                     help="gradient: only the FWI gradient leg (--shots shots, --grad-time seconds)")
     ap.add_argument("--grad-time", type=float, default=3.0, help="record length of the gradient leg (s)")
@@ -546,6 +548,8 @@ def main():
             ctx.set_option("grad_segment", args.grad_segment)
             if args.variant >= 0:
                 ctx.set_option("variant", args.variant)
+            if args.task_order >= 0:
+                ctx.set_option("task_order", args.task_order)
             if args.products_variant:
                 ctx.set_option("products_variant", args.products_variant)
             if args.adjoint_blocks:
@@ -591,6 +595,8 @@ def main():
     ctx = Context(local)
     if args.variant >= 0:
         ctx.set_option("variant", args.variant)
+    if args.task_order >= 0:
+        ctx.set_option("task_order", args.task_order)
     m = ctx.model(vp, rho, w["d"], w["d"], w["nb"], fd_order=args.fd_order)
     shots = [Shot(m, s, rec) for s in src]
     nrec_tot = nshots * rec.shape[0]

@@ -53,7 +53,7 @@ def test_roofline_traffic_and_minimal_bytes():
     import bench
     t2, t64 = bench.traffic_per_launch("c2", 2), bench.traffic_per_launch("c2", 64)
     assert t2 and t64 and t64["bytes"] > 30 * t2["bytes"] / 2 * 0.9
-    assert abs(t2["bytes"] - 1.626e9) < 0.01e9  # the measured 2-shot launch
+    assert abs(t2["bytes"] - 1.622e9) < 0.01e9  # the measured 2-shot launch
     for n in (1, 64):
         b = bench.dram_minimal_bytes(bench.WORKLOADS["c2"], n)
         assert 24.0 + 12.0 / n <= b <= 32.0 + 12.0 / n
