@@ -373,8 +373,8 @@ def extra_legs(device):
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         l4 = ctx.last_stats
         ctx.forward(shots, wave, kt_count=60, out=buf, plain=True)  # warm-up of the plain launch sequence
-        tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=60, out=buf, plain=True, sync=False))
-        prate = cells_step * 60 / tp / 1e9
+        tp, _ = _timed(lambda: ctx.forward(shots, wave, kt_count=300, out=buf, plain=True, sync=False))
+        prate = cells_step * 300 / tp / 1e9
         out["c4"] = {"workload": "48 shots on 601x301 / 1201x601 / 2401x801 layered models (16 each), nb 50, "
                                  "one launch per step for all; 300 of 3000 steps",
                      "gcells_per_s": rate, "shots_per_s": rate * 1e9 / (cells_step / 48 * st["fd_nt"]),

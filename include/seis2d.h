@@ -205,13 +205,13 @@ S2D_API const char *s2d_last_error(const void *ctx);
  *   "products_variant" s2d_gradient's forward recompute that keeps the step
  *                 derivatives: 3 plain loads, 19 plain loads with the next
  *                 column prefetched (default)
- *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 (default) or 4
- *                 blocks of 128 threads per SM, or 12: 2 blocks per SM with
- *                 the next column's loads issued before a column is computed,
- *                 or 13 / 14: 3 / 2 blocks per SM with the column inputs
- *                 copied into shared memory (cp.async) 1 / 2 columns ahead,
- *                 or 15: 3 blocks per SM with the per-shot inputs copied
- *                 2 columns ahead; every form computes the same bits
+ *   "adjoint_blocks" s2d_gradient adjoint kernel built for 2, 3 or 4 blocks
+ *                 of 128 threads per SM, or 12: 2 blocks per SM with the next
+ *                 column's loads issued before a column is computed, or
+ *                 13 (default) / 14: 3 / 2 blocks per SM with the column
+ *                 inputs copied into shared memory (cp.async) 1 / 2 columns
+ *                 ahead, or 15: 3 blocks per SM with the per-shot inputs
+ *                 copied 2 columns ahead; every form computes the same bits
  *   "grad_segment" s2d_gradient checkpoint interval in FD steps, 0 = the
  *                 longest that fits in free device memory (default)
  *   "inject_wait_fault"  test knob: >= 0 makes every warp skip the copies of

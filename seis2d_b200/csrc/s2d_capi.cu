@@ -167,7 +167,7 @@ struct Ctx {
     int opt_grad_segment = 0; // gradient checkpoint interval, 0 = from free memory
     int opt_graph_chunk = 64; // FD steps per captured graph
     int opt_fast_rows = 1;    // 0: every strip takes the general row path
-    int opt_adj_minb = 3;     // adjoint kernel compiled for 2, 3 or 4 blocks per SM
+    int opt_adj_minb = 13;    // adjoint kernel build ("adjoint_blocks"): 3 blocks per SM, inputs by cp.async
     int opt_adj8_form = 0;    // 8th-order adjoint: 0 streaming pass, 1 two cell-parallel passes
     int opt_prod_variant = kVariantLdgPfProducts;  // s2d_gradient's product-writing forward (4th order)
     int last_segment = 0;     // interval the last gradient call used

@@ -250,10 +250,10 @@ def test_products_variants_give_the_same_gradient(ctx):
 
 
 def test_adjoint_forms_give_the_same_gradient(ctx):
-    """The adjoint kernel's builds (3 blocks per SM, the default; 2; 2 with
-    the next column prefetched; 3 and 2 with the column inputs copied into
-    shared memory ahead) share its arithmetic: one shot's gradient is the
-    same bit for bit."""
+    """The adjoint kernel's builds (3 blocks per SM; 2; 2 with the next
+    column prefetched; 3 and 2 with the column inputs copied into shared
+    memory ahead, the first the default) share its arithmetic: one shot's
+    gradient is the same bit for bit."""
     from seis2d_b200 import Shot
     vp, rho = _model(47)
     src, rec = _geom(290.0)
@@ -266,7 +266,7 @@ def test_adjoint_forms_give_the_same_gradient(ctx):
             ctx.set_option("adjoint_blocks", ab)
             out[ab] = ctx.gradient([Shot(m, src, rec)], _wave(), adj)
     finally:
-        ctx.set_option("adjoint_blocks", 3)
+        ctx.set_option("adjoint_blocks", 13)
     for ab in (2, 12, 13, 14, 15):
         np.testing.assert_array_equal(out[ab].grad_vp, out[3].grad_vp)
         np.testing.assert_array_equal(out[ab].grad_rho, out[3].grad_rho)
