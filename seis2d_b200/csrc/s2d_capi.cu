@@ -843,7 +843,8 @@ constexpr int kNumTuneCandidates = (int)(sizeof(kTuneCandidates) / sizeof(kTuneC
 // Candidates of 8th-order batches: the register-window kernel at 3 blocks per
 // SM (168 registers) and at 2 (224 registers, no spills), and the
 // shared-memory-window kernel at 4 (128 registers).
-constexpr int kTuneCandidatesO8[][4] = {{kVariantO8, 128, 0, 1}, {kVariantO8r, 128, 0, 1}, {kVariantO8s, 128, 0, 1}};
+constexpr int kTuneCandidatesO8[][4] = {
+    {kVariantO8, 128, 0, 1}, {kVariantO8r, 128, 0, 1}, {kVariantO8s, 128, 0, 1}, {kVariantO8, 128, 0, 0}};
 constexpr int kNumTuneCandidatesO8 = (int)(sizeof(kTuneCandidatesO8) / sizeof(kTuneCandidatesO8[0]));
 constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
 // FD steps the trials take (a two-step candidate advances two per launch).
@@ -1657,6 +1658,9 @@ extern "C" int s2d_gradient(void *ctx, const s2d_shot *shots, int nshots, const 
     }
     // ---- backward over the segments ----
     StepArgs aa = fa;
+    // the adjoint's warps of a block take one tile of consecutive shots (task
+    // order 0): measured 1.5% faster than order 1 on the c5 gradient
+    aa.task_order = 0;
     aa.shots = adj_table.as<ShotDev>();
     aa.err = c->dev_err.as<int>();
     for (int j = nseg - 1; j >= 0; --j) {
