@@ -1119,6 +1119,9 @@ int s2d_model_create(void *ctx, int nx, int nz, float dx, float dz, int nb, cons
     if (8 * m->field_elems >= (size_t)1 << 31)
         return fail(c, S2D_ERR_ARG, "padded grid %d x %d is too large (8 fields of %zu cells exceed 2^31)", m->nnx,
                     m->nnz, m->field_elems);
+    // the per-cell set-up and gradient kernels put one padded column per grid row
+    if (m->nnx > 65535)
+        return fail(c, S2D_ERR_ARG, "padded grid has %d columns; at most 65535 are supported", m->nnx);
     const size_t raw = (size_t)nx * nz * sizeof(float);
     CK(m->vp.alloc(raw));
     CK(m->rho.alloc(raw));

@@ -73,3 +73,21 @@ def test_grid_beyond_the_addressing_limit_is_refused():
         assert b"too large" in L.lib().s2d_last_error(c._h)
     finally:
         c.close()
+
+
+def test_grid_wider_than_the_launch_limit_is_refused():
+    """A padded grid of more than 65535 columns (70000 x 4 cells, whose state
+    is well inside the addressing limit) is refused with S2D_ERR_ARG and a
+    message naming the limit, before any copy or allocation."""
+    from seis2d_b200 import Context
+    from seis2d_b200 import _lib as L
+    c = Context(0)
+    try:
+        tiny = np.zeros(4, np.float32)
+        mid = C.c_int(-1)
+        rc = L.lib().s2d_model_create(c._h, 70000, 4, 5.0, 5.0, 60, C.c_void_p(tiny.ctypes.data),
+                                      C.c_void_p(tiny.ctypes.data), 0, C.byref(mid))
+        assert rc == L.S2D_ERR_ARG and mid.value == -1
+        assert b"65535" in L.lib().s2d_last_error(c._h)
+    finally:
+        c.close()
