@@ -310,6 +310,21 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     return res
 
 
+def l2_copy_rate():
+    """Copy rate of an L2-resident buffer (GB/s, read + write bytes): torch's
+    copy of 24 MB into 24 MB, 200 times back to back, CUDA events — the L2
+    counterpart of the measured HBM copy peak, for the grids whose whole state
+    stays in the 126 MB L2."""
+    import torch
+    n = 6 * 1024 * 1024
+    a = torch.randn(n, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    t, _ = _timed(lambda: [b.copy_(a) for _ in range(200)])
+    return 2.0 * 4 * n * 200 / t / 1e9
+
+
 def extra_legs(device):
     """Rates of the other workload configurations (each a bounded part of its job)."""
     import torch
@@ -329,9 +344,11 @@ def extra_legs(device):
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         l1 = ctx.last_stats
         cells = m.padded_cells * st["fd_nt"]
+        l2 = l2_copy_rate()
         out["c1"] = {"workload": "1000x1000 two-layer, nb 40, 1 shot, full 2000 steps", "gcells_per_s": cells / t / 1e9,
                      "shots_per_s": 1.0 / t, "job_s": t, "roofline_frac": ctx.last_stats.alg_bytes / t / 1e9 / peak,
-                     "note": "whole job ~37 MB of state: L2-resident",
+                     "l2_copy_gbs": l2, "roofline_frac_l2": ctx.last_stats.alg_bytes / t / 1e9 / l2,
+                     "note": "whole job ~37 MB of state: L2-resident; roofline_frac_l2 against the L2 copy rate",
                      "launch": {"variant": l1.variant, "seg_len": l1.seg_len, "task_order": l1.task_order}}
         m.release()
         # c3: salt 3201x1201, d 7.62, nb 50, 20 Hz, dt 0.6 ms, nt 10000, 1 shot; 1000 of the 10000 steps
