@@ -731,7 +731,7 @@ def main():
                  "sample": f"{nshots} shots x {pch} FD steps, shot after shot"}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, err = ref_cpu_rate(w)
         if cpu is None:
             cpu = {"unavailable": err}
