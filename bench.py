@@ -286,7 +286,7 @@ def gradient_leg(ctx, nshots=32, T=3.0, fd_order=4):
     ms = ctx.model(start, rho, 10.0, 10.0, 50, fd_order=fd_order)
     shots = [Shot(ms, s_, rec) for s_ in src]
     fbuf = torch.zeros_like(dobs)
-    ctx.forward(shots, wave, kt_count=100, out=fbuf)  # autotunes this shape (>= 80 steps) outside the timing
+    ctx.forward(shots, wave, kt_count=120, out=fbuf)  # autotunes this shape (>= 112 steps) outside the timing
     tf, _ = _timed(lambda: ctx.forward(shots, wave, out=fbuf, sync=False))
     gvp = torch.zeros(1201, 401, dtype=torch.float32, device="cuda")
     grho = torch.zeros_like(gvp)
@@ -340,7 +340,7 @@ def extra_legs(device):
         st = derive_steps(wave)
         buf = torch.zeros(rec.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
         shots = [Shot(m, src[0], rec)]
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 80 steps)
+        ctx.forward(shots, wave, kt_count=120, out=buf)  # warm-up; autotunes this shape (>= 112 steps)
         t, _ = _timed(lambda: ctx.forward(shots, wave, out=buf, sync=False))
         l1 = ctx.last_stats
         cells = m.padded_cells * st["fd_nt"]
@@ -360,8 +360,8 @@ def extra_legs(device):
         rec = np.stack([np.arange(3201, dtype=np.float32) * np.float32(7.62), np.full(3201, 2 * 7.62, np.float32)], 1)
         buf = torch.zeros(3201 * st["real_nt"], dtype=torch.float32, device="cuda")
         shots = [Shot(m, src, rec)]
-        ctx.forward(shots, wave, kt_count=100, out=buf)
-        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=1000, out=buf, sync=False))
+        ctx.forward(shots, wave, kt_count=120, out=buf)  # warm-up; autotunes this shape (>= 112 steps)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=120, kt_count=1000, out=buf, sync=False))
         cells = m.padded_cells * 1000
         rate = cells / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
@@ -384,8 +384,8 @@ def extra_legs(device):
             cells_step += 16 * mm.padded_cells
             total_rec += 16 * rec.shape[0]
         buf = torch.zeros(total_rec * st["real_nt"], dtype=torch.float32, device="cuda")
-        ctx.forward(shots, wave, kt_count=100, out=buf)  # warm-up; autotunes this shape (>= 80 steps)
-        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=100, kt_count=300, out=buf, sync=False))
+        ctx.forward(shots, wave, kt_count=120, out=buf)  # warm-up; autotunes this shape (>= 112 steps)
+        t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=120, kt_count=300, out=buf, sync=False))
         rate = cells_step * 300 / t / 1e9
         frac = ctx.last_stats.alg_bytes / t / 1e9 / peak
         l4 = ctx.last_stats
@@ -410,8 +410,8 @@ def extra_legs(device):
             st = derive_steps(wave)
             shots = [Shot(m, s_, rec2) for s_ in src2[:16]]
             buf = torch.zeros(16 * rec2.shape[0] * st["real_nt"], dtype=torch.float32, device="cuda")
-            ctx.forward(shots, wave, kt_count=40, out=buf)
-            t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=40, kt_count=200, out=buf, sync=False))
+            ctx.forward(shots, wave, kt_count=70, out=buf)  # autotunes the shape (>= 64 steps)
+            t, _ = _timed(lambda: ctx.forward(shots, wave, kt_begin=70, kt_count=200, out=buf, sync=False))
             l8 = ctx.last_stats
             rate = 16 * m.padded_cells * 200 / t / 1e9
             out["c2_order8"] = {"workload": "5000x5000 two-layer, nb 60, 8th-order operator, 16 shots x 5000 "

@@ -152,15 +152,16 @@ S2D_API const char *s2d_last_error(const void *ctx);
 /*
  * Tuning knobs of the step kernel; no counterpart in the reference.  Keys:
  *   "autotune"    1 (default): the first s2d_forward of a batched run of a new
- *                 shape (models, grids, shot counts) with at least 80 steps
- *                 spends 40 of them on 9 candidate configurations (variants
- *                 4, 16, 15, 2, 5, 11, 12 in task order 1, and 16 and 15 in
- *                 task order 0, unless "task_order" was set), one untimed and
- *                 three timed launches each, in rounds (the results do not
- *                 change: every candidate computes the same bits), times them
- *                 with events and keeps the fastest per FD step for that shape
- *                 in the context; runs that do not tune (shorter calls,
- *                 S2D_PLAIN) use variant 16.
+ *                 shape (models, grids, shot counts) with at least 112 steps
+ *                 (64 for the 8th-order operator) spends up to 56 (32) of them
+ *                 on trials: 9 candidate configurations (variants 4, 16, 15,
+ *                 2, 5, 11, 12 in task order 1, and 16 and 15 in task order 0,
+ *                 unless "task_order" was set), one untimed and three timed
+ *                 launches each, in rounds, then four more timed launches each
+ *                 of the two fastest, alternating (the results do not change:
+ *                 every candidate computes the same bits); it keeps the fastest
+ *                 per FD step for that shape in the context; runs that do not
+ *                 tune (shorter calls, S2D_PLAIN) use variant 16.
  *                 0: use "variant", "block" and "stages".
  *                 Setting any of those three turns autotuning off.
  *   "variant"     0 bulk-copy pipeline, 1 plain loads, 2 bulk-copy pipeline

@@ -847,14 +847,17 @@ constexpr int kTuneCandidatesO8[][4] = {
     {kVariantO8, 128, 0, 1}, {kVariantO8r, 128, 0, 1}, {kVariantO8s, 128, 0, 1}, {kVariantO8, 128, 0, 0}};
 constexpr int kNumTuneCandidatesO8 = (int)(sizeof(kTuneCandidatesO8) / sizeof(kTuneCandidatesO8[0]));
 constexpr int kTuneWarm = 1, kTuneTimed = 3;  // launches per candidate
+constexpr int kTuneRunoff = 4;                 // more timed launches of each of the two best
 // FD steps the trials take (a two-step candidate advances two per launch).
 constexpr int tune_steps(const int (*cand)[4], int n) {
     int steps = 0;
     for (int i = 0; i < n; ++i) steps += (kTuneWarm + kTuneTimed) * steps_per_launch(cand[i][0]);
     return steps;
 }
-constexpr int kTuneSteps = tune_steps(kTuneCandidates, kNumTuneCandidates);
-constexpr int kTuneStepsO8 = tune_steps(kTuneCandidatesO8, kNumTuneCandidatesO8);
+// The most FD steps the trials and the runoff take (two two-step candidates
+// in the runoff at most).
+constexpr int kTuneSteps = tune_steps(kTuneCandidates, kNumTuneCandidates) + 2 * kTuneRunoff * 2;
+constexpr int kTuneStepsO8 = tune_steps(kTuneCandidatesO8, kNumTuneCandidatesO8) + 2 * kTuneRunoff * 2;
 
 // Sum of the task counts of a batched launch sequence.
 int batch_tasks(const Batch &b) {
@@ -869,18 +872,22 @@ int plain_tasks(const Batch &b, int s) {
     return (b.layout_tma ? tma_blocks(1, g.nstrips) : g.nstrips) * g.nsegs;
 }
 
-// Autotuner: advance the batch by kTuneSteps real FD steps from kt_begin,
-// kTuneWarm + kTuneTimed launches under each candidate configuration, in
-// rounds that visit every candidate once (every
+// Autotuner: advance the batch by real FD steps from kt_begin (*steps_used
+// of them, at most kTuneStepsMax): kTuneWarm + kTuneTimed launches under each
+// candidate configuration, in rounds that visit every candidate once (every
 // candidate computes the same bits: they share the update arithmetic and
 // differ only in how columns reach registers, how many steps a pass makes and
-// how tasks map to warps), with each timed launch between two events.  The
-// candidate with the lowest median time per FD step is cached for the batch's
-// shape and returned, its segment layout in place.
-int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best) {
+// how tasks map to warps), with each timed launch between two events; then a
+// runoff of kTuneRunoff more timed launches each, alternating, between the
+// two candidates with the lowest median time per FD step, which decides
+// between configurations whose medians lie within the trials' noise.  The
+// winner is cached for the batch's shape and returned, its segment layout in
+// place.
+int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCfg *best, int *steps_used) {
     const int (*const cands)[4] = b.order8 ? kTuneCandidatesO8 : kTuneCandidates;
     const int ncand = b.order8 ? kNumTuneCandidatesO8 : kNumTuneCandidates;
-    std::vector<cudaEvent_t> ev(2 * kTuneTimed * ncand, nullptr);
+    const int nev = 2 * std::max(kTuneTimed * ncand, 2 * kTuneRunoff);
+    std::vector<cudaEvent_t> ev(nev, nullptr);
     for (auto &e : ev) {
         cudaError_t ce = cudaEventCreate(&e);
         if (ce != cudaSuccess) {
@@ -889,9 +896,12 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
             return fail(c, S2D_ERR_CUDA, "autotune events: %s", cudaGetErrorString(ce));
         }
     }
-    auto release = [&]() {
-        for (auto &x : ev) cudaEventDestroy(x);
-    };
+    struct Release {
+        std::vector<cudaEvent_t> &ev;
+        ~Release() {
+            for (auto &x : ev) cudaEventDestroy(x);
+        }
+    } release{ev};
     std::vector<LaunchCfg> cfg(ncand), full(ncand);
     std::vector<bool> ok(ncand, false);
     for (int i = 0; i < ncand; ++i) {
@@ -900,61 +910,80 @@ int autotune(Ctx *c, Batch &b, StepArgs a, int kt_begin, int *launches, LaunchCf
             ok[i] = true;
             full[i].order = c->order_fixed ? -1 : k[3];
         } else {
-            if (i == 0) {
-                release();
-                return S2D_ERR_ARG;
-            }
+            if (i == 0) return S2D_ERR_ARG;
             // a configuration this device cannot run: its trial steps run
             // under the first candidate instead and are not counted
             full[i] = full[0];
         }
     }
-    // Rounds: one untimed, then kTuneTimed timed, each visiting every
-    // candidate once, so clock ramps and drift reach all candidates alike.
     int kt = kt_begin;
     bool graph_used = false;
+    // one launch of candidate i, timed between ev[e0] and ev[e0 + 1] when
+    // e0 >= 0; the interval starts after the launch-argument update (a small
+    // kernel of its own), so it holds the step launch alone
+    auto trial = [&](int i, int e0) -> int {
+        LaunchCfg lc = full[i];
+        int e = layout_groups(c, b, lc);
+        if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
+        if (e) return e;
+        lc.order = full[i].order;
+        cfg[i] = lc;
+        a.total_tasks = batch_tasks(b);
+        const int spl = steps_per_launch(lc.variant);
+        e = run_loop(c, b, lc, a, kt, spl, false, launches, &graph_used, e0 >= 0 ? ev[e0] : nullptr);
+        if (e) return e;
+        if (e0 >= 0) CK(cudaEventRecord(ev[e0 + 1], c->stream));
+        kt += spl;
+        return S2D_OK;
+    };
+    // Rounds: one untimed, then kTuneTimed timed, each visiting every
+    // candidate once, so clock ramps and drift reach all candidates alike.
     for (int r = 0; r < kTuneWarm + kTuneTimed; ++r) {
         const int t = r - kTuneWarm;
         for (int i = 0; i < ncand; ++i) {
-            LaunchCfg lc = full[i];
-            int e = layout_groups(c, b, lc);
-            if (!e) e = launch_config(c, b.max_tasks, &lc, lc.variant, lc.block, lc.stages);
-            if (e) {
-                release();
-                return e;
-            }
-            lc.order = full[i].order;
-            cfg[i] = lc;
-            a.total_tasks = batch_tasks(b);
-            const int spl = steps_per_launch(lc.variant);
-            // the trial interval starts after the launch-argument update (a
-            // small kernel of its own), so it holds the step launch alone
-            e = run_loop(c, b, lc, a, kt, spl, false, launches, &graph_used,
-                         t >= 0 ? ev[2 * (i * kTuneTimed + t)] : nullptr);
-            if (e) {
-                release();
-                return e;
-            }
-            if (t >= 0) CK(cudaEventRecord(ev[2 * (i * kTuneTimed + t) + 1], c->stream));
-            kt += spl;
+            int e = trial(i, t >= 0 ? 2 * (i * kTuneTimed + t) : -1);
+            if (e) return e;
         }
     }
-    cudaError_t ce = cudaStreamSynchronize(c->stream);
-    int pick = 0;
-    float pick_ms = 0;
-    for (int i = 0; i < ncand && ce == cudaSuccess; ++i) {
+    CK(cudaStreamSynchronize(c->stream));
+    int pick = 0, second = -1;
+    float pick_ms = 0, second_ms = 0;
+    for (int i = 0; i < ncand; ++i) {
         float t[kTuneTimed];
-        for (int s = 0; s < kTuneTimed && ce == cudaSuccess; ++s)
-            ce = cudaEventElapsedTime(&t[s], ev[2 * (i * kTuneTimed + s)], ev[2 * (i * kTuneTimed + s) + 1]);
+        for (int s = 0; s < kTuneTimed; ++s)
+            CK(cudaEventElapsedTime(&t[s], ev[2 * (i * kTuneTimed + s)], ev[2 * (i * kTuneTimed + s) + 1]));
         std::sort(t, t + kTuneTimed);
         const float med = t[kTuneTimed / 2] / (float)steps_per_launch(cfg[i].variant);  // per FD step
-        if (ok[i] && (i == 0 || med < pick_ms)) {
+        if (!ok[i]) continue;
+        if (i == 0 || med < pick_ms) {
+            second = i == 0 ? -1 : pick;
+            second_ms = pick_ms;
             pick = i;
             pick_ms = med;
+        } else if (second < 0 || med < second_ms) {
+            second = i;
+            second_ms = med;
         }
     }
-    release();
-    CK(ce);
+    // runoff between the two best: kTuneRunoff timed launches each, alternating
+    if (second >= 0) {
+        const int two[2] = {pick, second};
+        for (int r = 0; r < kTuneRunoff; ++r)
+            for (int q = 0; q < 2; ++q) {
+                int e = trial(two[q], 2 * (r * 2 + q));
+                if (e) return e;
+            }
+        CK(cudaStreamSynchronize(c->stream));
+        float tot[2] = {0.0f, 0.0f};
+        for (int r = 0; r < kTuneRunoff; ++r)
+            for (int q = 0; q < 2; ++q) {
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, ev[2 * (r * 2 + q)], ev[2 * (r * 2 + q) + 1]));
+                tot[q] += ms / (float)steps_per_launch(cfg[two[q]].variant);
+            }
+        if (tot[1] < tot[0]) pick = second;
+    }
+    *steps_used = kt - kt_begin;
     const int *k = cands[pick];
     c->tuned[tune_key(c, b)] = {k[0], k[1], k[2], full[pick].order};
     int e = layout_groups(c, b, cfg[pick]);
@@ -1225,9 +1254,10 @@ int s2d_forward(void *ctx, const s2d_shot *shots, int nshots, const s2d_wave *wa
     if (c->opt_autotune && !tuned && !b.plain && nsteps >= 2 * tune_len) {
         a.groups = b.groups_d.as<GroupDev>();
         a.ngroups = (int)b.groups.size();
-        int e = autotune(c, b, a, kt_begin, &launches, &lc);
+        int used = 0;
+        int e = autotune(c, b, a, kt_begin, &launches, &lc, &used);
         if (e) return e;
-        kt_run += tune_len;
+        kt_run += used;
         tuned_now = 1;
     }
     if (b.plain) {

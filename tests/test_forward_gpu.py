@@ -336,7 +336,7 @@ def test_variants_compute_the_same_bits(ctx):
 
 
 def test_autotuner_tunes_once_per_shape_and_keeps_the_bits():
-    """A fresh context tunes on the first run of a batch shape (40 of its
+    """A fresh context tunes on the first run of a batch shape (up to 56 of its
     steps, variant and task order), reuses the result for the next run of
     that shape, and the traces equal those of a fixed configuration."""
     from seis2d_b200 import Context
