@@ -762,7 +762,9 @@ __device__ __forceinline__ float4 &ring_at(float4 *ring, int field, int col, int
     return ring[(field * kTsRing + ((col + 2 * S2D_GX) & (kTsRing - 1))) * 32 + lane];
 }
 
-template <bool FAST, bool TWO>
+// XF: every column either step updates or differentiates (xa-4 .. xb+4)
+// lies in the shot's x-interior: literal column coefficients.
+template <bool FAST, bool TWO, bool XF = false>
 __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len,
                                         int kt, int par, int lane, float4 *ring) {
     const int xb = min(S.nnx, xa + seg_len);
@@ -809,8 +811,8 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const int PA = L - 1;
         const ptrdiff_t colA = (ptrdiff_t)PA * (ptrdiff_t)ld;
         const ptrdiff_t colV0 = (ptrdiff_t)(L - 3) * (ptrdiff_t)ld;
-        const float4 xa4 = __ldg(S.xcoef + (PA + S2D_GX));
-        const bool colm = xa4.x == 1.0f;
+        const float4 xa4 = XF ? make_float4(1.0f, la.kx, 1.0f, la.kx) : __ldg(S.xcoef + (PA + S2D_GX));
+        const bool colm = XF || xa4.x == 1.0f;
         const bool pz_live = !(FAST && colm);
         const float4 cvx = ld4(vxi + (ptrdiff_t)L * (ptrdiff_t)ld);
         const float4 cvz = ld4(vzi + colA);
@@ -824,7 +826,8 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const float4 vz = cvz;
         float4 pxn, pzn, dxv, dzv;
         const float4 kka = ckk;
-        const float4 pn = p_update(la, S, PA, xa4, colm, vq0, vq1, vq2, vq3, cpx, cpz, kka, vz, pxn, pzn, dxv, dzv);
+        const float4 pn =
+            p_update<FAST, XF>(la, S, PA, xa4, colm, vq0, vq1, vq2, vq3, cpx, cpz, kka, vz, pxn, pzn, dxv, dzv);
         const bool in_a = PA >= xa && PA < xb;
         if (TWO) {
             ring_at(ring, 0, PA, lane) = pxn;
@@ -842,7 +845,7 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const ptrdiff_t colVA = (ptrdiff_t)VA * (ptrdiff_t)ld;
         float4 vxn, vzn, dxp, dzp;
         const float4 bxa = cbx, bza = cbz;
-        v_update(la, S, VA, pq0, pq1, pq2, pq3, vq0, zq0, bxa, bza, vxn, vzn, dxp, dzp);
+        v_update<FAST, XF>(la, S, VA, pq0, pq1, pq2, pq3, vq0, zq0, bxa, bza, vxn, vzn, dxp, dzp);
         if (!TWO) {
             if (la.owner) {
                 st4(vxo + colVA, vxn);
@@ -857,11 +860,12 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const int PB = L - 4;
         const ptrdiff_t colB = (ptrdiff_t)PB * (ptrdiff_t)ld;
         const float4 vzb = ring_at(ring, 2, PB, lane);
-        const float4 xb4 = __ldg(S.xcoef + (PB + S2D_GX));
-        const bool colmb = xb4.x == 1.0f;
+        const float4 xb4 = XF ? make_float4(1.0f, lb.kx, 1.0f, lb.kx) : __ldg(S.xcoef + (PB + S2D_GX));
+        const bool colmb = XF || xb4.x == 1.0f;
         const bool pz_liveb = !(FAST && colmb);
         float4 pxm, pzm, dxw, dzw;
-        const float4 pm = p_update(lb, S, PB, xb4, colmb, ring_at(ring, 3, PB - 2, lane), ring_at(ring, 3, PB - 1, lane),
+        const float4 pm = p_update<FAST, XF>(lb, S, PB, xb4, colmb, ring_at(ring, 3, PB - 2, lane),
+                                             ring_at(ring, 3, PB - 1, lane),
                                    ring_at(ring, 3, PB, lane), ring_at(ring, 3, PB + 1, lane), ring_at(ring, 0, PB, lane),
                                    pz_liveb ? ring_at(ring, 1, PB, lane) : zero, ld4(kap + colB), vzb,
                                    pxm, pzm, dxw, dzw);
@@ -877,7 +881,8 @@ __device__ __forceinline__ void ts_task(const StepArgs &a, const ShotDev &S, int
         const int VB = L - 6;
         const ptrdiff_t colVB = (ptrdiff_t)VB * (ptrdiff_t)ld;
         float4 vxm, vzm, dxq, dzq;
-        v_update(lb, S, VB, ring_at(ring, 4, VB - 1, lane), ring_at(ring, 4, VB, lane), ring_at(ring, 4, VB + 1, lane),
+        v_update<FAST, XF>(lb, S, VB, ring_at(ring, 4, VB - 1, lane), ring_at(ring, 4, VB, lane),
+                           ring_at(ring, 4, VB + 1, lane),
                  ring_at(ring, 4, VB + 2, lane), ring_at(ring, 3, VB, lane), ring_at(ring, 2, VB, lane),
                  ld4(bxp + colVB), ld4(bzp + colVB), vxm, vzm, dxq, dzq);
         if (la.owner) {
@@ -905,10 +910,13 @@ __global__ void __launch_bounds__(128, 4) step_kernel_ts(const StepArgs *__restr
         const ShotDev &G = task_of(a, t, strip, xa, seg_len);
         warp_copy_shot(S, G, lane);
         const int c = strip * S2D_TS_OUT - 8;
-        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1))
-            ts_task<true, TWO>(a, S, strip, xa, seg_len, kt, par, lane, ring);
-        else
-            ts_task<false, TWO>(a, S, strip, xa, seg_len, kt, par, lane, ring);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1);
+        // columns xa-4 .. xb+4 take part (step A's p reaches xb+4, feeding its v at xb+2)
+        const bool xf = xa - 4 >= S.xfast_lo && min(S.nnx, xa + seg_len) + 4 < S.xfast_hi;
+        if (zf && xf) ts_task<true, TWO, true>(a, S, strip, xa, seg_len, kt, par, lane, ring);
+        else if (zf) ts_task<true, TWO, false>(a, S, strip, xa, seg_len, kt, par, lane, ring);
+        else if (xf) ts_task<false, TWO, true>(a, S, strip, xa, seg_len, kt, par, lane, ring);
+        else ts_task<false, TWO, false>(a, S, strip, xa, seg_len, kt, par, lane, ring);
     }
 }
 
