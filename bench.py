@@ -207,7 +207,7 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def traffic_per_launch(workload, nshots):
+def traffic_per_launch(workload, nshots, variant=None):
     """Measured DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum)
     of one step launch over ``nshots`` shots, from the committed ncu summary
     (profiles/traffic.json), scaled from the captured shot count by the
@@ -218,6 +218,8 @@ def traffic_per_launch(workload, nshots):
         return None
     try:
         t = json.load(open(p)).get(workload)
+        if variant is not None and int(t.get("variant", variant)) != int(variant):
+            return None  # captured for another step kernel
         b = float(t["per_shot_bytes"]) * nshots + float(t.get("per_model_bytes", 0.0))
         return {"bytes": b, "source": t["source"]}
     except (TypeError, KeyError, ValueError):
@@ -676,7 +678,7 @@ def main():
     # bytes of the launches / their device time (library events on its stream)
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (loop_ms * 1e-3) / 1e9
-    tr = traffic_per_launch(args.workload, nshots)
+    tr = traffic_per_launch(args.workload, nshots, next(iter(variants)) if len(variants) == 1 else None)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr["bytes"] if tr else None, "traffic_source": tr["source"] if tr else None,
             "peak_source": peak_kind, "bytes_per_launch": alg_bytes / max(1, fd_launches),
