@@ -54,6 +54,9 @@ def test_roofline_traffic_and_minimal_bytes():
     t2, t64 = bench.traffic_per_launch("c2", 2), bench.traffic_per_launch("c2", 64)
     assert t2 and t64 and t64["bytes"] > 30 * t2["bytes"] / 2 * 0.9
     assert abs(t2["bytes"] - 1.622e9) < 0.01e9  # the measured 2-shot launch
+    # the record holds one step kernel's capture: none for another kernel
+    assert bench.traffic_per_launch("c2", 64, 16) == t64
+    assert bench.traffic_per_launch("c2", 64, 5) is None
     for n in (1, 64):
         b = bench.dram_minimal_bytes(bench.WORKLOADS["c2"], n)
         assert 24.0 + 12.0 / n <= b <= 32.0 + 12.0 / n
