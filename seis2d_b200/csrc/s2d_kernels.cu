@@ -1131,7 +1131,8 @@ __device__ __forceinline__ float4 &o8_ring(float4 *ring, int field, int col, int
     return field == 2 ? ring[(16 + (col & 3)) * 32 + lane] : ring[(field * 8 + (col & 7)) * 32 + lane];
 }
 
-template <bool FAST>
+// XF: as for o8_task, literal column coefficients on x-interior tasks.
+template <bool FAST, bool XF = false>
 __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, int strip, int xa, int seg_len, int kt,
                                          int par, bool rec_step, int slot, int lane, float4 *ring) {
     const int xb = min(S.nnx, xa + seg_len);
@@ -1140,7 +1141,9 @@ __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, in
     Lane<FAST> ln;
     lane_setup(ln, S, c, lane, kt);
     ln.owner = lane >= 2 && lane <= 29;
-    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD);
+    // receivers only where the strip's rows hold some
+    const bool rec = rec_step && slot < S.real_nt && !(a.flags & S2D_STEP_NO_RECORD) &&
+                     c + S2D_STRIP_ROWS > S.rec_zlo && c <= S.rec_zhi;
     const size_t off = (size_t)(ln.z0 + S2D_GZ) + (size_t)S2D_GX * ld;
     const int fs = S.fstride;
     float *const sb = S.st[0][0] + off;
@@ -1167,12 +1170,13 @@ __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, in
         for (int i = 0; i < 7; ++i) w[i] = o8_ring(ring, 0, L - 7 + i, lane);
         o8_ring(ring, 0, L, lane) = w[7];  // the slot of column L-8, no longer needed
         const float4 vz = ld4(vzi + colP);
-        const float4 xc = __ldg(S.xcoef + (P + S2D_GX));
-        const bool colm = xc.x == 1.0f;
+        const float4 xc = XF ? make_float4(1.0f, ln.kx, 1.0f, ln.kx) : __ldg(S.xcoef + (P + S2D_GX));
+        const bool colm = XF || xc.x == 1.0f;
         const bool pz_live = !(FAST && colm);
         float4 pxn, pzn, dxv, dzv;
-        const float4 pn = p_update8(ln, S, P, xc, colm, w, ld4(pxi + colP), pz_live ? ld4(pzi + colP) : zero,
-                                    ld4(kap + colP), vz, pxn, pzn, dxv, dzv);
+        const float4 pn = p_update8<FAST, XF>(ln, S, P, xc, colm, w, ld4(pxi + colP),
+                                              pz_live ? ld4(pzi + colP) : zero, ld4(kap + colP), vz, pxn, pzn, dxv,
+                                              dzv);
         const bool in_seg = P >= xa && P < xb;
         if (in_seg && ln.owner) {
             st4(pxo + colP, pxn);
@@ -1190,7 +1194,7 @@ __device__ __forceinline__ void o8s_task(const StepArgs &a, const ShotDev &S, in
             for (int i = 0; i < 7; ++i) pw[i] = o8_ring(ring, 1, V - 3 + i, lane);
             pw[7] = pn;
             float4 vxn, vzn, dxp, dzp;
-            v_update8(ln, S, V, pw, w[0], vzV, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
+            v_update8<FAST, XF>(ln, S, V, pw, w[0], vzV, ld4(bxp + colV), ld4(bzp + colV), vxn, vzn, dxp, dzp);
             if (ln.owner) {
                 st4(vxo + colV, vxn);
                 st4(vzo + colV, vzn);
@@ -1273,10 +1277,14 @@ __global__ void __launch_bounds__(128, 4) step_kernel_o8s(const StepArgs *__rest
         warp_copy_shot(S, G, lane);
         if (!o8_in_bounds(a, S, strip, xa, seg_len)) continue;
         const int c = strip * S2D_TS_OUT - 8;
-        if (rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5)
-            o8s_task<true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
-        else
-            o8s_task<false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        const bool zf = rows_fast(S, c, c + S2D_STRIP_ROWS - 1) && c >= 4 && c + S2D_STRIP_ROWS - 1 <= S.nnz - 5;
+        // the columns of o8_task's x-interior condition
+        const int xb = min(S.nnx, xa + seg_len);
+        const bool xf = xa - 3 >= max(S.xfast_lo, 4) && xb + 3 < min(S.xfast_hi, S.nnx - 3);
+        if (zf && xf) o8s_task<true, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else if (zf) o8s_task<true, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else if (xf) o8s_task<false, true>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
+        else o8s_task<false, false>(a, S, strip, xa, seg_len, kt, par, rec_step, slot, lane, ring);
     }
 }
 
