@@ -687,6 +687,12 @@ def main():
             "launch_ms": loop_ms / max(1, fd_launches), "launches": fd_launches,
             "fd_steps_per_launch": 2 if variants == {5} else 1,
             "timed_region": f"the {args.steps} timed calls ({fd_launches} step launches)"}
+    if variants == {5}:
+        # the two-step kernel moves the state once per two steps: the fraction
+        # of the peak a one-step kernel would need for the same rate
+        one = roof["bytes_per_cell_update"] * 2
+        roof["one_step_equivalent"] = {"bytes_per_cell_update": one,
+                                       "frac": total_cells * one / (ms * 1e-3) / 1e9 / world / peak}
 
     # ---- end to end through the C ABI from pinned host memory ----
     e2e = None
